@@ -1,0 +1,260 @@
+/*
+ * solvix_gpu.h - C ABI of the B200 linear-static path of Solvix.
+ *
+ * This header is the drop-in boundary for solvix-core's linear-static hot
+ * path: Gauss-point element stiffness integration (CPS3 / CPS4 / C3D8),
+ * global CSR assembly, symmetric Dirichlet elimination, Jacobi-PCG and
+ * stress / reaction recovery.  In the reference these are the pub(crate)
+ * functions called from `solve_with_thermal`
+ * (crates/solvix-core/src/lib.rs:593-716, the steps at :614-703).
+ *
+ * Conventions
+ *   - Every function returns an `int` status (SVX_OK on success) and, where
+ *     a model can be rejected, fills a caller-owned `svx_error_t`.
+ *   - The caller owns every host array.  The library copies inputs in and
+ *     writes outputs into caller-allocated arrays.  Device memory is owned
+ *     by the library behind opaque handles and released by the *_free /
+ *     *_destroy functions.
+ *   - Calls on different contexts are thread safe (one CUDA stream per
+ *     context).  A single context or operator must not be used from two
+ *     threads at once.  Calls block until their host outputs are written.
+ *   - Indices are 0-based; node and element ids are the model's own ids and
+ *     are only used for error messages and reaction records.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     entry point returns SVX_CUDA_ERROR.
+ */
+#ifndef SOLVIX_GPU_H
+#define SOLVIX_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes.  1-4 are the reference's SolveError variants          */
+/* (crates/solvix-core/src/lib.rs:515-521); the rest are device-side.  */
+/* ------------------------------------------------------------------ */
+enum svx_status {
+    SVX_OK = 0,
+    SVX_EMPTY_MESH = 1,      /* SolveError::EmptyMesh */
+    SVX_NO_CONSTRAINTS = 2,  /* SolveError::NoConstraints */
+    SVX_INVALID_MODEL = 3,   /* SolveError::InvalidModel(message) */
+    SVX_NOT_CONVERGED = 4,   /* SolveError::NotConverged{iterations, residual} */
+    SVX_OOM = 5,             /* device memory (or admission budget) exhausted */
+    SVX_CUDA_ERROR = 6,      /* no device, launch failure, driver error */
+    SVX_BAD_ARGUMENT = 7,    /* null pointer, inconsistent sizes */
+    SVX_QUEUE_EMPTY = 8      /* server poll: nothing completed yet */
+};
+
+/* Element kinds, in the order of the reference's ElemKind enum
+ * (crates/solvix-core/src/lib.rs:54-73).  The GPU path integrates
+ * CPS3, CPS4 and C3D8; the other kinds are rejected as InvalidModel. */
+enum svx_elem_kind {
+    SVX_CPS3 = 0,
+    SVX_CPS4 = 1,
+    SVX_CPS8 = 2,
+    SVX_CPE4 = 3,
+    SVX_CPE8 = 4,
+    SVX_C3D8 = 5,
+    SVX_C3D4 = 6,
+    SVX_B31 = 7
+};
+
+/* Why an element was rejected (svx_error_t.reason). */
+enum svx_elem_reason {
+    SVX_REASON_NONE = 0,
+    SVX_REASON_NO_MATERIAL = 1,      /* assembly.rs:144-146 */
+    SVX_REASON_BAD_MATERIAL = 2,     /* assembly.rs:147-149 */
+    SVX_REASON_SOLID_POISSON = 3,    /* assembly.rs:150-160 */
+    SVX_REASON_DEGENERATE_TRI = 4,   /* assembly.rs:175 */
+    SVX_REASON_BAD_JACOBIAN = 5,     /* assembly.rs:195, :259-261 */
+    SVX_REASON_UNSUPPORTED_KIND = 6  /* kinds outside CPS3/CPS4/C3D8 */
+};
+
+/* Error record.  `message` holds the text the reference carries in the
+ * SolveError payload (e.g. "element 7: non-positive Jacobian determinant
+ * at a Gauss point" for InvalidModel), NUL terminated. */
+typedef struct svx_error {
+    int32_t code;        /* enum svx_status */
+    int32_t reason;      /* enum svx_elem_reason for element failures */
+    int64_t elem_index;  /* first failing element in enumeration order, or -1 */
+    int64_t iterations;  /* NotConverged: iteration reached */
+    double residual;     /* NotConverged: recursive ||r||/||f|| there */
+    char message[512];
+} svx_error_t;
+
+/* ------------------------------------------------------------------ */
+/* Reference-shaped model (solvix_core::Model after Model::load_state,  */
+/* crates/solvix-core/src/lib.rs:250-307, :388-403).  Node and element  */
+/* references are by id; materials are resolved through element sets.  */
+/* ------------------------------------------------------------------ */
+typedef struct svx_model_desc {
+    int64_t n_nodes;
+    const uint32_t* node_ids;     /* [n_nodes] */
+    const double* node_coords;    /* [3 * n_nodes], x y z per node */
+
+    int64_t n_elems;
+    const uint32_t* elem_ids;     /* [n_elems] */
+    const uint8_t* elem_kinds;    /* [n_elems] enum svx_elem_kind */
+    const int64_t* elem_conn_ptr; /* [n_elems + 1] */
+    const uint32_t* elem_conn;    /* node ids, [elem_conn_ptr[n_elems]] */
+
+    int32_t n_materials;
+    const char* const* material_names;
+    const double* youngs_modulus;
+    const double* poisson_ratio;
+
+    int32_t n_elsets;
+    const char* const* elset_names;
+    const int64_t* elset_ptr;        /* [n_elsets + 1] */
+    const uint32_t* elset_elem_ids;  /* element ids */
+
+    int32_t n_assignments;           /* (elset, material) pairs, in order */
+    const char* const* assign_elset;
+    const char* const* assign_material;
+
+    double thickness;
+
+    int32_t n_bcs;                   /* BoundaryCondition{node_ids, dofs} */
+    const int64_t* bc_node_ptr;      /* [n_bcs + 1] */
+    const uint32_t* bc_node_ids;
+    const int64_t* bc_dof_ptr;       /* [n_bcs + 1] */
+    const int64_t* bc_dofs;          /* 1-based dofs */
+
+    int64_t n_cloads;                /* ConcentratedLoad{node_id, dof, value} */
+    const uint32_t* cload_node_ids;
+    const int64_t* cload_dofs;       /* 1-based */
+    const double* cload_values;
+} svx_model_desc_t;
+
+/* ------------------------------------------------------------------ */
+/* Flat, index-resolved model: what the device path consumes.          */
+/* ------------------------------------------------------------------ */
+typedef struct svx_flat_model {
+    int64_t n_nodes;
+    const double* xyz;            /* [3 * n_nodes] */
+    const uint32_t* node_id;      /* [n_nodes] ids (NULL: index + 1) */
+
+    int64_t n_elem;
+    const uint8_t* kind;          /* [n_elem] enum svx_elem_kind */
+    const int64_t* conn_ptr;      /* [n_elem + 1] */
+    const int32_t* conn;          /* 0-based node indices */
+    const double* youngs;         /* [n_elem] E per element */
+    const double* poisson;        /* [n_elem] nu per element */
+    const uint8_t* no_material;   /* [n_elem] 1 = no material (NULL: all 0) */
+    const uint32_t* elem_id;      /* [n_elem] ids (NULL: index + 1) */
+
+    double thickness;             /* model-wide, plane elements only */
+    int32_t ndof;                 /* 2 (plane) or 3 (solid) */
+
+    int64_t n_fixed;              /* constrained dof rows in BC order */
+    const int64_t* fixed_row;     /* node_index * ndof + dof - 1 */
+    const double* f;              /* [n_nodes * ndof] load vector */
+} svx_flat_model_t;
+
+/* Resolved model produced from a svx_model_desc_t (owned by the library). */
+typedef struct svx_resolved svx_resolved_t;
+
+/* Precision forms of the PCG solve. */
+enum svx_precision {
+    SVX_FP64 = 0,   /* FP64 K, FP64 PCG: the plain form */
+    SVX_MIXED = 1   /* FP32-stored K, FP32 inner PCG, FP64 defect correction */
+};
+
+typedef struct svx_solve_opts {
+    double tol;            /* relative residual tolerance (reference: 1e-10) */
+    int64_t max_iter;      /* <= 0: max(1000, 10 * ndof_total) like lib.rs:632 */
+    int32_t precision;     /* enum svx_precision */
+    double inner_tol;      /* mixed: inner FP32 PCG tolerance (default 1e-5) */
+    int32_t check_every;   /* iterations per graph launch between host checks (0: auto) */
+    int32_t want_stress;   /* 1: compute von Mises + reactions */
+} svx_solve_opts_t;
+
+/* Results of one static solve; arrays are caller-allocated (NULL skips). */
+typedef struct svx_solution {
+    double* u;                 /* [n_nodes * ndof] */
+    double* displacements;     /* [3 * n_nodes] like Solution::displacements */
+    double* von_mises;         /* [n_elem] centroid von Mises */
+    double* nodal_von_mises;   /* [n_nodes] */
+    double* reactions;         /* [n_fixed] K_orig u - f at constrained rows */
+    int64_t iterations;        /* PCG iterations (outer+inner total for mixed) */
+    int64_t outer_iterations;  /* mixed: defect-correction steps */
+    double final_residual;     /* recursive ||r||/||f|| (mixed: true FP64 residual) */
+    double cond_estimate;      /* max|diag| / min|diag| of the Dirichlet-modified K */
+    double ms_assemble;        /* device time of element integration + assembly */
+    double ms_solve;           /* device time of the PCG */
+    double ms_stress;          /* device time of stress + reaction recovery */
+} svx_solution_t;
+
+typedef struct svx_ctx svx_ctx_t;
+typedef struct svx_op svx_op_t;
+
+/* Library version string. */
+const char* svx_version(void);
+
+/* Default options: tol 1e-10, max_iter auto, FP64, inner_tol 1e-5. */
+void svx_default_opts(svx_solve_opts_t* opts);
+
+/* ---- context ----------------------------------------------------- */
+int svx_ctx_create(int device, svx_ctx_t** out);
+int svx_ctx_destroy(svx_ctx_t* ctx);
+/* Copies the last error message of `ctx` (or of the calling thread when
+ * ctx is NULL) into buf. */
+int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len);
+
+/* ---- a1: id / material / load resolution (host, O(N)) -------------- */
+/* Replaces Mesh::node_index (lib.rs:106-108), Model::material_for_element
+ * (lib.rs:357-367), validate (lib.rs:406-436), ndof_per_node
+ * (lib.rs:725-752), the CLOAD loop of assemble_with (assembly.rs:365-380)
+ * and constrained_dofs (solver.rs:15-41).  Errors the reference raises
+ * before assembly are returned here; errors it raises after the element
+ * loop (CLOAD, BC) are kept pending inside the resolved model and reported
+ * by svx_solve_resolved only when no element fails first. */
+int svx_resolve(const svx_model_desc_t* desc, svx_resolved_t** out, svx_error_t* err);
+/* Borrowed view of the resolved flat model (valid until svx_resolved_free). */
+const svx_flat_model_t* svx_resolved_flat(const svx_resolved_t* res);
+int svx_resolved_free(svx_resolved_t* res);
+
+/* ---- K1-K4: assembly on the device ------------------------------- */
+/* Element integration + CSR pattern + fixed-order assembly + Dirichlet.
+ * Replaces assembly::assemble (assembly.rs:281-386), constrained_dofs /
+ * apply_dirichlet (solver.rs:15-62) and the K/f clones (lib.rs:623-628). */
+int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, svx_op_t** out,
+                 svx_error_t* err);
+int svx_op_free(svx_op_t* op);
+/* CSR sizes of an assembled operator. */
+int svx_op_dims(const svx_op_t* op, int64_t* n_rows, int64_t* nnz);
+/* Copies the assembled CSR (before Dirichlet) to host arrays of n+1 / nnz /
+ * nnz entries (any may be NULL). */
+int svx_op_get_csr(const svx_op_t* op, int64_t* row_ptr, int32_t* col_idx, double* vals);
+/* y = K x with the unmodified K (x, y host arrays of n_rows). */
+int svx_op_spmv(svx_op_t* op, const double* x, double* y);
+
+/* ---- K5-K7: PCG --------------------------------------------------- */
+/* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644). */
+int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol,
+                 svx_error_t* err);
+
+/* ---- K9-K10: stress + reactions ----------------------------------- */
+/* Uses the operator's last solution (svx_op_solve).  Replaces
+ * stress::{von_mises_at_centroids, nodal_von_mises, reactions}
+ * (stress.rs:22-118) and the displacement packaging of lib.rs:689-698. */
+int svx_op_stress(svx_op_t* op, svx_solution_t* sol);
+
+/* ---- one-call pipelines -------------------------------------------- */
+/* Whole linear-static path for a flat model: lib.rs:614-703. */
+int svx_solve_flat(svx_ctx_t* ctx, const svx_flat_model_t* model,
+                   const svx_solve_opts_t* opts, svx_solution_t* sol, svx_error_t* err);
+/* Same, for a resolved reference-shaped model (reports pending CLOAD / BC
+ * errors in the reference's order). */
+int svx_solve_resolved(svx_ctx_t* ctx, const svx_resolved_t* res,
+                       const svx_solve_opts_t* opts, svx_solution_t* sol, svx_error_t* err);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLVIX_GPU_H */

@@ -1,0 +1,350 @@
+"""CPU oracle bindings (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/libsvx_oracle.so`` (the C++ restatement of the reference's
+element / assembly / solver / stress arithmetic) and restates the reference's
+host-side model handling in plain Python:
+
+* ``Model::load_state``            crates/solvix-core/src/lib.rs:388-403
+* ``solve_with_thermal`` checks    lib.rs:596-612 (NoConstraints, validate, thickness)
+* ``Model::validate``              lib.rs:406-436
+* ``ndof_per_node``                lib.rs:725-752
+* ``Mesh::node_index``             lib.rs:106-108 (first node with the id)
+* ``Model::material_for_element``  lib.rs:357-367
+* CLOAD loop of ``assemble_with``  crates/solvix-core/src/assembly.rs:365-380
+* ``constrained_dofs``             crates/solvix-core/src/solver.rs:15-41
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from solvix_b200 import abi  # noqa: E402  (struct layouts only)
+from solvix_b200.marshal import FlatModel  # noqa: E402
+from solvix_b200.model import (ElemKind, InvalidModel, Model, NoConstraints,  # noqa: E402
+                               NotConverged, SolveError)
+
+LIB_PATH = os.path.join(HERE, "libsvx_oracle.so")
+
+
+class OracleCsr(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("nnz", C.c_int64),
+        ("row_ptr", abi.c_int64_p),
+        ("col_idx", abi.c_int64_p),
+        ("vals", abi.c_double_p),
+        ("f", abi.c_double_p),
+    ]
+
+
+_SIG = {
+    "svx_oracle_set_sort_mode": (None, [C.c_int]),
+    "svx_oracle_element_stiffness": (C.c_int, [C.c_int, abi.c_double_p, C.c_double, C.c_double,
+                                               C.c_double, abi.c_double_p]),
+    "svx_oracle_assemble": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_int,
+                                      C.POINTER(OracleCsr), C.POINTER(abi.SvxError)]),
+    "svx_oracle_csr_free": (None, [C.POINTER(OracleCsr)]),
+    "svx_oracle_spmv": (None, [C.POINTER(OracleCsr), abi.c_double_p, abi.c_double_p, C.c_int]),
+    "svx_oracle_apply_dirichlet": (None, [C.POINTER(OracleCsr), abi.c_double_p, abi.c_int64_p,
+                                          C.c_int64]),
+    "svx_oracle_pcg": (C.c_int, [C.POINTER(OracleCsr), abi.c_double_p, C.c_double, C.c_int64,
+                                 C.c_int, abi.c_double_p, abi.c_int64_p, abi.c_double_p]),
+    "svx_oracle_solve": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_int, C.c_double, C.c_int64,
+                                   C.POINTER(abi.SvxSolution), C.POINTER(abi.SvxError)]),
+}
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile libsvx_oracle.so with the Makefile beside this file."""
+    src = os.path.join(HERE, "svx_oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or \
+            os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE, "libsvx_oracle.so"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = abi.bind(C.CDLL(LIB_PATH), _SIG)
+    return _lib
+
+
+def set_sort_mode(mode: int) -> None:
+    """0: the reference's unstable row sort (default); 1: stable, the
+    triplet-stream order the CUDA assembly sums in."""
+    lib().svx_oracle_set_sort_mode(int(mode))
+
+
+def default_threads() -> int:
+    """min(8, cores), the reference's worker_threads (assembly.rs:17-21)."""
+    return max(1, min(8, os.cpu_count() or 1))
+
+
+# ----------------------------------------------------------------- host logic
+class Pending:
+    """An error the reference raises after the element loop (CLOAD, BC)."""
+
+    def __init__(self, err: SolveError):
+        self.err = err
+
+
+def ndof_per_node(kinds) -> int:
+    """lib.rs:725-752."""
+    ks = set(int(k) for k in np.unique(np.asarray(kinds)))
+    plane = bool(ks & {0, 1, 2, 3, 4})
+    solid = bool(ks & {5, 6})
+    beam = 7 in ks
+    if beam and (plane or solid):
+        raise InvalidModel("mixed beam and continuum elements (v1: B31-only models)")
+    if beam:
+        return 3
+    if plane and solid:
+        raise InvalidModel("mixed dimensionality")
+    return 3 if solid else 2
+
+
+def resolve(model: Model):
+    """Reference-shaped model -> (FlatModel, pending error or None).
+
+    Raises the SolveError the reference raises before assembly.
+    """
+    bcs, cloads, _dl, _g = model.load_state()
+    mesh = model.mesh
+    if len(bcs) == 0:
+        raise NoConstraints("no constraints")
+    # validate (lib.rs:406-436), mapped to InvalidModel("{:?}")
+    if mesh.n_nodes == 0 or mesh.n_elements == 0:
+        raise InvalidModel("EmptyMesh")
+    if len(model.materials) == 0:
+        raise InvalidModel("NoMaterial")
+    first_index = {}
+    for i, nid in enumerate(mesh.node_ids.tolist()):
+        first_index.setdefault(nid, i)
+    kinds = mesh.elem_kinds
+    conn_ids = mesh.conn.tolist()
+    for e in range(mesh.n_elements):
+        a, b = int(mesh.conn_ptr[e]), int(mesh.conn_ptr[e + 1])
+        if b - a != ElemKind(int(kinds[e])).node_count():
+            raise InvalidModel(f"MalformedElement({int(mesh.elem_ids[e])})")
+        for nid in conn_ids[a:b]:
+            if nid not in first_index:
+                raise InvalidModel(f"UnknownNode({nid})")
+    t = float(model.thickness)
+    if t <= 0.0 or t != t:
+        raise InvalidModel("thickness must be positive")
+    ndof = ndof_per_node(kinds)
+    conn = np.array([first_index[nid] for nid in conn_ids], dtype=np.int32)
+    # material_for_element (lib.rs:357-367)
+    set_by_name = {}
+    for s in model.elsets:
+        set_by_name.setdefault(s.name, s)
+    mat_by_name = {}
+    for m in model.materials:
+        mat_by_name.setdefault(m.name, m)
+    decided = {}
+    for set_name, mat_name in model.mat_assignments:
+        s = set_by_name.get(set_name)
+        if s is None:
+            continue
+        for eid in np.asarray(s.element_ids).tolist():
+            if eid not in decided:
+                decided[eid] = mat_by_name.get(mat_name)
+    n_elem = mesh.n_elements
+    E = np.zeros(n_elem)
+    nu = np.zeros(n_elem)
+    nomat = np.zeros(n_elem, dtype=np.uint8)
+    for e, eid in enumerate(mesh.elem_ids.tolist()):
+        m = decided.get(eid)
+        if m is None:
+            nomat[e] = 1
+        else:
+            E[e] = m.youngs_modulus
+            nu[e] = m.poisson_ratio
+    n = mesh.n_nodes * ndof
+    f = np.zeros(n)
+    pending = None
+    # CLOAD loop (assembly.rs:365-380)
+    for cl in cloads:
+        if cl.dof == 0 or cl.dof > ndof:
+            pending = Pending(InvalidModel(
+                f"load on node {cl.node_id} has unsupported dof {cl.dof}"))
+            break
+        idx = first_index.get(int(cl.node_id))
+        if idx is None:
+            pending = Pending(InvalidModel(f"load on unknown node {cl.node_id}"))
+            break
+        f[idx * ndof + cl.dof - 1] += cl.value
+    rows = []
+    if pending is None:
+        # constrained_dofs (solver.rs:15-41)
+        for bc in bcs:
+            for nid in bc.node_ids:
+                idx = first_index.get(int(nid))
+                if idx is None:
+                    pending = Pending(InvalidModel(
+                        f"boundary condition on unknown node {nid}"))
+                    break
+                for dof in bc.dofs:
+                    if dof == 0 or dof > ndof:
+                        pending = Pending(InvalidModel(
+                            f"boundary condition on node {nid} has unsupported dof {dof}"))
+                        break
+                    rows.append(idx * ndof + dof - 1)
+                if pending:
+                    break
+            if pending:
+                break
+    flat = FlatModel(xyz=mesh.coords, kind=kinds, conn_ptr=mesh.conn_ptr, conn=conn,
+                     youngs=E, poisson=nu, thickness=t, ndof=ndof,
+                     fixed_row=np.array(rows, dtype=np.int64), f=f,
+                     node_id=mesh.node_ids, elem_id=mesh.elem_ids, no_material=nomat)
+    return flat, pending
+
+
+# ----------------------------------------------------------------- numerics
+def element_stiffness(kind: int, coords, E: float, nu: float, t: float = 1.0):
+    coords = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1, 3))
+    N = {0: 6, 1: 8, 5: 24}[int(kind)]
+    ke = np.zeros((N, N))
+    r = lib().svx_oracle_element_stiffness(int(kind), abi.ptr(coords, C.c_double), E, nu, t,
+                                           abi.ptr(ke, C.c_double))
+    return r, ke
+
+
+class Csr:
+    """Host CSR copied out of the oracle."""
+
+    def __init__(self, c: OracleCsr):
+        n, nnz = int(c.n), int(c.nnz)
+        self.n, self.nnz = n, nnz
+        self.row_ptr = np.ctypeslib.as_array(c.row_ptr, shape=(n + 1,)).copy()
+        self.col_idx = np.ctypeslib.as_array(c.col_idx, shape=(nnz,)).copy() if nnz else \
+            np.zeros(0, np.int64)
+        self.vals = np.ctypeslib.as_array(c.vals, shape=(nnz,)).copy() if nnz else np.zeros(0)
+        self.f = np.ctypeslib.as_array(c.f, shape=(n,)).copy() if n else np.zeros(0)
+
+    def struct(self):
+        s = OracleCsr()
+        s.n, s.nnz = self.n, self.nnz
+        s.row_ptr = abi.ptr(self.row_ptr, C.c_int64)
+        s.col_idx = abi.ptr(self.col_idx, C.c_int64)
+        s.vals = abi.ptr(self.vals, C.c_double)
+        s.f = abi.ptr(self.f, C.c_double)
+        return s
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.vals, self.col_idx, self.row_ptr), shape=(self.n, self.n))
+
+
+def _raise_err(err: abi.SvxError):
+    code = err.code
+    msg = err.message.decode()
+    if code == abi.SVX_INVALID_MODEL:
+        raise InvalidModel(msg, reason=err.reason, elem_index=err.elem_index)
+    if code == abi.SVX_NOT_CONVERGED:
+        raise NotConverged(int(err.iterations), float(err.residual))
+    raise SolveError(msg)
+
+
+def assemble(flat: FlatModel, threads: int | None = None) -> Csr:
+    s = flat.as_struct()
+    out = OracleCsr()
+    err = abi.SvxError()
+    st = lib().svx_oracle_assemble(C.byref(s), threads or default_threads(), C.byref(out),
+                                   C.byref(err))
+    if st != abi.SVX_OK:
+        _raise_err(err)
+    try:
+        return Csr(out)
+    finally:
+        lib().svx_oracle_csr_free(C.byref(out))
+
+
+def spmv(k: Csr, x, threads: int | None = None):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(k.n)
+    s = k.struct()
+    lib().svx_oracle_spmv(C.byref(s), abi.ptr(x, C.c_double), abi.ptr(y, C.c_double),
+                          threads or default_threads())
+    return y
+
+
+def apply_dirichlet(k: Csr, f, rows):
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    s = k.struct()
+    lib().svx_oracle_apply_dirichlet(C.byref(s), abi.ptr(f, C.c_double),
+                                     abi.ptr(rows, C.c_int64), rows.shape[0])
+
+
+def pcg(k: Csr, f, tol=1e-10, max_iter=1000, threads: int | None = None):
+    """Returns (status, u, iterations, residual)."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    u = np.zeros(k.n)
+    it = C.c_int64(0)
+    res = C.c_double(0.0)
+    s = k.struct()
+    st = lib().svx_oracle_pcg(C.byref(s), abi.ptr(f, C.c_double), tol, max_iter,
+                              threads or default_threads(), abi.ptr(u, C.c_double),
+                              C.byref(it), C.byref(res))
+    return st, u, int(it.value), float(res.value)
+
+
+class OracleSolution:
+    def __init__(self, flat: FlatModel):
+        n = flat.n_dof
+        self.u = np.zeros(n)
+        self.displacements = np.zeros((flat.n_nodes, 3))
+        self.von_mises = np.zeros(flat.n_elem)
+        self.nodal_von_mises = np.zeros(flat.n_nodes)
+        self.reaction_values = np.zeros(flat.fixed_row.shape[0])
+        self.iterations = 0
+        self.final_residual = 0.0
+        self.cond_estimate = 0.0
+
+
+def solve_flat(flat: FlatModel, tol=1e-10, max_iter=0, threads: int | None = None):
+    """Full linear-static pipeline on a flat model; raises SolveError."""
+    out = OracleSolution(flat)
+    sol = abi.SvxSolution()
+    sol.u = abi.ptr(out.u, C.c_double)
+    sol.displacements = abi.ptr(out.displacements, C.c_double)
+    sol.von_mises = abi.ptr(out.von_mises, C.c_double)
+    sol.nodal_von_mises = abi.ptr(out.nodal_von_mises, C.c_double)
+    sol.reactions = abi.ptr(out.reaction_values, C.c_double)
+    err = abi.SvxError()
+    s = flat.as_struct()
+    st = lib().svx_oracle_solve(C.byref(s), threads or default_threads(), tol, max_iter,
+                                C.byref(sol), C.byref(err))
+    if st != abi.SVX_OK:
+        _raise_err(err)
+    out.iterations = int(sol.iterations)
+    out.final_residual = float(sol.final_residual)
+    out.cond_estimate = float(sol.cond_estimate)
+    return out
+
+
+def solve(model: Model, tol=1e-10, threads: int | None = None):
+    """Reference-order solve of a reference-shaped model (Method::Pcg)."""
+    flat, pending = resolve(model)
+    if pending is not None:
+        # Element failures come first (assembly runs before the CLOAD loop).
+        assemble(flat, threads)
+        raise pending.err
+    return solve_flat(flat, tol=tol, threads=threads), flat

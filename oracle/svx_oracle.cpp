@@ -1,0 +1,989 @@
+// svx_oracle.cpp - CPU oracle (test infrastructure) for the Solvix
+// linear-static path.  A C++ restatement of the reference's Rust code; every
+// function cites the file:line it follows.  Build with -O2 -ffp-contract=off
+// (Rust never fuses a*b+c) and without -ffast-math, so that each expression
+// rounds exactly like the reference's.
+//
+// csr_from_triplets (assembly.rs:87-116) sums duplicate (row, col) triplets
+// in the order `sort_unstable_by_key` leaves them.  The oracle restates that
+// sort (the row-sort section below), so its K, and with it the whole PCG
+// trajectory, is bit-identical to the reference's: every published iteration
+// count and residual of the reference's decks is reproduced.  A stable mode
+// (triplet-stream order) is kept for bit-exact comparison with the CUDA
+// assembly, which sums in ascending element order.
+//
+// Only the serial sums and the threaded row-chunked SpMV of the reference are
+// restated; the threaded element loop writes each element's triplets at a
+// fixed offset, which equals the reference's chunk-ordered merge
+// (assembly.rs:306-363).
+
+#include "svx_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using std::size_t;
+
+// ---------------------------------------------------------------- D matrices
+// element.rs:10-17
+void d_matrix(double e, double nu, double d[3][3]) {
+    double c = e / (1.0 - nu * nu);
+    d[0][0] = c;
+    d[0][1] = nu * c;
+    d[0][2] = 0.0;
+    d[1][0] = nu * c;
+    d[1][1] = c;
+    d[1][2] = 0.0;
+    d[2][0] = 0.0;
+    d[2][1] = 0.0;
+    d[2][2] = c * (1.0 - nu) / 2.0;
+}
+
+// element.rs:33-47
+void d3_matrix(double e, double nu, double d[6][6]) {
+    double lam = e * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    double mu = e / (2.0 * (1.0 + nu));
+    double diag = lam + 2.0 * mu;
+    for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c) d[r][c] = 0.0;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) d[r][c] = (r == c) ? diag : lam;
+    d[3][3] = mu;
+    d[4][4] = mu;
+    d[5][5] = mu;
+}
+
+// ---------------------------------------------------------------- btdb
+// element.rs:830-851: DB = D*B first, then for a <= c the w-scaled
+// B^T*DB entry is added to ke[a][c] and mirrored to ke[c][a].
+template <int N, int S>
+void btdb(double* ke, const double b[S][N], const double d[S][S], double w) {
+    double db[S][N];
+    for (int r = 0; r < S; ++r)
+        for (int c = 0; c < N; ++c) {
+            double s = 0.0;
+            for (int k = 0; k < S; ++k) s += d[r][k] * b[k][c];
+            db[r][c] = s;
+        }
+    for (int a = 0; a < N; ++a)
+        for (int c = a; c < N; ++c) {
+            double s = 0.0;
+            for (int r = 0; r < S; ++r) s += b[r][a] * db[r][c];
+            double v = w * s;
+            ke[a * N + c] += v;
+            if (a != c) ke[c * N + a] += v;
+        }
+}
+
+// ---------------------------------------------------------------- CPS3
+// element.rs:91-116; returns false for a zero signed area.
+bool cps3_b_matrix(const double xy[3][2], double bm[3][6], double* two_a_out) {
+    double b[3] = {xy[1][1] - xy[2][1], xy[2][1] - xy[0][1], xy[0][1] - xy[1][1]};
+    double c[3] = {xy[2][0] - xy[1][0], xy[0][0] - xy[2][0], xy[1][0] - xy[0][0]};
+    double two_a = b[0] * c[1] - b[1] * c[0];
+    if (two_a == 0.0) return false;
+    double inv = 1.0 / two_a;
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 6; ++k) bm[r][k] = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        bm[0][2 * i] = b[i] * inv;
+        bm[1][2 * i + 1] = c[i] * inv;
+        bm[2][2 * i] = c[i] * inv;
+        bm[2][2 * i + 1] = b[i] * inv;
+    }
+    *two_a_out = two_a;
+    return true;
+}
+
+// ---------------------------------------------------------------- CPS4
+const double QUAD_CORNERS[4][2] = {{-1.0, -1.0}, {1.0, -1.0}, {1.0, 1.0}, {-1.0, 1.0}};
+
+// element.rs:134-144
+void quad_shape_derivs(double xi, double eta, double dxi[4], double deta[4]) {
+    for (int i = 0; i < 4; ++i) {
+        double xi_i = QUAD_CORNERS[i][0], eta_i = QUAD_CORNERS[i][1];
+        dxi[i] = 0.25 * xi_i * (1.0 + eta * eta_i);
+        deta[i] = 0.25 * eta_i * (1.0 + xi * xi_i);
+    }
+}
+
+// element.rs:147-171; false when det(J) <= 0 (a NaN determinant passes).
+bool quad_b(const double xy[4][2], double xi, double eta, double bm[3][8], double* detj_out) {
+    double dxi[4], deta[4];
+    quad_shape_derivs(xi, eta, dxi, deta);
+    double j00 = 0.0, j01 = 0.0, j10 = 0.0, j11 = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        j00 += dxi[i] * xy[i][0];
+        j01 += dxi[i] * xy[i][1];
+        j10 += deta[i] * xy[i][0];
+        j11 += deta[i] * xy[i][1];
+    }
+    double detj = j00 * j11 - j01 * j10;
+    if (detj <= 0.0) return false;
+    double inv = 1.0 / detj;
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 8; ++k) bm[r][k] = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        double dnx = inv * (j11 * dxi[i] - j01 * deta[i]);
+        double dny = inv * (j00 * deta[i] - j10 * dxi[i]);
+        bm[0][2 * i] = dnx;
+        bm[1][2 * i + 1] = dny;
+        bm[2][2 * i] = dny;
+        bm[2][2 * i + 1] = dnx;
+    }
+    *detj_out = detj;
+    return true;
+}
+
+// ---------------------------------------------------------------- C3D8
+const double HEX_CORNERS[8][3] = {{-1.0, -1.0, -1.0}, {1.0, -1.0, -1.0}, {1.0, 1.0, -1.0},
+                                  {-1.0, 1.0, -1.0},  {-1.0, -1.0, 1.0}, {1.0, -1.0, 1.0},
+                                  {1.0, 1.0, 1.0},    {-1.0, 1.0, 1.0}};
+
+// element.rs:441-445
+double det3(const double m[3][3]) {
+    return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+           m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+}
+
+// element.rs:448-463: transposed cofactors times 1/det.
+void inv3(const double m[3][3], double det, double out[3][3]) {
+    double id = 1.0 / det;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            int r = j, c = i;  // cof(j, i)
+            int a = (r + 1) % 3, b = (r + 2) % 3;
+            int d = (c + 1) % 3, e = (c + 2) % 3;
+            double sign = ((r + c) % 2 == 0) ? 1.0 : -1.0;
+            double cof = sign * (m[a][d] * m[b][e] - m[a][e] * m[b][d]);
+            out[i][j] = cof * id;
+        }
+}
+
+// element.rs:467-475
+void hex_shape_derivs(double xi, double eta, double zeta, double dn[3][8]) {
+    for (int i = 0; i < 8; ++i) {
+        double a = HEX_CORNERS[i][0], b = HEX_CORNERS[i][1], c = HEX_CORNERS[i][2];
+        dn[0][i] = 0.125 * a * (1.0 + eta * b) * (1.0 + zeta * c);
+        dn[1][i] = 0.125 * b * (1.0 + xi * a) * (1.0 + zeta * c);
+        dn[2][i] = 0.125 * c * (1.0 + xi * a) * (1.0 + eta * b);
+    }
+}
+
+// element.rs:479-521
+bool hex_b(const double xyz[8][3], double xi, double eta, double zeta, double bm[6][24],
+           double* detj_out) {
+    double dn[3][8];
+    hex_shape_derivs(xi, eta, zeta, dn);
+    double j[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    for (int i = 0; i < 8; ++i)
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) j[a][b] += dn[a][i] * xyz[i][b];
+    double detj = det3(j);
+    if (detj <= 0.0) return false;
+    double inv[3][3];
+    inv3(j, detj, inv);
+    for (int r = 0; r < 6; ++r)
+        for (int k = 0; k < 24; ++k) bm[r][k] = 0.0;
+    for (int i = 0; i < 8; ++i) {
+        double dnv[3] = {dn[0][i], dn[1][i], dn[2][i]};
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) g[b] += inv[b][a] * dnv[a];
+        int c = 3 * i;
+        bm[0][c] = g[0];
+        bm[1][c + 1] = g[1];
+        bm[2][c + 2] = g[2];
+        bm[3][c] = g[1];
+        bm[3][c + 1] = g[0];
+        bm[4][c + 1] = g[2];
+        bm[4][c + 2] = g[1];
+        bm[5][c] = g[2];
+        bm[5][c + 2] = g[0];
+    }
+    *detj_out = detj;
+    return true;
+}
+
+int node_count(int kind) {
+    switch (kind) {
+        case SVX_CPS3: return 3;
+        case SVX_CPS4: return 4;
+        case SVX_C3D8: return 8;
+        default: return 0;
+    }
+}
+
+// Element stiffness for the three kinds on the path.  Returns 0 or the
+// svx_elem_reason.  Follows cps3_stiffness (element.rs:121-129),
+// cps4_stiffness (:186-211; xi outer, eta inner, unit weights, w = t*detJ)
+// and c3d8_stiffness (:535-561; xi, eta, zeta loops, w = detJ).
+int element_ke(int kind, const double* coords, double e, double nu, double t, double* ke) {
+    const double g = 1.0 / std::sqrt(3.0);
+    if (kind == SVX_CPS3) {
+        double d[3][3];
+        d_matrix(e, nu, d);
+        double xy[3][2];
+        for (int i = 0; i < 3; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        double bm[3][6], two_a;
+        if (!cps3_b_matrix(xy, bm, &two_a)) return SVX_REASON_DEGENERATE_TRI;
+        std::memset(ke, 0, sizeof(double) * 36);
+        btdb<6, 3>(ke, bm, d, t * std::fabs(two_a) / 2.0);
+        return 0;
+    }
+    if (kind == SVX_CPS4) {
+        double d[3][3];
+        d_matrix(e, nu, d);
+        double xy[4][2];
+        for (int i = 0; i < 4; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        std::memset(ke, 0, sizeof(double) * 64);
+        const double pts[2] = {-g, g};
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                double bm[3][8], detj;
+                if (!quad_b(xy, pts[a], pts[b], bm, &detj)) return SVX_REASON_BAD_JACOBIAN;
+                btdb<8, 3>(ke, bm, d, t * detj);
+            }
+        double bc[3][8], dj;
+        if (!quad_b(xy, 0.0, 0.0, bc, &dj)) return SVX_REASON_BAD_JACOBIAN;
+        return 0;
+    }
+    if (kind == SVX_C3D8) {
+        double d[6][6];
+        d3_matrix(e, nu, d);
+        double xyz[8][3];
+        for (int i = 0; i < 8; ++i)
+            for (int k = 0; k < 3; ++k) xyz[i][k] = coords[3 * i + k];
+        std::memset(ke, 0, sizeof(double) * 576);
+        const double pts[2] = {-g, g};
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 2; ++c) {
+                    double bm[6][24], detj;
+                    if (!hex_b(xyz, pts[a], pts[b], pts[c], bm, &detj))
+                        return SVX_REASON_BAD_JACOBIAN;
+                    btdb<24, 6>(ke, bm, d, detj);
+                }
+        double bc[6][24], dj;
+        if (!hex_b(xyz, 0.0, 0.0, 0.0, bc, &dj)) return SVX_REASON_BAD_JACOBIAN;
+        return 0;
+    }
+    return SVX_REASON_UNSUPPORTED_KIND;
+}
+
+// ---------------------------------------------------------------- stress
+// element.rs:854-863
+template <int N, int S>
+void strain(const double b[S][N], const double* ue, double* e) {
+    for (int r = 0; r < S; ++r) {
+        double s = 0.0;
+        for (int c = 0; c < N; ++c) s += b[r][c] * ue[c];
+        e[r] = s;
+    }
+}
+
+// element.rs:867-881
+template <int N>
+void plane_stress(const double b[3][N], const double d[3][3], const double* ue, double s[6]) {
+    double e[3];
+    strain<N, 3>(b, ue, e);
+    s[0] = d[0][0] * e[0] + d[0][1] * e[1];
+    s[1] = d[1][0] * e[0] + d[1][1] * e[1];
+    s[2] = 0.0;
+    s[3] = d[2][2] * e[2];
+    s[4] = 0.0;
+    s[5] = 0.0;
+}
+
+// element.rs:904-915
+template <int N>
+void solid_stress(const double b[6][N], const double d[6][6], const double* ue, double s[6]) {
+    double e[6];
+    strain<N, 6>(b, ue, e);
+    for (int r = 0; r < 6; ++r) {
+        double acc = 0.0;
+        for (int k = 0; k < 6; ++k) acc += d[r][k] * e[k];
+        s[r] = acc;
+    }
+}
+
+// element.rs:917-923
+double von_mises(const double s[6]) {
+    return std::sqrt(0.5 * ((s[0] - s[1]) * (s[0] - s[1]) + (s[1] - s[2]) * (s[1] - s[2]) +
+                            (s[2] - s[0]) * (s[2] - s[0])) +
+                     3.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5]));
+}
+
+const double GP_SIGNS[4][2] = {{-1.0, -1.0}, {-1.0, 1.0}, {1.0, -1.0}, {1.0, 1.0}};
+const double GP3_SIGNS[8][3] = {{-1.0, -1.0, -1.0}, {-1.0, -1.0, 1.0}, {-1.0, 1.0, -1.0},
+                                {-1.0, 1.0, 1.0},   {1.0, -1.0, -1.0}, {1.0, -1.0, 1.0},
+                                {1.0, 1.0, -1.0},   {1.0, 1.0, 1.0}};
+
+double hfun(double s) { return 0.5 * (1.0 + s * std::sqrt(3.0)); }
+
+// Centroid stress and the nodal (extrapolated) stresses of one element:
+// centroid_stress (element.rs:926-943), nodal_stresses (:948-994),
+// extrapolate_to_corners (:1005-1018) and extrapolate_to_corners3
+// (:1040-1053).  nodal has room for 8 x 6 values.
+void element_stresses(int kind, const double* coords, double e, double nu, double t,
+                      const double* ue, double centroid[6], double nodal[8][6]) {
+    (void)t;
+    const double g = 1.0 / std::sqrt(3.0);
+    if (kind == SVX_CPS3) {
+        double d[3][3];
+        d_matrix(e, nu, d);
+        double xy[3][2];
+        for (int i = 0; i < 3; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        double bm[3][6], two_a;
+        cps3_b_matrix(xy, bm, &two_a);
+        plane_stress<6>(bm, d, ue, centroid);
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 6; ++k) nodal[i][k] = centroid[k];
+        return;
+    }
+    if (kind == SVX_CPS4) {
+        double d[3][3];
+        d_matrix(e, nu, d);
+        double xy[4][2];
+        for (int i = 0; i < 4; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        double bc[3][8], dj;
+        quad_b(xy, 0.0, 0.0, bc, &dj);
+        plane_stress<8>(bc, d, ue, centroid);
+        double gp[4][6];
+        const double pts[2] = {-g, g};
+        int k = 0;
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                double bm[3][8];
+                quad_b(xy, pts[a], pts[b], bm, &dj);
+                plane_stress<8>(bm, d, ue, gp[k]);
+                ++k;
+            }
+        for (int i = 0; i < 4; ++i) {
+            for (int m = 0; m < 6; ++m) nodal[i][m] = 0.0;
+            for (int j = 0; j < 4; ++j) {
+                double w = hfun(QUAD_CORNERS[i][0] * GP_SIGNS[j][0]) *
+                           hfun(QUAD_CORNERS[i][1] * GP_SIGNS[j][1]);
+                for (int m = 0; m < 6; ++m) nodal[i][m] += w * gp[j][m];
+            }
+        }
+        return;
+    }
+    // C3D8
+    double d[6][6];
+    d3_matrix(e, nu, d);
+    double xyz[8][3];
+    for (int i = 0; i < 8; ++i)
+        for (int k = 0; k < 3; ++k) xyz[i][k] = coords[3 * i + k];
+    double bc[6][24], dj;
+    hex_b(xyz, 0.0, 0.0, 0.0, bc, &dj);
+    solid_stress<24>(bc, d, ue, centroid);
+    double gp[8][6];
+    const double pts[2] = {-g, g};
+    int k = 0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) {
+                double bm[6][24];
+                hex_b(xyz, pts[a], pts[b], pts[c], bm, &dj);
+                solid_stress<24>(bm, d, ue, gp[k]);
+                ++k;
+            }
+    for (int i = 0; i < 8; ++i) {
+        for (int m = 0; m < 6; ++m) nodal[i][m] = 0.0;
+        for (int j = 0; j < 8; ++j) {
+            double w = hfun(HEX_CORNERS[i][0] * GP3_SIGNS[j][0]) *
+                       hfun(HEX_CORNERS[i][1] * GP3_SIGNS[j][1]) *
+                       hfun(HEX_CORNERS[i][2] * GP3_SIGNS[j][2]);
+            for (int m = 0; m < 6; ++m) nodal[i][m] += w * gp[j][m];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- row sort
+// csr_from_triplets sorts each row with `sort_unstable_by_key(|&(c, _)| c)`
+// (assembly.rs:97), so the order in which duplicate (row, col) triplets are
+// summed is whatever the Rust standard library's unstable sort leaves.  To
+// reproduce the reference's K bit for bit, the oracle restates that
+// published algorithm (Rust >= 1.81 `slice::sort_unstable`: insertion sort
+// up to 20 elements, otherwise ipnsort = existing-run detection + quicksort
+// with median-of-3 / recursive pseudo-median pivots, branchless cyclic
+// Lomuto partitions, a stable small-sort below 33 elements and a heapsort
+// fallback), specialised for 16-byte (usize, f64) items keyed by column.
+struct Trip {
+    int64_t c;
+    double v;
+};
+
+inline bool trip_less(const Trip& a, const Trip& b) { return a.c < b.c; }
+
+// Stable insertion of v[1..n) (insertion_sort_shift_left with offset 1).
+void rs_insertion_sort(Trip* v, int64_t n) {
+    for (int64_t i = 1; i < n; ++i) {
+        if (!trip_less(v[i], v[i - 1])) continue;
+        Trip tmp = v[i];
+        int64_t j = i;
+        do {
+            v[j] = v[j - 1];
+            --j;
+        } while (j > 0 && trip_less(tmp, v[j - 1]));
+        v[j] = tmp;
+    }
+}
+
+// The general small-sort (sort8/sort4 presorting, insertion, bidirectional
+// merge) is stable, so its result equals a stable sort of the slice.
+void rs_small_sort(Trip* v, int64_t n) {
+    std::stable_sort(v, v + n, trip_less);
+}
+
+const Trip* rs_median3(const Trip* a, const Trip* b, const Trip* c) {
+    bool x = trip_less(*a, *b);
+    bool y = trip_less(*a, *c);
+    if (x == y) {
+        bool z = trip_less(*b, *c);
+        return (z ^ x) ? c : b;
+    }
+    return a;
+}
+
+const Trip* rs_median3_rec(const Trip* a, const Trip* b, const Trip* c, int64_t n) {
+    if (n * 8 >= 64) {
+        int64_t n8 = n / 8;
+        a = rs_median3_rec(a, a + n8 * 4, a + n8 * 7, n8);
+        b = rs_median3_rec(b, b + n8 * 4, b + n8 * 7, n8);
+        c = rs_median3_rec(c, c + n8 * 4, c + n8 * 7, n8);
+    }
+    return rs_median3(a, b, c);
+}
+
+int64_t rs_choose_pivot(const Trip* v, int64_t len) {
+    int64_t len_div_8 = len / 8;
+    const Trip* a = v;
+    const Trip* b = v + len_div_8 * 4;
+    const Trip* c = v + len_div_8 * 7;
+    const Trip* m = (len < 64) ? rs_median3(a, b, c) : rs_median3_rec(a, b, c, len_div_8);
+    return int64_t(m - v);
+}
+
+// Branchless cyclic Lomuto partition of v[0..len) around `pivot`: elements
+// are visited in order v[1], ..., v[len-1] and finally the saved v[0].
+template <class Less>
+int64_t rs_lomuto_cyclic(Trip* v, int64_t len, const Trip& pivot, Less less) {
+    if (len == 0) return 0;
+    Trip gap_value = v[0];
+    int64_t gap = 0, num_lt = 0;
+    for (int64_t r = 1; r < len; ++r) {
+        Trip x = v[r];
+        bool lt = less(x, pivot);
+        v[gap] = v[num_lt];
+        v[num_lt] = x;
+        gap = r;
+        num_lt += lt ? 1 : 0;
+    }
+    bool lt = less(gap_value, pivot);
+    v[gap] = v[num_lt];
+    v[num_lt] = gap_value;
+    num_lt += lt ? 1 : 0;
+    return num_lt;
+}
+
+template <class Less>
+int64_t rs_partition(Trip* v, int64_t len, int64_t pivot, Less less) {
+    std::swap(v[0], v[pivot]);
+    Trip pv = v[0];
+    int64_t num_lt = rs_lomuto_cyclic(v + 1, len - 1, pv, less);
+    std::swap(v[0], v[num_lt]);
+    return num_lt;
+}
+
+void rs_sift_down(Trip* v, int64_t len, int64_t node) {
+    for (;;) {
+        int64_t child = 2 * node + 1;
+        if (child >= len) break;
+        if (child + 1 < len) child += trip_less(v[child], v[child + 1]) ? 1 : 0;
+        if (!trip_less(v[node], v[child])) break;
+        std::swap(v[node], v[child]);
+        node = child;
+    }
+}
+
+void rs_heapsort(Trip* v, int64_t len) {
+    for (int64_t i = len + len / 2 - 1; i >= 0; --i) {
+        int64_t sift_idx;
+        if (i >= len) {
+            sift_idx = i - len;
+        } else {
+            std::swap(v[0], v[i]);
+            sift_idx = 0;
+        }
+        rs_sift_down(v, std::min(i, len), sift_idx);
+    }
+}
+
+void rs_quicksort(Trip* v, int64_t len, const Trip* ancestor, uint32_t limit) {
+    for (;;) {
+        if (len <= 32) {
+            rs_small_sort(v, len);
+            return;
+        }
+        if (limit == 0) {
+            rs_heapsort(v, len);
+            return;
+        }
+        --limit;
+        int64_t pivot_pos = rs_choose_pivot(v, len);
+        if (ancestor && !trip_less(*ancestor, v[pivot_pos])) {
+            int64_t num_lt = rs_partition(v, len, pivot_pos,
+                                          [](const Trip& a, const Trip& b) { return !trip_less(b, a); });
+            v += num_lt + 1;
+            len -= num_lt + 1;
+            ancestor = nullptr;
+            continue;
+        }
+        int64_t num_lt = rs_partition(v, len, pivot_pos, trip_less);
+        rs_quicksort(v, num_lt, ancestor, limit);
+        ancestor = v + num_lt;
+        v += num_lt + 1;
+        len -= num_lt + 1;
+    }
+}
+
+void rust_sort_unstable(Trip* v, int64_t len) {
+    if (len < 2) return;
+    if (len <= 20) {
+        rs_insertion_sort(v, len);
+        return;
+    }
+    // ipnsort: an existing ascending / strictly descending run of the whole
+    // slice is kept (descending reversed).
+    int64_t run = 2;
+    bool desc = trip_less(v[1], v[0]);
+    if (desc)
+        while (run < len && trip_less(v[run], v[run - 1])) ++run;
+    else
+        while (run < len && !trip_less(v[run], v[run - 1])) ++run;
+    if (run == len) {
+        if (desc) std::reverse(v, v + len);
+        return;
+    }
+    uint32_t lg = 0;
+    for (uint64_t x = uint64_t(len) | 1; x > 1; x >>= 1) ++lg;
+    rs_quicksort(v, len, nullptr, 2 * lg);
+}
+
+// Row-sort mode: 0 = the reference's unstable sort (default), 1 = stable
+// (triplet-stream order: seed first, then elements in enumeration order).
+int g_sort_mode = 0;
+
+// ---------------------------------------------------------------- helpers
+template <class F>
+void parallel_for(int64_t n, int threads, F&& fn) {
+    if (threads <= 1 || n < 2) {
+        fn(int64_t(0), n);
+        return;
+    }
+    int64_t chunk = (n + threads - 1) / threads;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) {
+        int64_t a = t * chunk, b = std::min(n, a + chunk);
+        if (a >= b) break;
+        pool.emplace_back([&fn, a, b] { fn(a, b); });
+    }
+    for (auto& th : pool) th.join();
+}
+
+uint32_t elem_id_of(const svx_flat_model_t* m, int64_t e) {
+    return m->elem_id ? m->elem_id[e] : uint32_t(e + 1);
+}
+
+void set_error(svx_error_t* err, int code, int reason, int64_t elem, const char* msg) {
+    if (!err) return;
+    err->code = code;
+    err->reason = reason;
+    err->elem_index = elem;
+    err->iterations = 0;
+    err->residual = 0.0;
+    std::snprintf(err->message, sizeof(err->message), "%s", msg);
+}
+
+const char* reason_text(int reason) {
+    switch (reason) {
+        case SVX_REASON_NO_MATERIAL: return "no material assigned";
+        case SVX_REASON_BAD_MATERIAL: return "invalid material constants";
+        case SVX_REASON_SOLID_POISSON:
+            return "poisson ratio must be < 0.5 for solids and plane strain";
+        case SVX_REASON_DEGENERATE_TRI: return "degenerate (zero-area) triangle";
+        case SVX_REASON_BAD_JACOBIAN: return "non-positive Jacobian determinant at a Gauss point";
+        default: return "element kind outside the linear-static GPU path (CPS3, CPS4, C3D8)";
+    }
+}
+
+// element_entry's checks before geometry (assembly.rs:143-160).
+int material_check(const svx_flat_model_t* m, int64_t e) {
+    if (m->no_material && m->no_material[e]) return SVX_REASON_NO_MATERIAL;
+    double E = m->youngs[e], nu = m->poisson[e];
+    if (E <= 0.0 || std::fabs(nu) >= 1.0) return SVX_REASON_BAD_MATERIAL;
+    int kind = m->kind[e];
+    bool solid = (kind == SVX_C3D8 || kind == SVX_C3D4);
+    bool plane_strain = (kind == SVX_CPE4 || kind == SVX_CPE8);
+    if ((solid || plane_strain) && nu >= 0.5) return SVX_REASON_SOLID_POISSON;
+    if (node_count(kind) == 0) return SVX_REASON_UNSUPPORTED_KIND;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void svx_oracle_set_sort_mode(int mode) { g_sort_mode = mode; }
+
+int svx_oracle_element_stiffness(int kind, const double* coords, double E, double nu,
+                                 double thickness, double* ke) {
+    return element_ke(kind, coords, E, nu, thickness, ke);
+}
+
+// assembly.rs:291-386 with csr_from_triplets (:87-116) and scatter (:120-133).
+int svx_oracle_assemble(const svx_flat_model_t* m, int threads, svx_oracle_csr_t* out,
+                        svx_error_t* err) {
+    std::memset(out, 0, sizeof(*out));
+    const int ndof = m->ndof;
+    const int64_t n = m->n_nodes * ndof;
+    const int64_t ne = m->n_elem;
+    // Triplet stream: n diagonal seeds, then each element's N*N entries.
+    std::vector<int64_t> toff(ne + 1, 0);
+    for (int64_t e = 0; e < ne; ++e) {
+        int64_t nn = m->conn_ptr[e + 1] - m->conn_ptr[e];
+        int64_t N = nn * ndof;
+        toff[e + 1] = toff[e] + N * N;
+    }
+    const int64_t nt = n + toff[ne];
+    std::vector<int64_t> tr(nt), tc(nt);
+    std::vector<double> tv(nt);
+    for (int64_t i = 0; i < n; ++i) {
+        tr[i] = i;
+        tc[i] = i;
+        tv[i] = 0.0;
+    }
+    std::vector<int> fail(ne, 0);
+    auto run = [&](int64_t a, int64_t b) {
+        double ke[576];
+        double coords[24];
+        for (int64_t e = a; e < b; ++e) {
+            int r = material_check(m, e);
+            if (r) {
+                fail[e] = r;
+                continue;
+            }
+            int kind = m->kind[e];
+            int nn = node_count(kind);
+            const int32_t* cn = m->conn + m->conn_ptr[e];
+            for (int i = 0; i < nn; ++i)
+                for (int k = 0; k < 3; ++k) coords[3 * i + k] = m->xyz[3 * int64_t(cn[i]) + k];
+            r = element_ke(kind, coords, m->youngs[e], m->poisson[e], m->thickness, ke);
+            if (r) {
+                fail[e] = r;
+                continue;
+            }
+            const int N = nn * ndof;
+            int64_t o = n + toff[e];
+            for (int aa = 0; aa < N; ++aa) {
+                int64_t gr = int64_t(cn[aa / ndof]) * ndof + aa % ndof;
+                for (int cc = 0; cc < N; ++cc) {
+                    int64_t gc = int64_t(cn[cc / ndof]) * ndof + cc % ndof;
+                    tr[o] = gr;
+                    tc[o] = gc;
+                    tv[o] = ke[aa * N + cc];
+                    ++o;
+                }
+            }
+        }
+    };
+    int n_chunks = (threads > 1 && ne >= 256) ? 2 * threads : 1;
+    if (n_chunks == 1)
+        run(0, ne);
+    else
+        parallel_for(ne, threads, run);
+    for (int64_t e = 0; e < ne; ++e)
+        if (fail[e]) {
+            char msg[400];
+            std::snprintf(msg, sizeof msg, "element %u: %s", elem_id_of(m, e),
+                          reason_text(fail[e]));
+            set_error(err, SVX_INVALID_MODEL, fail[e], e, msg);
+            return SVX_INVALID_MODEL;
+        }
+    // csr_from_triplets: bucket by row in stream order, stable-sort each row
+    // by column, sum runs left to right starting from 0.0.
+    std::vector<int64_t> rcount(n + 1, 0);
+    for (int64_t t = 0; t < nt; ++t) rcount[tr[t] + 1]++;
+    for (int64_t i = 0; i < n; ++i) rcount[i + 1] += rcount[i];
+    std::vector<int64_t> pos(rcount.begin(), rcount.end() - 1);
+    std::vector<int64_t> perm(nt);
+    for (int64_t t = 0; t < nt; ++t) perm[pos[tr[t]]++] = t;
+    std::vector<int64_t> rp(n + 1, 0);
+    std::vector<int64_t> ci;
+    std::vector<double> cv;
+    ci.reserve(nt / 2 + n);
+    cv.reserve(nt / 2 + n);
+    std::vector<Trip> row;
+    for (int64_t i = 0; i < n; ++i) {
+        row.clear();
+        for (int64_t q = rcount[i]; q < rcount[i + 1]; ++q) {
+            int64_t t = perm[q];
+            row.push_back(Trip{tc[t], tv[t]});
+        }
+        if (g_sort_mode == 0)
+            rust_sort_unstable(row.data(), int64_t(row.size()));
+        else
+            std::stable_sort(row.begin(), row.end(), trip_less);
+        size_t k = 0;
+        while (k < row.size()) {
+            int64_t c = row[k].c;
+            double v = 0.0;
+            while (k < row.size() && row[k].c == c) {
+                v += row[k].v;
+                ++k;
+            }
+            ci.push_back(c);
+            cv.push_back(v);
+        }
+        rp[i + 1] = int64_t(ci.size());
+    }
+    out->n = n;
+    out->nnz = int64_t(ci.size());
+    out->row_ptr = (int64_t*)std::malloc(sizeof(int64_t) * (n + 1));
+    out->col_idx = (int64_t*)std::malloc(sizeof(int64_t) * (ci.size() + 1));
+    out->vals = (double*)std::malloc(sizeof(double) * (cv.size() + 1));
+    out->f = (double*)std::malloc(sizeof(double) * (n + 1));
+    std::memcpy(out->row_ptr, rp.data(), sizeof(int64_t) * (n + 1));
+    std::memcpy(out->col_idx, ci.data(), sizeof(int64_t) * ci.size());
+    std::memcpy(out->vals, cv.data(), sizeof(double) * cv.size());
+    for (int64_t i = 0; i < n; ++i) out->f[i] = m->f ? m->f[i] : 0.0;
+    if (err) set_error(err, SVX_OK, 0, -1, "");
+    return SVX_OK;
+}
+
+void svx_oracle_csr_free(svx_oracle_csr_t* csr) {
+    if (!csr) return;
+    std::free(csr->row_ptr);
+    std::free(csr->col_idx);
+    std::free(csr->vals);
+    std::free(csr->f);
+    std::memset(csr, 0, sizeof(*csr));
+}
+
+// assembly.rs:46-72: row-chunked when threads > 1 and n > 20,000; each row
+// keeps its serial order.
+void svx_oracle_spmv(const svx_oracle_csr_t* k, const double* x, double* y, int threads) {
+    const int64_t n = k->n;
+    auto rows = [&](int64_t a, int64_t b) {
+        for (int64_t r = a; r < b; ++r) {
+            double o = 0.0;
+            for (int64_t idx = k->row_ptr[r]; idx < k->row_ptr[r + 1]; ++idx)
+                o += k->vals[idx] * x[k->col_idx[idx]];
+            y[r] = o;
+        }
+    };
+    if (threads > 1 && n > 20000)
+        parallel_for(n, threads, rows);
+    else
+        rows(0, n);
+}
+
+// solver.rs:45-62
+void svx_oracle_apply_dirichlet(svx_oracle_csr_t* k, double* f, const int64_t* rows,
+                                int64_t n_rows) {
+    const int64_t n = k->n;
+    std::vector<char> is_c(n, 0);
+    for (int64_t i = 0; i < n_rows; ++i) is_c[rows[i]] = 1;
+    for (int64_t r = 0; r < n; ++r)
+        for (int64_t idx = k->row_ptr[r]; idx < k->row_ptr[r + 1]; ++idx) {
+            int64_t c = k->col_idx[idx];
+            if (is_c[r] || is_c[c]) k->vals[idx] = (r == c) ? 1.0 : 0.0;
+        }
+    for (int64_t i = 0; i < n_rows; ++i) f[rows[i]] = 0.0;
+}
+
+// solver.rs:82-149 (serial dots, threaded SpMV).
+int svx_oracle_pcg(const svx_oracle_csr_t* k, const double* f, double tol, int64_t max_iter,
+                   int threads, double* u, int64_t* iterations, double* residual) {
+    const int64_t n = k->n;
+    std::vector<double> r(f, f + n), z(n), p(n), kp(n), inv_diag(n);
+    for (int64_t i = 0; i < n; ++i) u[i] = 0.0;
+    auto dot = [n](const double* a, const double* b) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+        return s;
+    };
+    double b_norm = std::sqrt(dot(f, f));
+    if (b_norm == 0.0) {
+        *iterations = 0;
+        *residual = 0.0;
+        return SVX_OK;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        double d = 0.0;
+        for (int64_t idx = k->row_ptr[i]; idx < k->row_ptr[i + 1]; ++idx)
+            if (k->col_idx[idx] == i) {
+                d = k->vals[idx];
+                break;
+            }
+        inv_diag[i] = (d == 0.0) ? 0.0 : 1.0 / d;
+    }
+    auto rel_res = [&]() { return std::sqrt(dot(r.data(), r.data())) / b_norm; };
+    for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv_diag[i];
+    p = z;
+    double rz = dot(r.data(), z.data());
+    for (int64_t it = 1; it <= max_iter; ++it) {
+        svx_oracle_spmv(k, p.data(), kp.data(), threads);
+        double pap = dot(p.data(), kp.data());
+        if (pap <= 0.0 || std::isnan(pap)) {
+            *iterations = it;
+            *residual = rel_res();
+            return SVX_NOT_CONVERGED;
+        }
+        double alpha = rz / pap;
+        for (int64_t i = 0; i < n; ++i) u[i] += alpha * p[i];
+        for (int64_t i = 0; i < n; ++i) r[i] -= alpha * kp[i];
+        double res = rel_res();
+        if (res <= tol) {
+            *iterations = it;
+            *residual = res;
+            return SVX_OK;
+        }
+        for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv_diag[i];
+        double rz_new = dot(r.data(), z.data());
+        double beta = rz_new / rz;
+        rz = rz_new;
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    }
+    *iterations = max_iter;
+    *residual = rel_res();
+    return SVX_NOT_CONVERGED;
+}
+
+// lib.rs:593-716 (Method::Pcg): assemble -> keep K, f -> Dirichlet -> PCG
+// -> jacobi_cond -> displacements -> stresses -> reactions.
+int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t max_iter,
+                     svx_solution_t* sol, svx_error_t* err) {
+    svx_oracle_csr_t k;
+    int st = svx_oracle_assemble(m, threads, &k, err);
+    if (st != SVX_OK) return st;
+    const int ndof = m->ndof;
+    const int64_t n = k.n;
+    std::vector<double> f_orig(k.f, k.f + n);
+    svx_oracle_csr_t k_orig;
+    k_orig.n = k.n;
+    k_orig.nnz = k.nnz;
+    k_orig.row_ptr = k.row_ptr;
+    k_orig.col_idx = k.col_idx;
+    std::vector<double> vals_orig(k.vals, k.vals + k.nnz);
+    k_orig.vals = vals_orig.data();
+    k_orig.f = nullptr;
+    std::vector<double> f(k.f, k.f + n);
+    svx_oracle_apply_dirichlet(&k, f.data(), m->fixed_row, m->n_fixed);
+    if (max_iter <= 0) max_iter = std::max<int64_t>(1000, 10 * n);
+    std::vector<double> u(n, 0.0);
+    int64_t iters = 0;
+    double res = 0.0;
+    st = svx_oracle_pcg(&k, f.data(), tol, max_iter, threads, u.data(), &iters, &res);
+    if (st != SVX_OK) {
+        char msg[200];
+        std::snprintf(msg, sizeof msg, "not converged after %lld iterations",
+                      (long long)iters);
+        set_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
+        if (err) {
+            err->iterations = iters;
+            err->residual = res;
+        }
+        svx_oracle_csr_free(&k);
+        return st;
+    }
+    // jacobi_cond (lib.rs:634-644): extreme |diag| of the modified K.
+    double hi = 0.0, lo = INFINITY;
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t idx = k.row_ptr[i]; idx < k.row_ptr[i + 1]; ++idx)
+            if (k.col_idx[idx] == i) {
+                double a = std::fabs(k.vals[idx]);
+                hi = std::fmax(hi, a);
+                lo = std::fmin(lo, a);
+                break;
+            }
+    sol->iterations = iters;
+    sol->outer_iterations = 0;
+    sol->final_residual = res;
+    sol->cond_estimate = hi / lo;
+    if (sol->u) std::memcpy(sol->u, u.data(), sizeof(double) * n);
+    if (sol->displacements)
+        for (int64_t i = 0; i < m->n_nodes; ++i) {
+            int64_t b = i * ndof;
+            sol->displacements[3 * i] = u[b];
+            sol->displacements[3 * i + 1] = u[b + 1];
+            sol->displacements[3 * i + 2] = (ndof == 3) ? u[b + 2] : 0.0;
+        }
+    // stress.rs:22-98
+    std::vector<double> sum(6 * m->n_nodes, 0.0);
+    std::vector<uint32_t> count(m->n_nodes, 0);
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        int kind = m->kind[e];
+        int nn = node_count(kind);
+        const int32_t* cn = m->conn + m->conn_ptr[e];
+        double coords[24], ue[24], cen[6], nod[8][6];
+        for (int i = 0; i < nn; ++i) {
+            for (int q = 0; q < 3; ++q) coords[3 * i + q] = m->xyz[3 * int64_t(cn[i]) + q];
+            for (int q = 0; q < ndof; ++q) ue[i * ndof + q] = u[int64_t(cn[i]) * ndof + q];
+        }
+        element_stresses(kind, coords, m->youngs[e], m->poisson[e], m->thickness, ue, cen, nod);
+        if (sol->von_mises) sol->von_mises[e] = von_mises(cen);
+        for (int i = 0; i < nn; ++i) {
+            int64_t node = cn[i];
+            for (int q = 0; q < 6; ++q) sum[6 * node + q] += nod[i][q];
+            count[node] += 1;
+        }
+    }
+    if (sol->nodal_von_mises)
+        for (int64_t i = 0; i < m->n_nodes; ++i) {
+            if (count[i] == 0) {
+                sol->nodal_von_mises[i] = 0.0;
+                continue;
+            }
+            double c = double(count[i]);
+            double avg[6];
+            for (int q = 0; q < 6; ++q) avg[q] = sum[6 * i + q] / c;
+            sol->nodal_von_mises[i] = von_mises(avg);
+        }
+    // stress.rs:103-118
+    if (sol->reactions) {
+        std::vector<double> ku(n);
+        svx_oracle_spmv(&k_orig, u.data(), ku.data(), threads);
+        for (int64_t i = 0; i < m->n_fixed; ++i) {
+            int64_t row = m->fixed_row[i];
+            sol->reactions[i] = ku[row] - f_orig[row];
+        }
+    }
+    svx_oracle_csr_free(&k);
+    if (err) set_error(err, SVX_OK, 0, -1, "");
+    return SVX_OK;
+}
+
+}  // extern "C"

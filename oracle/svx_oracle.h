@@ -1,0 +1,71 @@
+/*
+ * svx_oracle.h - CPU oracle for the Solvix linear-static path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a C++ restatement of the reference's
+ * Rust arithmetic (crates/solvix-core/src/{element,assembly,solver,stress,
+ * lib}.rs) used as the checker for the CUDA path and as the timed CPU
+ * baseline.  Nothing in the product links it or calls it.
+ *
+ * Parity is pinned against the reference's published golden values for
+ * examples/cantilever.inp, examples/cantilever3d.inp, examples/plate_hole.inp,
+ * the bench patch deck and the cantilever refinement table (see the tests
+ * under tests/ that load tests/golden/).
+ */
+#ifndef SVX_ORACLE_H
+#define SVX_ORACLE_H
+
+#include "solvix_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct svx_oracle_csr {
+    int64_t n;
+    int64_t nnz;
+    int64_t* row_ptr; /* [n + 1] */
+    int64_t* col_idx; /* [nnz] */
+    double* vals;     /* [nnz] */
+    double* f;        /* [n] assembled load vector (copy of the model's) */
+} svx_oracle_csr_t;
+
+/* Order in which csr_from_triplets sums duplicate (row, col) triplets:
+ * 0 (default) = the reference's `sort_unstable_by_key` restated, so K is
+ * bit-identical to the reference's; 1 = stable (triplet-stream order:
+ * diagonal seed, then elements in enumeration order), the order the CUDA
+ * assembly uses. */
+void svx_oracle_set_sort_mode(int mode);
+
+/* Element stiffness of one element (row-major N x N into ke); returns 0 or
+ * the svx_elem_reason of the failure.  coords: [n_nodes][3]. */
+int svx_oracle_element_stiffness(int kind, const double* coords, double E, double nu,
+                                 double thickness, double* ke);
+
+/* assembly::assemble_with restated (assembly.rs:291-386): triplets -> CSR,
+ * duplicates summed in the order of the current sort mode. */
+int svx_oracle_assemble(const svx_flat_model_t* m, int threads, svx_oracle_csr_t* out,
+                        svx_error_t* err);
+void svx_oracle_csr_free(svx_oracle_csr_t* csr);
+
+/* Csr::mat_vec_with (assembly.rs:46-72). */
+void svx_oracle_spmv(const svx_oracle_csr_t* k, const double* x, double* y, int threads);
+
+/* solver::apply_dirichlet (solver.rs:45-62) in place on k and f. */
+void svx_oracle_apply_dirichlet(svx_oracle_csr_t* k, double* f, const int64_t* rows,
+                                int64_t n_rows);
+
+/* solver::pcg_with_threads (solver.rs:82-149).  Returns SVX_OK or
+ * SVX_NOT_CONVERGED (iterations / residual filled either way). */
+int svx_oracle_pcg(const svx_oracle_csr_t* k, const double* f, double tol, int64_t max_iter,
+                   int threads, double* u, int64_t* iterations, double* residual);
+
+/* Full linear-static pipeline (lib.rs:593-716 without the LDLT fallback;
+ * Method::Pcg).  Output arrays of `sol` are caller-allocated. */
+int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t max_iter,
+                     svx_solution_t* sol, svx_error_t* err);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
