@@ -222,16 +222,27 @@ int svx_resolved_free(svx_resolved_t* res);
 /* Element integration + CSR pattern + fixed-order assembly + Dirichlet.
  * Replaces assembly::assemble (assembly.rs:281-386), constrained_dofs /
  * apply_dirichlet (solver.rs:15-62) and the K/f clones (lib.rs:623-628). */
-int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, svx_op_t** out,
-                 svx_error_t* err);
+enum svx_assemble_flags {
+    SVX_KEEP_ORIGINAL = 1  /* keep a device copy of K before Dirichlet */
+};
+int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, uint32_t flags,
+                 svx_op_t** out, svx_error_t* err);
 int svx_op_free(svx_op_t* op);
 /* CSR sizes of an assembled operator. */
 int svx_op_dims(const svx_op_t* op, int64_t* n_rows, int64_t* nnz);
-/* Copies the assembled CSR (before Dirichlet) to host arrays of n+1 / nnz /
- * nnz entries (any may be NULL). */
-int svx_op_get_csr(const svx_op_t* op, int64_t* row_ptr, int32_t* col_idx, double* vals);
-/* y = K x with the unmodified K (x, y host arrays of n_rows). */
+/* Copies the CSR to host arrays of n+1 / nnz / nnz entries (any may be
+ * NULL).  which = 0: the PCG operator (K after Dirichlet); which = 1: the
+ * assembled K before Dirichlet (needs SVX_KEEP_ORIGINAL). */
+int svx_op_get_csr(const svx_op_t* op, int which, int64_t* row_ptr, int32_t* col_idx,
+                   double* vals);
+/* Copies the load vector (which = 0: after Dirichlet, 1: before) and the
+ * Jacobi inverse diagonal (NULL skips) to host arrays of n_rows. */
+int svx_op_get_vectors(const svx_op_t* op, int which, double* f, double* inv_diag);
+/* y = K x with the PCG operator (x, y host arrays of n_rows). */
 int svx_op_spmv(svx_op_t* op, const double* x, double* y);
+/* Installs u (host, n_rows) as the operator's solution, e.g. to recover
+ * stresses for a displacement field computed elsewhere. */
+int svx_op_set_solution(svx_op_t* op, const double* u);
 
 /* ---- K5-K7: PCG --------------------------------------------------- */
 /* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644). */

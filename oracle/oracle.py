@@ -63,6 +63,9 @@ _SIG = {
                                  C.c_int, abi.c_double_p, abi.c_int64_p, abi.c_double_p]),
     "svx_oracle_solve": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_int, C.c_double, C.c_int64,
                                    C.POINTER(abi.SvxSolution), C.POINTER(abi.SvxError)]),
+    "svx_oracle_stress": (C.c_int, [C.POINTER(abi.SvxFlatModel), abi.c_double_p, C.c_int,
+                                    abi.c_double_p, abi.c_double_p, abi.c_double_p,
+                                    C.POINTER(abi.SvxError)]),
 }
 
 _lib = None
@@ -338,6 +341,22 @@ def solve_flat(flat: FlatModel, tol=1e-10, max_iter=0, threads: int | None = Non
     out.final_residual = float(sol.final_residual)
     out.cond_estimate = float(sol.cond_estimate)
     return out
+
+
+def stress(flat: FlatModel, u, threads: int | None = None):
+    """(von Mises per element, per node, reactions) for a given u."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    vm = np.zeros(flat.n_elem)
+    vmn = np.zeros(flat.n_nodes)
+    re = np.zeros(flat.fixed_row.shape[0])
+    err = abi.SvxError()
+    s = flat.as_struct()
+    st = lib().svx_oracle_stress(C.byref(s), abi.ptr(u, C.c_double), threads or default_threads(),
+                                 abi.ptr(vm, C.c_double), abi.ptr(vmn, C.c_double),
+                                 abi.ptr(re, C.c_double), C.byref(err))
+    if st != abi.SVX_OK:
+        _raise_err(err)
+    return vm, vmn, re
 
 
 def solve(model: Model, tol=1e-10, threads: int | None = None):

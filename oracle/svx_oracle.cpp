@@ -654,6 +654,60 @@ int material_check(const svx_flat_model_t* m, int64_t e) {
 
 }  // namespace
 
+extern "C" void svx_oracle_spmv(const svx_oracle_csr_t* k, const double* x, double* y, int threads);
+
+namespace {
+
+// stress.rs:22-118: centroid von Mises, nodal (extrapolated, averaged)
+// von Mises and reactions K_orig u - f_orig at the constrained rows.
+void recover(const svx_flat_model_t* m, const double* u, const svx_oracle_csr_t* k_orig,
+             const double* f_orig, int threads, double* vm, double* vm_node, double* reactions) {
+    const int ndof = m->ndof;
+    const int64_t n = m->n_nodes * ndof;
+    // stress.rs:22-98
+    std::vector<double> sum(6 * m->n_nodes, 0.0);
+    std::vector<uint32_t> count(m->n_nodes, 0);
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        int kind = m->kind[e];
+        int nn = node_count(kind);
+        const int32_t* cn = m->conn + m->conn_ptr[e];
+        double coords[24], ue[24], cen[6], nod[8][6];
+        for (int i = 0; i < nn; ++i) {
+            for (int q = 0; q < 3; ++q) coords[3 * i + q] = m->xyz[3 * int64_t(cn[i]) + q];
+            for (int q = 0; q < ndof; ++q) ue[i * ndof + q] = u[int64_t(cn[i]) * ndof + q];
+        }
+        element_stresses(kind, coords, m->youngs[e], m->poisson[e], m->thickness, ue, cen, nod);
+        if (vm) vm[e] = von_mises(cen);
+        for (int i = 0; i < nn; ++i) {
+            int64_t node = cn[i];
+            for (int q = 0; q < 6; ++q) sum[6 * node + q] += nod[i][q];
+            count[node] += 1;
+        }
+    }
+    if (vm_node)
+        for (int64_t i = 0; i < m->n_nodes; ++i) {
+            if (count[i] == 0) {
+                vm_node[i] = 0.0;
+                continue;
+            }
+            double c = double(count[i]);
+            double avg[6];
+            for (int q = 0; q < 6; ++q) avg[q] = sum[6 * i + q] / c;
+            vm_node[i] = von_mises(avg);
+        }
+    // stress.rs:103-118
+    if (reactions) {
+        std::vector<double> ku(n);
+        svx_oracle_spmv(k_orig, u, ku.data(), threads);
+        for (int64_t i = 0; i < m->n_fixed; ++i) {
+            int64_t row = m->fixed_row[i];
+            reactions[i] = ku[row] - f_orig[row];
+        }
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 void svx_oracle_set_sort_mode(int mode) { g_sort_mode = mode; }
@@ -941,48 +995,20 @@ int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t
             sol->displacements[3 * i + 1] = u[b + 1];
             sol->displacements[3 * i + 2] = (ndof == 3) ? u[b + 2] : 0.0;
         }
-    // stress.rs:22-98
-    std::vector<double> sum(6 * m->n_nodes, 0.0);
-    std::vector<uint32_t> count(m->n_nodes, 0);
-    for (int64_t e = 0; e < m->n_elem; ++e) {
-        int kind = m->kind[e];
-        int nn = node_count(kind);
-        const int32_t* cn = m->conn + m->conn_ptr[e];
-        double coords[24], ue[24], cen[6], nod[8][6];
-        for (int i = 0; i < nn; ++i) {
-            for (int q = 0; q < 3; ++q) coords[3 * i + q] = m->xyz[3 * int64_t(cn[i]) + q];
-            for (int q = 0; q < ndof; ++q) ue[i * ndof + q] = u[int64_t(cn[i]) * ndof + q];
-        }
-        element_stresses(kind, coords, m->youngs[e], m->poisson[e], m->thickness, ue, cen, nod);
-        if (sol->von_mises) sol->von_mises[e] = von_mises(cen);
-        for (int i = 0; i < nn; ++i) {
-            int64_t node = cn[i];
-            for (int q = 0; q < 6; ++q) sum[6 * node + q] += nod[i][q];
-            count[node] += 1;
-        }
-    }
-    if (sol->nodal_von_mises)
-        for (int64_t i = 0; i < m->n_nodes; ++i) {
-            if (count[i] == 0) {
-                sol->nodal_von_mises[i] = 0.0;
-                continue;
-            }
-            double c = double(count[i]);
-            double avg[6];
-            for (int q = 0; q < 6; ++q) avg[q] = sum[6 * i + q] / c;
-            sol->nodal_von_mises[i] = von_mises(avg);
-        }
-    // stress.rs:103-118
-    if (sol->reactions) {
-        std::vector<double> ku(n);
-        svx_oracle_spmv(&k_orig, u.data(), ku.data(), threads);
-        for (int64_t i = 0; i < m->n_fixed; ++i) {
-            int64_t row = m->fixed_row[i];
-            sol->reactions[i] = ku[row] - f_orig[row];
-        }
-    }
+    recover(m, u.data(), &k_orig, f_orig.data(), threads, sol->von_mises, sol->nodal_von_mises,
+            sol->reactions);
     svx_oracle_csr_free(&k);
     if (err) set_error(err, SVX_OK, 0, -1, "");
+    return SVX_OK;
+}
+
+int svx_oracle_stress(const svx_flat_model_t* m, const double* u, int threads, double* vm,
+                      double* vm_node, double* reactions, svx_error_t* err) {
+    svx_oracle_csr_t k;
+    int st = svx_oracle_assemble(m, threads, &k, err);
+    if (st != SVX_OK) return st;
+    recover(m, u, &k, k.f, threads, vm, vm_node, reactions);
+    svx_oracle_csr_free(&k);
     return SVX_OK;
 }
 

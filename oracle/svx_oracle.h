@@ -64,6 +64,12 @@ int svx_oracle_pcg(const svx_oracle_csr_t* k, const double* f, double tol, int64
 int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t max_iter,
                      svx_solution_t* sol, svx_error_t* err);
 
+/* Stress + reaction recovery for a given u (stress.rs:22-118); K_orig for
+ * the reactions is assembled with the current sort mode.  Output arrays may
+ * be NULL. */
+int svx_oracle_stress(const svx_flat_model_t* m, const double* u, int threads, double* vm,
+                      double* vm_node, double* reactions, svx_error_t* err);
+
 #ifdef __cplusplus
 }
 #endif

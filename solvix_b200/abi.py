@@ -31,6 +31,8 @@ SVX_QUEUE_EMPTY = 8
 # enum svx_elem_kind (order of ElemKind, crates/solvix-core/src/lib.rs:54-73)
 SVX_CPS3, SVX_CPS4, SVX_CPS8, SVX_CPE4, SVX_CPE8, SVX_C3D8, SVX_C3D4, SVX_B31 = range(8)
 
+SVX_KEEP_ORIGINAL = 1
+
 # enum svx_precision
 SVX_FP64 = 0
 SVX_MIXED = 1
@@ -156,11 +158,14 @@ SIGNATURES = {
     "svx_resolve": (C.c_int, [C.POINTER(SvxModelDesc), C.POINTER(_VP), C.POINTER(SvxError)]),
     "svx_resolved_flat": (C.POINTER(SvxFlatModel), [_VP]),
     "svx_resolved_free": (C.c_int, [_VP]),
-    "svx_assemble": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.POINTER(_VP), C.POINTER(SvxError)]),
+    "svx_assemble": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.c_uint32, C.POINTER(_VP),
+                               C.POINTER(SvxError)]),
     "svx_op_free": (C.c_int, [_VP]),
     "svx_op_dims": (C.c_int, [_VP, c_int64_p, c_int64_p]),
-    "svx_op_get_csr": (C.c_int, [_VP, c_int64_p, c_int32_p, c_double_p]),
+    "svx_op_get_csr": (C.c_int, [_VP, C.c_int, c_int64_p, c_int32_p, c_double_p]),
+    "svx_op_get_vectors": (C.c_int, [_VP, C.c_int, c_double_p, c_double_p]),
     "svx_op_spmv": (C.c_int, [_VP, c_double_p, c_double_p]),
+    "svx_op_set_solution": (C.c_int, [_VP, c_double_p]),
     "svx_op_solve": (C.c_int, [_VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),
                                C.POINTER(SvxError)]),
     "svx_op_stress": (C.c_int, [_VP, C.POINTER(SvxSolution)]),

@@ -1,0 +1,269 @@
+"""Host-side API over the C ABI: contexts, operators and the solve entry
+points that mirror solvix-core's ``solve`` / ``solve_with_method``
+(crates/solvix-core/src/lib.rs:556-590).
+
+Every compute call goes through ``libsolvix_b200.so``; when the library or
+the CUDA device is unavailable the calls raise (there is no CPU path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .marshal import FlatModel, model_desc
+from .model import (DeviceError, EmptyMesh, InvalidModel, Method, Model, NoConstraints,
+                    NotConverged, Reaction, SolveError, Solution)
+
+
+def _raise(status: int, err: abi.SvxError | None, what: str = ""):
+    msg = err.message.decode(errors="replace") if err is not None else what
+    if status == abi.SVX_INVALID_MODEL:
+        raise InvalidModel(msg, reason=int(err.reason) if err is not None else 0,
+                           elem_index=int(err.elem_index) if err is not None else -1)
+    if status == abi.SVX_NOT_CONVERGED:
+        raise NotConverged(int(err.iterations), float(err.residual))
+    if status == abi.SVX_NO_CONSTRAINTS:
+        raise NoConstraints("no constraints")
+    if status == abi.SVX_EMPTY_MESH:
+        raise EmptyMesh("empty mesh")
+    if status == abi.SVX_BAD_ARGUMENT:
+        raise ValueError(msg or "bad argument")
+    raise DeviceError(msg or f"status {status}")
+
+
+class Context:
+    """One device context: a CUDA stream and a caching device allocator."""
+
+    def __init__(self, device: int = 0):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        st = self.lib.svx_ctx_create(int(device), C.byref(h))
+        if st != abi.SVX_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.svx_last_error(None, buf, 512)
+            raise DeviceError(buf.value.decode() or f"svx_ctx_create failed ({st})")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.svx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def assemble(self, flat: FlatModel, keep_original: bool = False) -> "Operator":
+        s = flat.as_struct()
+        h = C.c_void_p()
+        err = abi.SvxError()
+        flags = abi.SVX_KEEP_ORIGINAL if keep_original else 0
+        st = self.lib.svx_assemble(self.handle, C.byref(s), flags, C.byref(h), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        return Operator(self, h, flat)
+
+    def solve_flat(self, flat: FlatModel, tol: float = 1e-10, max_iter: int = 0,
+                   precision: int = abi.SVX_FP64, inner_tol: float = 1e-5,
+                   want_stress: bool = True, check_every: int = 0) -> Solution:
+        out = _SolutionBuffers(flat.n_nodes, flat.ndof, flat.n_elem, flat.fixed_row.shape[0])
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
+                                inner_tol=inner_tol, want_stress=int(want_stress),
+                                check_every=check_every)
+        err = abi.SvxError()
+        s = flat.as_struct()
+        st = self.lib.svx_solve_flat(self.handle, C.byref(s), C.byref(opts),
+                                     C.byref(out.struct), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        return out.solution(flat, precision)
+
+    def solve_model(self, model: Model, tol: float = 1e-10, precision: int = abi.SVX_FP64,
+                    inner_tol: float = 1e-5) -> Solution:
+        """The reference-shaped path: resolve ids / sets on the host (C++),
+        then assemble, solve and recover stresses on the device."""
+        _bcs, _cl, dloads, gravity = model.load_state()
+        if dloads or gravity:
+            raise InvalidModel("distributed loads and gravity are outside the linear-static "
+                               "GPU path (concentrated loads only)")
+        desc, keep = model_desc(model)
+        res = C.c_void_p()
+        err = abi.SvxError()
+        st = self.lib.svx_resolve(C.byref(desc), C.byref(res), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        try:
+            flat_s = self.lib.svx_resolved_flat(res).contents
+            n_nodes, ndof = int(flat_s.n_nodes), int(flat_s.ndof)
+            out = _SolutionBuffers(n_nodes, ndof, int(flat_s.n_elem), int(flat_s.n_fixed))
+            opts = abi.default_opts(tol=tol, precision=precision, inner_tol=inner_tol)
+            st = self.lib.svx_solve_resolved(self.handle, res, C.byref(opts),
+                                             C.byref(out.struct), C.byref(err))
+            if st != abi.SVX_OK:
+                _raise(st, err)
+            rows = np.ctypeslib.as_array(flat_s.fixed_row, shape=(int(flat_s.n_fixed),)).copy() \
+                if flat_s.n_fixed else np.zeros(0, np.int64)
+            node_ids = np.ctypeslib.as_array(flat_s.node_id, shape=(n_nodes,)).copy()
+        finally:
+            self.lib.svx_resolved_free(res)
+        return out.solution_from(rows, node_ids, ndof, precision)
+
+
+class _SolutionBuffers:
+    def __init__(self, n_nodes, ndof, n_elem, n_fixed):
+        self.u = np.zeros(n_nodes * ndof)
+        self.disp = np.zeros((n_nodes, 3))
+        self.vm = np.zeros(n_elem)
+        self.vm_node = np.zeros(n_nodes)
+        self.react = np.zeros(n_fixed)
+        s = abi.SvxSolution()
+        s.u = abi.ptr(self.u, C.c_double)
+        s.displacements = abi.ptr(self.disp, C.c_double)
+        s.von_mises = abi.ptr(self.vm, C.c_double)
+        s.nodal_von_mises = abi.ptr(self.vm_node, C.c_double)
+        s.reactions = abi.ptr(self.react, C.c_double)
+        self.struct = s
+
+    def solution_from(self, rows, node_ids, ndof, precision) -> Solution:
+        s = self.struct
+        reactions = [Reaction(int(node_ids[r // ndof]), int(r % ndof) + 1, float(v))
+                     for r, v in zip(rows.tolist(), self.react.tolist())] \
+            if rows.shape[0] <= 200000 else []
+        return Solution(
+            displacements=self.disp, von_mises=self.vm, nodal_von_mises=self.vm_node,
+            reactions=reactions, iterations=int(s.iterations),
+            final_residual=float(s.final_residual),
+            solver_method="pcg" if precision == abi.SVX_FP64 else "pcg-mixed",
+            cond_estimate=float(s.cond_estimate), u=self.u, reaction_values=self.react,
+            outer_iterations=int(s.outer_iterations), ms_assemble=float(s.ms_assemble),
+            ms_solve=float(s.ms_solve), ms_stress=float(s.ms_stress))
+
+    def solution(self, flat: FlatModel, precision) -> Solution:
+        node_ids = flat.node_id if flat.node_id is not None else \
+            np.arange(1, flat.n_nodes + 1, dtype=np.uint32)
+        return self.solution_from(flat.fixed_row, node_ids, flat.ndof, precision)
+
+
+class Operator:
+    """An assembled system resident on the device (svx_op_t)."""
+
+    def __init__(self, ctx: Context, handle, flat: FlatModel):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.handle = handle
+        self.flat = flat
+        n = C.c_int64()
+        nnz = C.c_int64()
+        self.lib.svx_op_dims(handle, C.byref(n), C.byref(nnz))
+        self.n, self.nnz = int(n.value), int(nnz.value)
+
+    def free(self):
+        if getattr(self, "handle", None):
+            self.lib.svx_op_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def csr(self, which: int = 0):
+        rp = np.zeros(self.n + 1, dtype=np.int64)
+        ci = np.zeros(self.nnz, dtype=np.int32)
+        v = np.zeros(self.nnz)
+        st = self.lib.svx_op_get_csr(self.handle, int(which), abi.ptr(rp, C.c_int64),
+                                     abi.ptr(ci, C.c_int32), abi.ptr(v, C.c_double))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_get_csr failed")
+        return rp, ci, v
+
+    def vectors(self, which: int = 0):
+        f = np.zeros(self.n)
+        d = np.zeros(self.n)
+        st = self.lib.svx_op_get_vectors(self.handle, int(which), abi.ptr(f, C.c_double),
+                                         abi.ptr(d, C.c_double))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_get_vectors failed")
+        return f, d
+
+    def spmv(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.n)
+        st = self.lib.svx_op_spmv(self.handle, abi.ptr(x, C.c_double), abi.ptr(y, C.c_double))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_spmv failed")
+        return y
+
+    def set_solution(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        st = self.lib.svx_op_set_solution(self.handle, abi.ptr(u, C.c_double))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_set_solution failed")
+
+    def solve(self, tol=1e-10, max_iter=0, precision=abi.SVX_FP64, inner_tol=1e-5,
+              check_every=0):
+        u = np.zeros(self.n)
+        sol = abi.SvxSolution()
+        sol.u = abi.ptr(u, C.c_double)
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
+                                inner_tol=inner_tol, check_every=check_every)
+        err = abi.SvxError()
+        st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        return u, int(sol.iterations), float(sol.final_residual), float(sol.cond_estimate)
+
+    def stress(self):
+        fl = self.flat
+        out = _SolutionBuffers(fl.n_nodes, fl.ndof, fl.n_elem, fl.fixed_row.shape[0])
+        st = self.lib.svx_op_stress(self.handle, C.byref(out.struct))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_stress failed")
+        return out.vm, out.vm_node, out.react, out.disp
+
+
+_default = {}
+_default_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _default_lock:
+        ctx = _default.get(device)
+        if ctx is None:
+            ctx = Context(device)
+            _default[device] = ctx
+        return ctx
+
+
+def solve_with_method(model: Model, method: Method = Method.Auto,
+                      ctx: Optional[Context] = None) -> Solution:
+    """Linear-static solve of a reference-shaped model on the GPU.
+
+    ``Method.Auto`` and ``Method.Pcg`` run the FP64 Jacobi-PCG; a budget
+    overrun surfaces as ``NotConverged`` (no direct CPU fallback).
+    """
+    if method == Method.Ldlt:
+        raise InvalidModel("the direct LDLT solver is outside the GPU path (Jacobi-PCG only)")
+    return (ctx or default_context()).solve_model(model)
+
+
+def solve(model: Model, ctx: Optional[Context] = None) -> Solution:
+    """solvix_core::solve for linear-static models (lib.rs:556-581)."""
+    if model.steps and model.steps[-1].nlgeom:
+        raise InvalidModel("NLGEOM steps are outside the linear-static GPU path")
+    return solve_with_method(model, Method.Auto, ctx)

@@ -1,0 +1,630 @@
+// svx_api.cpp - the C ABI of libsolvix_b200: contexts, operators and the
+// one-call linear-static pipeline that replaces the body of
+// solve_with_thermal (crates/solvix-core/src/lib.rs:614-703).
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "svx_internal.h"
+
+namespace svx {
+
+// ------------------------------------------------------------ DevicePool
+DevicePool::~DevicePool() {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device_);
+    for (auto& kv : sizes_) cudaFree(kv.first);
+    cudaSetDevice(prev);
+}
+
+static size_t round_bytes(size_t b) {
+    // 2 MiB granules for large blocks, 512 B below: repeated solves of the
+    // same shape hit the cache exactly.
+    if (b >= (size_t(1) << 21)) return (b + (size_t(1) << 21) - 1) & ~((size_t(1) << 21) - 1);
+    return (b + 511) & ~size_t(511);
+}
+
+void* DevicePool::alloc(size_t bytes) {
+    size_t want = round_bytes(bytes);
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = free_.lower_bound(want);
+    if (it != free_.end() && it->first <= want + want / 8) {
+        void* p = it->second;
+        free_.erase(it);
+        cached_ -= sizes_[p];
+        in_use_ += sizes_[p];
+        return p;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        // drop the cache and retry once
+        cudaGetLastError();
+        for (auto& kv : free_) {
+            cudaFree(kv.second);
+            sizes_.erase(kv.second);
+        }
+        free_.clear();
+        cached_ = 0;
+        e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw ModelFail{SVX_OOM, 0, -1,
+                            "device allocation of " + std::to_string(want) + " bytes failed"};
+        }
+    }
+    sizes_[p] = want;
+    in_use_ += want;
+    return p;
+}
+
+void DevicePool::release(void* p) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = sizes_.find(p);
+    if (it == sizes_.end()) return;
+    in_use_ -= it->second;
+    cached_ += it->second;
+    free_.emplace(it->second, p);
+}
+
+void DevicePool::trim() {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto& kv : free_) {
+        cudaFree(kv.second);
+        sizes_.erase(kv.second);
+    }
+    free_.clear();
+    cached_ = 0;
+}
+
+}  // namespace svx
+
+using namespace svx;
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+void fill_error(svx_error_t* err, int code, int reason, int64_t elem, const std::string& msg) {
+    if (!err) return;
+    err->code = code;
+    err->reason = reason;
+    err->elem_index = elem;
+    err->iterations = 0;
+    err->residual = 0.0;
+    std::snprintf(err->message, sizeof(err->message), "%s", msg.c_str());
+}
+
+void clear_error(svx_error_t* err) { fill_error(err, SVX_OK, 0, -1, ""); }
+
+// Runs fn, mapping exceptions to status codes and error records.
+template <class F>
+int guarded(svx_ctx* ctx, svx_error_t* err, F&& fn) {
+    try {
+        return fn();
+    } catch (const ModelFail& m) {
+        fill_error(err, m.code, m.reason, m.elem_index, m.message);
+        if (ctx) ctx->last_error = m.message;
+        g_thread_error = m.message;
+        return m.code;
+    } catch (const CudaFail& c) {
+        std::string msg = std::string("CUDA error: ") + cudaGetErrorString(c.code) + " (" +
+                          c.where + ")";
+        cudaGetLastError();
+        fill_error(err, SVX_CUDA_ERROR, 0, -1, msg);
+        if (ctx) ctx->last_error = msg;
+        g_thread_error = msg;
+        return SVX_CUDA_ERROR;
+    } catch (const std::bad_alloc&) {
+        fill_error(err, SVX_OOM, 0, -1, "host allocation failed");
+        g_thread_error = "host allocation failed";
+        return SVX_OOM;
+    }
+}
+
+int node_count(int kind) {
+    switch (kind) {
+        case SVX_CPS3: return 3;
+        case SVX_CPS4: return 4;
+        case SVX_CPS8: return 8;
+        case SVX_CPE4: return 4;
+        case SVX_CPE8: return 8;
+        case SVX_C3D8: return 8;
+        case SVX_C3D4: return 4;
+        case SVX_B31: return 2;
+        default: return -1;
+    }
+}
+
+const char* kind_name(int kind) {
+    static const char* names[] = {"CPS3", "CPS4", "CPS8", "CPE4", "CPE8", "C3D8", "C3D4", "B31"};
+    return (kind >= 0 && kind < 8) ? names[kind] : "unknown";
+}
+
+const char* reason_text(int reason) {
+    switch (reason) {
+        case SVX_REASON_NO_MATERIAL: return "no material assigned";
+        case SVX_REASON_BAD_MATERIAL: return "invalid material constants";
+        case SVX_REASON_SOLID_POISSON:
+            return "poisson ratio must be < 0.5 for solids and plane strain";
+        case SVX_REASON_DEGENERATE_TRI: return "degenerate (zero-area) triangle";
+        case SVX_REASON_BAD_JACOBIAN: return "non-positive Jacobian determinant at a Gauss point";
+        default: return "element kind outside the linear-static GPU path (CPS3, CPS4, C3D8)";
+    }
+}
+
+uint32_t elem_id_of(const svx_flat_model_t* m, int64_t e) {
+    return m->elem_id ? m->elem_id[e] : uint32_t(e + 1);
+}
+
+// element_entry's checks that precede the geometry (assembly.rs:143-160),
+// plus the kinds this path integrates.
+int material_reason(const svx_flat_model_t* m, int64_t e) {
+    if (m->no_material && m->no_material[e]) return SVX_REASON_NO_MATERIAL;
+    double E = m->youngs[e], nu = m->poisson[e];
+    if (E <= 0.0 || std::fabs(nu) >= 1.0) return SVX_REASON_BAD_MATERIAL;
+    int k = m->kind[e];
+    bool solid = (k == SVX_C3D8 || k == SVX_C3D4);
+    bool plane_strain = (k == SVX_CPE4 || k == SVX_CPE8);
+    if ((solid || plane_strain) && nu >= 0.5) return SVX_REASON_SOLID_POISSON;
+    if (!(k == SVX_CPS3 || k == SVX_CPS4 || k == SVX_C3D8)) return SVX_REASON_UNSUPPORTED_KIND;
+    return 0;
+}
+
+std::string element_message(const svx_flat_model_t* m, int64_t e, int reason) {
+    std::string msg = "element " + std::to_string(elem_id_of(m, e)) + ": ";
+    if (reason == SVX_REASON_UNSUPPORTED_KIND)
+        msg += std::string("element kind ") + kind_name(m->kind[e]) +
+               " is outside the linear-static GPU path (CPS3, CPS4, C3D8)";
+    else
+        msg += reason_text(reason);
+    return msg;
+}
+
+void check_flat(const svx_flat_model_t* m) {
+    auto bad = [](const std::string& s) { throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, s}; };
+    if (!m) bad("null model");
+    if (m->n_nodes < 0 || m->n_elem < 0 || m->n_fixed < 0) bad("negative size");
+    if (m->ndof != 2 && m->ndof != 3) bad("ndof must be 2 or 3");
+    if (m->n_nodes > 0 && !m->xyz) bad("null xyz");
+    if (m->n_elem > 0 && (!m->kind || !m->conn_ptr || !m->conn || !m->youngs || !m->poisson))
+        bad("null element array");
+    if (m->n_fixed > 0 && !m->fixed_row) bad("null fixed_row");
+    if (m->n_nodes >= (int64_t(1) << 31) / 3) bad("too many nodes for int32 indices");
+    if (m->n_elem > 0 && m->conn_ptr[0] != 0) bad("conn_ptr[0] must be 0");
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        int64_t a = m->conn_ptr[e], b = m->conn_ptr[e + 1];
+        int nn = node_count(m->kind[e]);
+        if (nn < 0) bad("unknown element kind " + std::to_string(int(m->kind[e])));
+        if (b - a != nn)
+            bad("element " + std::to_string(elem_id_of(m, e)) + " has " + std::to_string(b - a) +
+                " nodes, kind needs " + std::to_string(nn));
+        for (int64_t q = a; q < b; ++q)
+            if (m->conn[q] < 0 || m->conn[q] >= m->n_nodes)
+                bad("element " + std::to_string(elem_id_of(m, e)) + " references node index " +
+                    std::to_string(m->conn[q]) + " out of range");
+    }
+    const int64_t n = m->n_nodes * m->ndof;
+    for (int64_t k = 0; k < m->n_fixed; ++k)
+        if (m->fixed_row[k] < 0 || m->fixed_row[k] >= n)
+            bad("fixed row " + std::to_string(m->fixed_row[k]) + " out of range");
+}
+
+template <class T>
+void upload(svx_ctx* ctx, DBuf<T>& dst, const T* src, size_t count) {
+    dst.alloc(ctx->pool, count + 1);
+    if (count)
+        SVX_CUDA(cudaMemcpyAsync(dst.p, src, count * sizeof(T), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    SVX_CUDA(cudaEventSynchronize(b));
+    SVX_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+// K1-K4 for a validated flat model; throws ModelFail for element errors.
+svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
+    SVX_CUDA(cudaSetDevice(ctx->device));
+    check_flat(m);
+    // ndof_per_node (lib.rs:725-752) runs before assembly
+    bool solid = false, plane = false, beam = false;
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        int k = m->kind[e];
+        if (k == SVX_C3D8 || k == SVX_C3D4) solid = true;
+        else if (k == SVX_B31) beam = true;
+        else plane = true;
+    }
+    if (beam && (plane || solid))
+        throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                        "mixed beam and continuum elements (v1: B31-only models)"};
+    if (solid && plane) throw ModelFail{SVX_INVALID_MODEL, 0, -1, "mixed dimensionality"};
+    if (m->ndof != ((solid || beam) ? 3 : 2))
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "ndof does not match the element kinds"};
+    // first element failing a material / kind check (host, O(n_elem))
+    int64_t m_fail = -1;
+    int m_reason = 0;
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        int r = material_reason(m, e);
+        if (r) {
+            m_fail = e;
+            m_reason = r;
+            break;
+        }
+    }
+
+    std::unique_ptr<svx_op> op(new svx_op());
+    op->ctx = ctx;
+    op->n_nodes = m->n_nodes;
+    op->n_elem = (m_fail >= 0) ? m_fail : m->n_elem;  // elements before a material failure
+    op->ndof = m->ndof;
+    op->n = m->n_nodes * m->ndof;
+    op->thickness = m->thickness;
+    cudaStream_t st = ctx->stream;
+    SVX_CUDA(cudaEventRecord(ctx->ev[2], st));
+    upload(ctx, op->xyz, m->xyz, size_t(3 * m->n_nodes));
+    upload(ctx, op->kind, m->kind, size_t(op->n_elem));
+    upload(ctx, op->conn_ptr, m->conn_ptr, size_t(op->n_elem + 1));
+    upload(ctx, op->conn, m->conn, size_t(op->n_elem > 0 ? m->conn_ptr[op->n_elem] : 0));
+    upload(ctx, op->youngs, m->youngs, size_t(op->n_elem));
+    upload(ctx, op->poisson, m->poisson, size_t(op->n_elem));
+    int max_nn = 0;
+    for (int64_t e = 0; e < op->n_elem; ++e) max_nn = std::max(max_nn, node_count(m->kind[e]));
+    op->pat.max_nn = std::max(max_nn, 1);
+    const int max_N = max_nn * m->ndof;
+    op->pat.ke_stride = std::max(1, max_N * max_N);
+
+    // K1: element integration (only up to a material failure)
+    DBuf<double> ke;
+    ke.alloc(ctx->pool, size_t(op->n_elem) * op->pat.ke_stride + 1);
+    uint64_t g = integrate_elements(ctx, op.get(), ke.p, op->pat.ke_stride);
+    int64_t g_fail = (g == ~uint64_t(0)) ? -1 : int64_t(g >> 8);
+    int g_reason = int(g & 0xff);
+    if (g_fail >= 0) {
+        throw ModelFail{SVX_INVALID_MODEL, g_reason, g_fail, element_message(m, g_fail, g_reason)};
+    }
+    if (m_fail >= 0) {
+        throw ModelFail{SVX_INVALID_MODEL, m_reason, m_fail, element_message(m, m_fail, m_reason)};
+    }
+    // K3 pattern, K2 fixed-order assembly
+    build_pattern(ctx, op.get());
+    op->vals.alloc(ctx->pool, op->pat.nnz + 1);
+    assemble_values(ctx, op.get(), ke.p, op->pat.ke_stride, op->vals.p);
+    ke.reset();
+    if (flags & SVX_KEEP_ORIGINAL) {
+        op->vals_orig.alloc(ctx->pool, op->pat.nnz + 1);
+        SVX_CUDA(cudaMemcpyAsync(op->vals_orig.p, op->vals.p, op->pat.nnz * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st));
+    }
+    // loads and constraints
+    std::vector<double> f(size_t(op->n), 0.0);
+    if (m->f) std::memcpy(f.data(), m->f, sizeof(double) * op->n);
+    upload(ctx, op->f_orig, f.data(), size_t(op->n));
+    op->n_fixed = m->n_fixed;
+    op->h_fixed_row.assign(m->fixed_row, m->fixed_row + m->n_fixed);
+    upload(ctx, op->fixed_row, op->h_fixed_row.data(), size_t(m->n_fixed));
+    op->h_node_id.resize(size_t(m->n_nodes));
+    for (int64_t i = 0; i < m->n_nodes; ++i)
+        op->h_node_id[i] = m->node_id ? m->node_id[i] : uint32_t(i + 1);
+    // K4
+    apply_dirichlet(ctx, op.get());
+    op->spmv_group = choose_spmv_group(op.get());
+    SVX_CUDA(cudaEventRecord(ctx->ev[3], st));
+    op->ms_assemble = elapsed_ms(ctx->ev[2], ctx->ev[3]);
+    return op.release();
+}
+
+long long default_max_iter(int64_t n) { return std::max<long long>(1000, 10 * (long long)n); }
+
+int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_error_t* err) {
+    svx_ctx* ctx = op->ctx;
+    SVX_CUDA(cudaSetDevice(ctx->device));
+    svx_solve_opts_t opts;
+    svx_default_opts(&opts);
+    if (o) opts = *o;
+    long long max_iter = opts.max_iter > 0 ? opts.max_iter : default_max_iter(op->n);
+    op->u.alloc(ctx->pool, op->n + 1);
+    PcgResult r;
+    long long outer = 0;
+    if (opts.precision == SVX_MIXED)
+        r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol > 0 ? opts.inner_tol : 1e-5,
+                      opts.check_every, op->u.p, &outer);
+    else
+        r = pcg_fp64(ctx, op, opts.tol, max_iter, opts.check_every, op->u.p);
+    op->has_solution = true;
+    if (sol) {
+        sol->iterations = r.iterations;
+        sol->outer_iterations = outer;
+        sol->final_residual = r.residual;
+        sol->cond_estimate = op->cond_estimate;
+        sol->ms_assemble = op->ms_assemble;
+        sol->ms_solve = r.ms;
+        if (sol->u)
+            SVX_CUDA(cudaMemcpyAsync(sol->u, op->u.p, op->n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (r.status != PCG_CONVERGED) {
+        SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::string msg = "not converged after " + std::to_string(r.iterations) + " iterations";
+        fill_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
+        if (err) {
+            err->iterations = r.iterations;
+            err->residual = r.residual;
+        }
+        ctx->last_error = msg;
+        return SVX_NOT_CONVERGED;
+    }
+    if (sol && opts.want_stress) {
+        SVX_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+        DBuf<double> vm_e, vm_n, react, disp;
+        if (sol->von_mises) vm_e.alloc(ctx->pool, op->n_elem + 1);
+        if (sol->nodal_von_mises) vm_n.alloc(ctx->pool, op->n_nodes + 1);
+        if (sol->reactions) react.alloc(ctx->pool, op->n_fixed + 1);
+        if (sol->displacements) disp.alloc(ctx->pool, 3 * op->n_nodes + 1);
+        recover_stress(ctx, op, op->u.p, vm_e.p, vm_n.p, react.p, disp.p);
+        SVX_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
+        cudaStream_t st = ctx->stream;
+        if (sol->von_mises && op->n_elem)
+            SVX_CUDA(cudaMemcpyAsync(sol->von_mises, vm_e.p, op->n_elem * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->nodal_von_mises && op->n_nodes)
+            SVX_CUDA(cudaMemcpyAsync(sol->nodal_von_mises, vm_n.p, op->n_nodes * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->reactions && op->n_fixed)
+            SVX_CUDA(cudaMemcpyAsync(sol->reactions, react.p, op->n_fixed * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->displacements && op->n_nodes)
+            SVX_CUDA(cudaMemcpyAsync(sol->displacements, disp.p, 3 * op->n_nodes * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        sol->ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+    }
+    SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+    clear_error(err);
+    return SVX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* svx_version(void) { return "solvix_b200 0.1.0 (sm_100a)"; }
+
+void svx_default_opts(svx_solve_opts_t* opts) {
+    if (!opts) return;
+    opts->tol = 1e-10;
+    opts->max_iter = 0;
+    opts->precision = SVX_FP64;
+    opts->inner_tol = 1e-5;
+    opts->check_every = 0;
+    opts->want_stress = 1;
+}
+
+int svx_ctx_create(int device, svx_ctx_t** out) {
+    if (!out) return SVX_BAD_ARGUMENT;
+    *out = nullptr;
+    return guarded(nullptr, nullptr, [&]() -> int {
+        int count = 0;
+        SVX_CUDA(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count)
+            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                            "CUDA device " + std::to_string(device) + " is not available"};
+        SVX_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        SVX_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                            std::string("device ") + prop.name +
+                                " is not sm_100 (B200); this library is built for sm_100a only"};
+        std::unique_ptr<svx_ctx> ctx(new svx_ctx());
+        ctx->device = device;
+        ctx->sm_count = prop.multiProcessorCount;
+        SVX_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        for (auto& e : ctx->ev) SVX_CUDA(cudaEventCreate(&e));
+        ctx->pool = new DevicePool(device);
+        *out = ctx.release();
+        return SVX_OK;
+    });
+}
+
+int svx_ctx_destroy(svx_ctx_t* ctx) {
+    if (!ctx) return SVX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx->pool;
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SVX_OK;
+}
+
+int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len) {
+    if (!buf || len == 0) return SVX_BAD_ARGUMENT;
+    const std::string& s = ctx ? ctx->last_error : g_thread_error;
+    std::snprintf(buf, len, "%s", s.c_str());
+    return SVX_OK;
+}
+
+int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, uint32_t flags, svx_op_t** out,
+                 svx_error_t* err) {
+    if (!ctx || !out) return SVX_BAD_ARGUMENT;
+    *out = nullptr;
+    return guarded(ctx, err, [&]() -> int {
+        *out = assemble_impl(ctx, model, flags);
+        clear_error(err);
+        return SVX_OK;
+    });
+}
+
+int svx_op_free(svx_op_t* op) {
+    if (!op) return SVX_OK;
+    cudaSetDevice(op->ctx->device);
+    cudaStreamSynchronize(op->ctx->stream);
+    delete op;
+    return SVX_OK;
+}
+
+int svx_op_dims(const svx_op_t* op, int64_t* n_rows, int64_t* nnz) {
+    if (!op) return SVX_BAD_ARGUMENT;
+    if (n_rows) *n_rows = op->n;
+    if (nnz) *nnz = op->pat.nnz;
+    return SVX_OK;
+}
+
+int svx_op_get_csr(const svx_op_t* op, int which, int64_t* row_ptr, int32_t* col_idx,
+                   double* vals) {
+    if (!op) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        if (row_ptr) {
+            std::vector<int32_t> rp(size_t(op->n + 1));
+            SVX_CUDA(cudaMemcpyAsync(rp.data(), op->pat.row_ptr.p, (op->n + 1) * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, st));
+            SVX_CUDA(cudaStreamSynchronize(st));
+            for (int64_t i = 0; i <= op->n; ++i) row_ptr[i] = rp[i];
+        }
+        if (col_idx && op->pat.nnz)
+            SVX_CUDA(cudaMemcpyAsync(col_idx, op->pat.col_idx.p, op->pat.nnz * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, st));
+        if (vals && op->pat.nnz) {
+            const double* src = which == 1 ? op->vals_orig.p : op->vals.p;
+            if (!src)
+                throw ModelFail{SVX_BAD_ARGUMENT, 0, -1,
+                                "K before Dirichlet was not kept (assemble with SVX_KEEP_ORIGINAL)"};
+            SVX_CUDA(cudaMemcpyAsync(vals, src, op->pat.nnz * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        }
+        SVX_CUDA(cudaStreamSynchronize(st));
+        return SVX_OK;
+    });
+}
+
+int svx_op_get_vectors(const svx_op_t* op, int which, double* f, double* inv_diag) {
+    if (!op) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        if (f && op->n)
+            SVX_CUDA(cudaMemcpyAsync(f, which == 1 ? op->f_orig.p : op->f.p, op->n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (inv_diag && op->n)
+            SVX_CUDA(cudaMemcpyAsync(inv_diag, op->inv_diag.p, op->n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        return SVX_OK;
+    });
+}
+
+int svx_op_spmv(svx_op_t* op, const double* x, double* y) {
+    if (!op || !x || !y) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        DBuf<double> dx, dy;
+        dx.alloc(ctx->pool, op->n + 1);
+        dy.alloc(ctx->pool, op->n + 1);
+        SVX_CUDA(cudaMemcpyAsync(dx.p, x, op->n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        spmv_fp64(ctx, op, op->vals.p, dx.p, dy.p);
+        SVX_CUDA(cudaMemcpyAsync(y, dy.p, op->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+        return SVX_OK;
+    });
+}
+
+int svx_op_set_solution(svx_op_t* op, const double* u) {
+    if (!op || !u) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        op->u.alloc(ctx->pool, op->n + 1);
+        SVX_CUDA(cudaMemcpyAsync(op->u.p, u, op->n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+        op->has_solution = true;
+        return SVX_OK;
+    });
+}
+
+int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol,
+                 svx_error_t* err) {
+    if (!op) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, err, [&]() -> int {
+        svx_solve_opts_t o;
+        svx_default_opts(&o);
+        if (opts) o = *opts;
+        o.want_stress = 0;
+        svx_solution_t tmp{};
+        if (sol) tmp = *sol;
+        int st = solve_impl(op, &o, sol ? &tmp : nullptr, err);
+        if (sol) {
+            sol->iterations = tmp.iterations;
+            sol->outer_iterations = tmp.outer_iterations;
+            sol->final_residual = tmp.final_residual;
+            sol->cond_estimate = tmp.cond_estimate;
+            sol->ms_assemble = tmp.ms_assemble;
+            sol->ms_solve = tmp.ms_solve;
+        }
+        return st;
+    });
+}
+
+int svx_op_stress(svx_op_t* op, svx_solution_t* sol) {
+    if (!op || !sol) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        if (!op->has_solution)
+            throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "operator has no solution yet"};
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        SVX_CUDA(cudaEventRecord(ctx->ev[4], st));
+        DBuf<double> vm_e, vm_n, react, disp;
+        if (sol->von_mises) vm_e.alloc(ctx->pool, op->n_elem + 1);
+        if (sol->nodal_von_mises) vm_n.alloc(ctx->pool, op->n_nodes + 1);
+        if (sol->reactions) react.alloc(ctx->pool, op->n_fixed + 1);
+        if (sol->displacements) disp.alloc(ctx->pool, 3 * op->n_nodes + 1);
+        recover_stress(ctx, op, op->u.p, vm_e.p, vm_n.p, react.p, disp.p);
+        SVX_CUDA(cudaEventRecord(ctx->ev[5], st));
+        if (sol->von_mises && op->n_elem)
+            SVX_CUDA(cudaMemcpyAsync(sol->von_mises, vm_e.p, op->n_elem * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->nodal_von_mises && op->n_nodes)
+            SVX_CUDA(cudaMemcpyAsync(sol->nodal_von_mises, vm_n.p, op->n_nodes * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->reactions && op->n_fixed)
+            SVX_CUDA(cudaMemcpyAsync(sol->reactions, react.p, op->n_fixed * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->displacements && op->n_nodes)
+            SVX_CUDA(cudaMemcpyAsync(sol->displacements, disp.p, 3 * op->n_nodes * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        if (sol->u)
+            SVX_CUDA(cudaMemcpyAsync(sol->u, op->u.p, op->n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+        sol->ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+        SVX_CUDA(cudaStreamSynchronize(st));
+        return SVX_OK;
+    });
+}
+
+int svx_solve_flat(svx_ctx_t* ctx, const svx_flat_model_t* model, const svx_solve_opts_t* opts,
+                   svx_solution_t* sol, svx_error_t* err) {
+    if (!ctx) return SVX_BAD_ARGUMENT;
+    return guarded(ctx, err, [&]() -> int {
+        std::unique_ptr<svx_op> op(assemble_impl(ctx, model, 0));
+        return solve_impl(op.get(), opts, sol, err);
+    });
+}
+
+}  // extern "C"

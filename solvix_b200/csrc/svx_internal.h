@@ -1,0 +1,230 @@
+// svx_internal.h - internal types shared by the host and device translation
+// units of libsolvix_b200 (not part of the public C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "solvix_gpu.h"
+
+namespace svx {
+
+// ------------------------------------------------------------------ errors
+struct CudaFail {
+    cudaError_t code;
+    std::string where;
+};
+
+#define SVX_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) throw ::svx::CudaFail{e_, std::string(#call) + " @ " \
+                                                         __FILE__ ":" + std::to_string(__LINE__)}; \
+    } while (0)
+
+#define SVX_LAUNCH_CHECK() SVX_CUDA(cudaGetLastError())
+
+// Error thrown for model / argument problems (carries the svx_error_t).
+struct ModelFail {
+    int code;
+    int reason;
+    int64_t elem_index;
+    std::string message;
+};
+
+// ------------------------------------------------------------------ memory
+// Caching device allocator owned by a context: freed blocks are kept and
+// reused by later requests of the same rounded size, so repeated solves on
+// one context do not call cudaMalloc.
+class DevicePool {
+public:
+    explicit DevicePool(int device) : device_(device) {}
+    ~DevicePool();
+    void* alloc(size_t bytes);
+    void release(void* p);
+    void trim();  // return cached blocks to the driver
+    size_t bytes_in_use() const { return in_use_; }
+    size_t bytes_cached() const { return cached_; }
+
+private:
+    int device_;
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;      // size -> block
+    std::map<void*, size_t> sizes_;          // live + cached blocks
+    size_t in_use_ = 0, cached_ = 0;
+};
+
+// Typed device buffer returned to the pool on destruction.
+template <class T>
+struct DBuf {
+    DevicePool* pool = nullptr;
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : pool(o.pool), p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        reset();
+        pool = o.pool; p = o.p; n = o.n;
+        o.p = nullptr; o.n = 0;
+        return *this;
+    }
+    ~DBuf() { reset(); }
+    void alloc(DevicePool* pl, size_t count) {
+        reset();
+        pool = pl;
+        n = count;
+        p = count ? static_cast<T*>(pl->alloc(count * sizeof(T))) : nullptr;
+    }
+    void reset() {
+        if (p && pool) pool->release(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace svx
+
+// ------------------------------------------------------------------ context
+struct svx_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    svx::DevicePool* pool = nullptr;
+    std::string last_error;
+    cudaEvent_t ev[8] = {};
+};
+
+namespace svx {
+
+// Device scalars of one PCG run (one 128-byte line).
+struct PcgScalars {
+    double rz;       // r . z of the current iterate
+    double pap;      // p . Kp of the current iteration
+    double alpha;
+    double beta;
+    double rr;       // r . r of the current iterate
+    double bnorm;    // ||f||
+    double tol;
+    double res;      // ||r|| / ||f|| of the current iterate
+    long long it;        // iterations completed
+    long long max_iter;
+    int status;          // PCG_RUNNING / PCG_CONVERGED / PCG_BREAKDOWN / PCG_MAXITER
+    unsigned int count_a;  // last-block-done counters
+    unsigned int count_b;
+    unsigned int count_c;
+};
+
+enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_BREAKDOWN = 2, PCG_MAXITER = 3 };
+
+// Mesh pattern: node -> incident element slots and node adjacency.
+struct Pattern {
+    int64_t n_nodes = 0, n_elem = 0;
+    int ndof = 0;
+    int max_nn = 0;            // max nodes per element in the model
+    int ke_stride = 0;         // doubles per element in the Ke buffer (max N^2)
+    int64_t n_slots = 0;       // sum of nodes over elements
+    int max_deg = 0;           // max node degree (adjacency incl. itself)
+    int max_slots = 0;         // max incident slots of a node
+    int64_t nnz = 0;
+    int64_t n = 0;             // rows = n_nodes * ndof
+    DBuf<int64_t> slot_ptr;    // [n_nodes + 1]
+    DBuf<int32_t> slot_elem;   // [n_slots] element index, ascending per node
+    DBuf<uint8_t> slot_local;  // [n_slots] local node position in the element
+    DBuf<uint16_t> slot_map;   // [n_slots * max_nn] adjacency position of each element node
+    DBuf<int64_t> adj_ptr;     // [n_nodes + 1]
+    DBuf<int32_t> adj;         // sorted neighbour node indices
+    DBuf<int64_t> node_base;   // [n_nodes + 1] first nnz of the node's rows
+    DBuf<int32_t> row_ptr;     // [n + 1]
+    DBuf<int32_t> col_idx;     // [nnz]
+    DBuf<int32_t> diag_pos;    // [n] nnz index of the diagonal
+};
+
+}  // namespace svx
+
+// ------------------------------------------------------------------ operator
+struct svx_op {
+    svx_ctx* ctx = nullptr;
+    // model on the device
+    int64_t n_nodes = 0, n_elem = 0, n = 0;
+    int ndof = 0;
+    double thickness = 1.0;
+    svx::DBuf<double> xyz;
+    svx::DBuf<uint8_t> kind;
+    svx::DBuf<int64_t> conn_ptr;
+    svx::DBuf<int32_t> conn;
+    svx::DBuf<double> youngs, poisson;
+    svx::Pattern pat;
+    // assembled system
+    svx::DBuf<double> vals;        // K after Dirichlet (the PCG operator)
+    svx::DBuf<float> vals32;       // FP32 copy (mixed precision)
+    svx::DBuf<double> f;           // load vector after Dirichlet
+    svx::DBuf<double> f_orig;      // load vector before Dirichlet
+    svx::DBuf<double> inv_diag;
+    svx::DBuf<uint8_t> is_fixed;
+    // constrained rows of the unmodified K (reactions)
+    int64_t n_fixed = 0;
+    int64_t n_fixed_rows = 0;
+    svx::DBuf<int64_t> fixed_row;      // [n_fixed] BC order
+    svx::DBuf<int32_t> fixed_slot;     // [n_fixed] -> compact row
+    svx::DBuf<int32_t> kc_ptr;         // [n_fixed_rows + 1]
+    svx::DBuf<int32_t> kc_col;
+    svx::DBuf<double> kc_val;
+    std::vector<int64_t> h_fixed_row;
+    std::vector<uint32_t> h_node_id;
+    // solution state
+    svx::DBuf<double> u;
+    bool has_solution = false;
+    double cond_estimate = 0.0;
+    double ms_assemble = 0.0;
+    // K before Dirichlet is reconstructable only for the constrained rows;
+    // svx_op_get_csr / svx_op_spmv use this copy when kept.
+    svx::DBuf<double> vals_orig;
+    // PCG tuning picked for this operator
+    int spmv_group = 8;
+    int spmv_block = 256;
+};
+
+namespace svx {
+
+// ---- host entry points implemented in the .cu files -------------------
+// Pattern (svx_pattern.cu).
+void build_pattern(svx_ctx* ctx, svx_op* op);
+// Element integration into a Ke buffer; returns the first failing element
+// as (index << 8 | reason) or UINT64_MAX (svx_element.cu).
+uint64_t integrate_elements(svx_ctx* ctx, svx_op* op, double* ke, int ke_stride);
+// Fixed-order gather of Ke into CSR values (svx_assemble.cu).
+void assemble_values(svx_ctx* ctx, svx_op* op, const double* ke, int ke_stride, double* vals);
+// Dirichlet + inverse diagonal + condition estimate (svx_assemble.cu).
+void apply_dirichlet(svx_ctx* ctx, svx_op* op);
+// Stress recovery (svx_element.cu).
+void recover_stress(svx_ctx* ctx, svx_op* op, const double* u, double* vm_elem,
+                    double* vm_node, double* reactions, double* disp3);
+
+// PCG (svx_pcg.cu).
+struct PcgResult {
+    int status;
+    long long iterations;
+    double residual;
+    double ms;
+};
+PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int check_every,
+                   double* u_dev);
+PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
+                    int check_every, double* u_dev, long long* outer_steps);
+void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y);
+int choose_spmv_group(const svx_op* op);
+
+// Generic device helpers (svx_pattern.cu).
+void exclusive_scan_i64(svx_ctx* ctx, const int64_t* in, int64_t* out, int64_t n,
+                        int64_t* total_host);
+
+}  // namespace svx

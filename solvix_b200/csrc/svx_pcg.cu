@@ -1,0 +1,637 @@
+// svx_pcg.cu - K5 CSR SpMV, K6 fused PCG vector kernels and K7 mixed
+// precision defect correction.
+//
+// The plain form restates solver::pcg_with_threads
+// (crates/solvix-core/src/solver.rs:82-149) on the device:
+//   per iteration  q = K p ; pap = p.q            (spmv_dot, one pass)
+//                  alpha = rz / pap ; u += alpha p ; r -= alpha q ;
+//                  rr = r.r ; z = r * inv_diag ; rz' = r.z   (update, one pass)
+//                  beta = rz' / rz ; p = z + beta p          (p_update, one pass)
+// with the same stopping rule (||r|| / ||f|| <= tol, checked after the r
+// update; pap <= 0 or NaN is a breakdown) and the same iteration count
+// semantics.  Every reduction is deterministic: fixed launch geometry,
+// warp-shuffle then shared-memory trees inside a block, and the last block
+// to finish (atomic ticket) sums the per-block partials in index order.
+// The three kernels of an iteration run as a CUDA graph of `check_every`
+// iterations; kernels return immediately once the device status says the
+// solve stopped, and the host reads the status once per graph launch.
+//
+// SpMV layout: G consecutive lanes own one row (G picked from the mean row
+// length: 81 nnz/row C3D8 rows use G = 16); lanes stream col_idx / vals
+// with unit stride (coalesced), gather x through L1/L2 (the x window of a
+// row block of a structured mesh is three node planes, far larger than
+// shared memory, so x is not staged there), and combine with shuffles.
+
+#include "svx_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace svx {
+
+namespace {
+
+constexpr int BLOCK = 256;
+
+// ------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Block sum of one value (all threads get the result).
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+    if (w == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Publishes a block partial; returns true in exactly one block (the last
+// to arrive), after which that block can read every partial.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = atomicAdd(counter, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// Fixed-order sum of partials[0..n) by one block.
+__device__ __forceinline__ double sum_partials(const double* partials, int n, double* sh) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) v += ((volatile const double*)partials)[k];
+    return block_sum(v, sh);
+}
+
+// ------------------------------------------------------------ kernels
+template <int G, class V>
+__device__ __forceinline__ double row_dot(const int32_t* __restrict__ col_idx,
+                                          const V* __restrict__ vals, const V* __restrict__ x,
+                                          int32_t a, int32_t b, int gl) {
+    double acc0 = 0.0, acc1 = 0.0;
+    int32_t j = a + gl;
+    for (; j + G < b; j += 2 * G) {
+        int32_t c0 = __ldg(col_idx + j), c1 = __ldg(col_idx + j + G);
+        double v0 = double(__ldg(vals + j)), v1 = double(__ldg(vals + j + G));
+        acc0 += v0 * double(x[c0]);
+        acc1 += v1 * double(x[c1]);
+    }
+    if (j < b) acc0 += double(__ldg(vals + j)) * double(x[__ldg(col_idx + j)]);
+    return acc0 + acc1;
+}
+
+// q = K p and per-block partial of p.q; the last block forms pap and alpha.
+template <int G, class V>
+__global__ void __launch_bounds__(BLOCK)
+spmv_dot_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
+                const int32_t* __restrict__ col_idx, const V* __restrict__ vals,
+                const V* __restrict__ p, V* __restrict__ q, double* __restrict__ partials,
+                PcgScalars* __restrict__ s) {
+    __shared__ double sh[32];
+    if (s->status != PCG_RUNNING) return;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t groups_per_block = BLOCK / G;
+    double dot = 0.0;
+    for (int64_t r = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; r < n;
+         r += int64_t(gridDim.x) * groups_per_block) {
+        double v = row_dot<G, V>(col_idx, vals, p, row_ptr[r], row_ptr[r + 1], gl);
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (gl == 0) {
+            V qv = V(v);
+            q[r] = qv;
+            dot += double(p[r]) * double(qv);
+        }
+    }
+    double bs = block_sum(dot, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+    if (last_block(&s->count_a)) {
+        double pap = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            s->count_a = 0;
+            s->pap = pap;
+            if (pap <= 0.0 || isnan(pap)) {
+                s->status = PCG_BREAKDOWN;
+                s->it = s->it + 1;
+                s->res = sqrt(s->rr) / s->bnorm;
+            } else {
+                s->alpha = s->rz / pap;
+            }
+        }
+    }
+}
+
+// u += alpha p ; r -= alpha q ; partials of r.r and r.z (z = r * inv_diag).
+template <class V, class U>
+__global__ void __launch_bounds__(BLOCK)
+update_kernel(int64_t n, U* __restrict__ u, V* __restrict__ r, const V* __restrict__ p,
+              const V* __restrict__ q, const V* __restrict__ inv_diag,
+              double* __restrict__ partials, PcgScalars* __restrict__ s) {
+    __shared__ double sh[32];
+    if (s->status != PCG_RUNNING) return;
+    const double alpha = s->alpha;
+    const V a = V(alpha);
+    double rr = 0.0, rz = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK) {
+        V pi = p[i];
+        u[i] = U(u[i] + U(a) * U(pi));
+        V ri = r[i] - a * q[i];
+        r[i] = ri;
+        V zi = ri * inv_diag[i];
+        rr += double(ri) * double(ri);
+        rz += double(ri) * double(zi);
+    }
+    double brr = block_sum(rr, sh);
+    double brz = block_sum(rz, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = brr;
+        partials[2 * blockIdx.x + 1] = brz;
+    }
+    if (last_block(&s->count_b)) {
+        double v0 = 0.0, v1 = 0.0;
+        for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
+            v0 += ((volatile double*)partials)[2 * k];
+            v1 += ((volatile double*)partials)[2 * k + 1];
+        }
+        double trr = block_sum(v0, sh);
+        double trz = block_sum(v1, sh);
+        if (threadIdx.x == 0) {
+            s->count_b = 0;
+            s->it = s->it + 1;
+            s->rr = trr;
+            double res = sqrt(trr) / s->bnorm;
+            s->res = res;
+            if (res <= s->tol) {
+                s->status = PCG_CONVERGED;
+            } else if (s->it >= s->max_iter) {
+                s->status = PCG_MAXITER;
+            } else {
+                s->beta = trz / s->rz;
+                s->rz = trz;
+            }
+        }
+    }
+}
+
+// p = z + beta p with z = r * inv_diag recomputed.
+template <class V>
+__global__ void __launch_bounds__(BLOCK)
+p_update_kernel(int64_t n, V* __restrict__ p, const V* __restrict__ r,
+                const V* __restrict__ inv_diag, const PcgScalars* __restrict__ s) {
+    if (s->status != PCG_RUNNING) return;
+    const V beta = V(s->beta);
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK)
+        p[i] = r[i] * inv_diag[i] + beta * p[i];
+}
+
+// r = b ; u = 0 ; p = z = r * inv_diag ; partials of b.b and r.z.
+template <class V, class B>
+__global__ void __launch_bounds__(BLOCK)
+init_kernel(int64_t n, const B* __restrict__ b, double b_scale, V* __restrict__ u,
+            V* __restrict__ r, V* __restrict__ p, const V* __restrict__ inv_diag,
+            double* __restrict__ partials, PcgScalars* __restrict__ s) {
+    __shared__ double sh[32];
+    double bb = 0.0, rz = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK) {
+        V ri = V(double(b[i]) * b_scale);
+        u[i] = V(0);
+        r[i] = ri;
+        V zi = ri * inv_diag[i];
+        p[i] = zi;
+        bb += double(ri) * double(ri);
+        rz += double(ri) * double(zi);
+    }
+    double bbb = block_sum(bb, sh);
+    double brz = block_sum(rz, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = bbb;
+        partials[2 * blockIdx.x + 1] = brz;
+    }
+    if (last_block(&s->count_c)) {
+        double v0 = 0.0, v1 = 0.0;
+        for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
+            v0 += ((volatile double*)partials)[2 * k];
+            v1 += ((volatile double*)partials)[2 * k + 1];
+        }
+        double tbb = block_sum(v0, sh);
+        double trz = block_sum(v1, sh);
+        if (threadIdx.x == 0) {
+            s->count_c = 0;
+            s->bnorm = sqrt(tbb);
+            s->rr = tbb;
+            s->rz = trz;
+            s->it = 0;
+            s->res = 0.0;
+            s->status = (s->bnorm == 0.0) ? PCG_CONVERGED : PCG_RUNNING;
+            if (s->bnorm != 0.0) s->res = 1.0;
+        }
+    }
+}
+
+// Plain y = K x (FP64), one row per G lanes.
+template <int G>
+__global__ void __launch_bounds__(BLOCK)
+spmv_kernel(int64_t n, const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col_idx,
+            const double* __restrict__ vals, const double* __restrict__ x,
+            double* __restrict__ y) {
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t groups_per_block = BLOCK / G;
+    for (int64_t r = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; r < n;
+         r += int64_t(gridDim.x) * groups_per_block) {
+        double v = row_dot<G, double>(col_idx, vals, x, row_ptr[r], row_ptr[r + 1], gl);
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (gl == 0) y[r] = v;
+    }
+}
+
+// Mixed precision outer step: r = f - K u (FP64), partial of r.r.
+template <int G>
+__global__ void __launch_bounds__(BLOCK)
+residual_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
+                const int32_t* __restrict__ col_idx, const double* __restrict__ vals,
+                const double* __restrict__ u, const double* __restrict__ f,
+                double* __restrict__ r, double* __restrict__ partials,
+                unsigned int* counter, double* __restrict__ out_rr) {
+    __shared__ double sh[32];
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t groups_per_block = BLOCK / G;
+    double rr = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; i < n;
+         i += int64_t(gridDim.x) * groups_per_block) {
+        double v = row_dot<G, double>(col_idx, vals, u, row_ptr[i], row_ptr[i + 1], gl);
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (gl == 0) {
+            double ri = f[i] - v;
+            r[i] = ri;
+            rr += ri * ri;
+        }
+    }
+    double b = block_sum(rr, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = b;
+    if (last_block(counter)) {
+        double t = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            *out_rr = t;
+        }
+    }
+}
+
+// u64 += scale * d32
+__global__ void correct_kernel(int64_t n, double* __restrict__ u, const float* __restrict__ d,
+                               double scale) {
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK)
+        u[i] += scale * double(d[i]);
+}
+
+__global__ void to_float_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK)
+        b[i] = float(a[i]);
+}
+
+// ------------------------------------------------------------ host side
+int pick_group(double mean_row) {
+    if (mean_row < 6) return 2;
+    if (mean_row < 12) return 4;
+    if (mean_row < 40) return 8;
+    if (mean_row < 96) return 16;
+    return 32;
+}
+
+unsigned grid_rows(const svx_ctx* ctx, int64_t n, int G) {
+    int64_t per_block = BLOCK / G;
+    int64_t need = (n + per_block - 1) / per_block;
+    int64_t cap = int64_t(ctx->sm_count) * 8;
+    return unsigned(std::max<int64_t>(1, std::min(need, cap)));
+}
+
+unsigned grid_vec(const svx_ctx* ctx, int64_t n) {
+    int64_t need = (n + BLOCK - 1) / BLOCK;
+    int64_t cap = int64_t(ctx->sm_count) * 8;
+    return unsigned(std::max<int64_t>(1, std::min(need, cap)));
+}
+
+template <class V>
+void launch_spmv_dot(int G, unsigned grid, cudaStream_t st, int64_t n, const svx_op* op,
+                     const V* vals, const V* p, V* q, double* partials, PcgScalars* s) {
+    const int32_t* rp = op->pat.row_ptr.p;
+    const int32_t* ci = op->pat.col_idx.p;
+    switch (G) {
+        case 2: spmv_dot_kernel<2, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 4: spmv_dot_kernel<4, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 8: spmv_dot_kernel<8, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 16: spmv_dot_kernel<16, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        default: spmv_dot_kernel<32, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+    }
+}
+
+// One PCG run in value type V (the vectors and K) with solution type U.
+template <class V, class U>
+struct PcgRun {
+    svx_ctx* ctx;
+    const svx_op* op;
+    int64_t n;
+    int G;
+    unsigned grid_r, grid_v;
+    const V* vals;
+    const V* inv_diag;
+    U* u;
+    V *r, *p, *q;
+    double* partials;
+    PcgScalars* s;
+    PcgScalars* h_s;  // pinned
+
+    void enqueue_iteration(cudaStream_t st) {
+        launch_spmv_dot<V>(G, grid_r, st, n, op, vals, p, q, partials, s);
+        update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
+        p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
+    }
+
+    // Runs until the device status leaves RUNNING; returns the status.
+    int iterate(int check_every) {
+        cudaStream_t st = ctx->stream;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        SVX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < check_every; ++k) enqueue_iteration(st);
+        cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        if (ce != cudaSuccess) throw CudaFail{ce, "cudaStreamEndCapture"};
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            throw CudaFail{ce, "cudaGraphInstantiate"};
+        }
+        int status = PCG_RUNNING;
+        try {
+            // the device stops at max_iter; the host bound only guards
+            // against a status that never leaves RUNNING
+            SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            SVX_CUDA(cudaStreamSynchronize(st));
+            const long long launches_max = h_s->max_iter / check_every + 2;
+            for (long long launch = 0;; ++launch) {
+                if (launch >= launches_max)
+                    throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                    "PCG status did not leave RUNNING within max_iter"};
+                SVX_CUDA(cudaGraphLaunch(exec, st));
+                SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+                SVX_CUDA(cudaStreamSynchronize(st));
+                status = h_s->status;
+                if (status != PCG_RUNNING) break;
+            }
+        } catch (...) {
+            cudaGraphExecDestroy(exec);
+            cudaGraphDestroy(graph);
+            throw;
+        }
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        return status;
+    }
+};
+
+struct PinnedScalars {
+    PcgScalars* h = nullptr;
+    PinnedScalars() { SVX_CUDA(cudaMallocHost(&h, sizeof(PcgScalars))); }
+    ~PinnedScalars() {
+        if (h) cudaFreeHost(h);
+    }
+};
+
+int auto_check_every(int64_t n, int64_t nnz) {
+    // ~30 us per iteration at C3D8 3.5M dofs vs ~5 us at 10k dofs: keep one
+    // host check per few hundred microseconds of device work.
+    (void)n;
+    if (nnz > 50000000) return 8;
+    if (nnz > 5000000) return 32;
+    return 64;
+}
+
+}  // namespace
+
+void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y) {
+    const int G = op->spmv_group;
+    unsigned grid = grid_rows(ctx, op->n, G);
+    cudaStream_t st = ctx->stream;
+    const int32_t* rp = op->pat.row_ptr.p;
+    const int32_t* ci = op->pat.col_idx.p;
+    switch (G) {
+        case 2: spmv_kernel<2><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
+        case 4: spmv_kernel<4><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
+        case 8: spmv_kernel<8><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
+        case 16: spmv_kernel<16><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
+        default: spmv_kernel<32><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
+    }
+    SVX_LAUNCH_CHECK();
+}
+
+int choose_spmv_group(const svx_op* op) {
+    double mean = op->n > 0 ? double(op->pat.nnz) / double(op->n) : 1.0;
+    return pick_group(mean);
+}
+
+PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int check_every,
+                   double* u_dev) {
+    const int64_t n = op->n;
+    cudaStream_t st = ctx->stream;
+    PcgResult out{PCG_CONVERGED, 0, 0.0, 0.0};
+    if (check_every <= 0) check_every = auto_check_every(n, op->pat.nnz);
+    DBuf<double> r, p, q, partials;
+    DBuf<PcgScalars> s;
+    r.alloc(ctx->pool, n + 1);
+    p.alloc(ctx->pool, n + 1);
+    q.alloc(ctx->pool, n + 1);
+    const int G = op->spmv_group;
+    PcgRun<double, double> run;
+    run.ctx = ctx;
+    run.op = op;
+    run.n = n;
+    run.G = G;
+    run.grid_r = grid_rows(ctx, n, G);
+    run.grid_v = grid_vec(ctx, n);
+    partials.alloc(ctx->pool, 2 * size_t(std::max(run.grid_r, run.grid_v)) + 2);
+    s.alloc(ctx->pool, 1);
+    PinnedScalars hs;
+    PcgScalars init{};
+    init.tol = tol;
+    init.max_iter = max_iter;
+    init.status = PCG_RUNNING;
+    SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+    init_kernel<double, double><<<run.grid_v, BLOCK, 0, st>>>(n, op->f.p, 1.0, u_dev, r.p, p.p,
+                                                             op->inv_diag.p, partials.p, s.p);
+    SVX_LAUNCH_CHECK();
+    run.vals = op->vals.p;
+    run.inv_diag = op->inv_diag.p;
+    run.u = u_dev;
+    run.r = r.p;
+    run.p = p.p;
+    run.q = q.p;
+    run.partials = partials.p;
+    run.s = s.p;
+    run.h_s = hs.h;
+    SVX_CUDA(cudaMemcpyAsync(hs.h, s.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    SVX_CUDA(cudaStreamSynchronize(st));
+    int status = hs.h->status;
+    if (status == PCG_RUNNING) status = run.iterate(check_every);
+    SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+    SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    out.status = status;
+    out.iterations = hs.h->it;
+    out.residual = hs.h->res;
+    out.ms = ms;
+    return out;
+}
+
+PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
+                    int check_every, double* u_dev, long long* outer_steps) {
+    const int64_t n = op->n;
+    cudaStream_t st = ctx->stream;
+    if (check_every <= 0) check_every = auto_check_every(n, op->pat.nnz);
+    const int G = op->spmv_group;
+    // FP32 copies of K and the Jacobi diagonal
+    if (!op->vals32.p) {
+        op->vals32.alloc(ctx->pool, op->pat.nnz + 1);
+        to_float_kernel<<<grid_vec(ctx, op->pat.nnz), BLOCK, 0, st>>>(op->pat.nnz, op->vals.p,
+                                                                       op->vals32.p);
+        SVX_LAUNCH_CHECK();
+    }
+    DBuf<float> inv32, r32, p32, q32, d32;
+    DBuf<double> r64, partials, rr_dev;
+    DBuf<PcgScalars> s;
+    DBuf<unsigned int> counter;
+    inv32.alloc(ctx->pool, n + 1);
+    r32.alloc(ctx->pool, n + 1);
+    p32.alloc(ctx->pool, n + 1);
+    q32.alloc(ctx->pool, n + 1);
+    d32.alloc(ctx->pool, n + 1);
+    r64.alloc(ctx->pool, n + 1);
+    rr_dev.alloc(ctx->pool, 1);
+    counter.alloc(ctx->pool, 1);
+    SVX_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned int), st));
+    to_float_kernel<<<grid_vec(ctx, n), BLOCK, 0, st>>>(n, op->inv_diag.p, inv32.p);
+    SVX_LAUNCH_CHECK();
+    PcgRun<float, float> run;
+    run.ctx = ctx;
+    run.op = op;
+    run.n = n;
+    run.G = G;
+    run.grid_r = grid_rows(ctx, n, G);
+    run.grid_v = grid_vec(ctx, n);
+    partials.alloc(ctx->pool, 2 * size_t(std::max(run.grid_r, run.grid_v)) + 2);
+    s.alloc(ctx->pool, 1);
+    PinnedScalars hs;
+    run.vals = op->vals32.p;
+    run.inv_diag = inv32.p;
+    run.u = d32.p;
+    run.r = r32.p;
+    run.p = p32.p;
+    run.q = q32.p;
+    run.partials = partials.p;
+    run.s = s.p;
+    run.h_s = hs.h;
+
+    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+    SVX_CUDA(cudaMemsetAsync(u_dev, 0, n * sizeof(double), st));
+    // ||f||
+    double* h_rr = &hs.h->rr;  // scratch slot of the pinned struct
+    auto true_residual = [&]() -> double {
+        unsigned grid = grid_rows(ctx, n, G);
+        const int32_t* rp = op->pat.row_ptr.p;
+        const int32_t* ci = op->pat.col_idx.p;
+        switch (G) {
+            case 2: residual_kernel<2><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
+            case 4: residual_kernel<4><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
+            case 8: residual_kernel<8><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
+            case 16: residual_kernel<16><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
+            default: residual_kernel<32><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
+        }
+        SVX_LAUNCH_CHECK();
+        SVX_CUDA(cudaMemcpyAsync(h_rr, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        return *h_rr;
+    };
+    double ff = true_residual();  // u = 0: r = f
+    double bnorm = std::sqrt(ff);
+    PcgResult out{PCG_CONVERGED, 0, 0.0, 0.0};
+    long long total_inner = 0, outer = 0;
+    double res = bnorm == 0.0 ? 0.0 : 1.0;
+    double rnorm = bnorm;
+    int status = PCG_CONVERGED;
+    const int max_outer = 200;
+    while (bnorm != 0.0) {
+        if (res <= tol) {
+            status = PCG_CONVERGED;
+            break;
+        }
+        if (outer >= max_outer || total_inner >= max_iter) {
+            status = PCG_MAXITER;
+            break;
+        }
+        ++outer;
+        // inner solve K32 d = r / ||r|| in FP32 with FP64 dots
+        PcgScalars init{};
+        init.tol = inner_tol;
+        init.max_iter = std::max<long long>(1, max_iter - total_inner);
+        init.status = PCG_RUNNING;
+        SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+        init_kernel<float, double><<<run.grid_v, BLOCK, 0, st>>>(
+            n, r64.p, 1.0 / rnorm, d32.p, r32.p, p32.p, inv32.p, partials.p, s.p);
+        SVX_LAUNCH_CHECK();
+        int inner_status = run.iterate(check_every);
+        total_inner += hs.h->it;
+        if (inner_status == PCG_BREAKDOWN && hs.h->it <= 1) {
+            status = PCG_BREAKDOWN;
+            break;
+        }
+        correct_kernel<<<run.grid_v, BLOCK, 0, st>>>(n, u_dev, d32.p, rnorm);
+        SVX_LAUNCH_CHECK();
+        double rr = true_residual();
+        double new_norm = std::sqrt(rr);
+        double new_res = new_norm / bnorm;
+        if (!(new_res < res)) {  // no progress: the FP32 operator cannot refine further
+            res = new_res;
+            rnorm = new_norm;
+            status = (new_res <= tol) ? PCG_CONVERGED : PCG_BREAKDOWN;
+            break;
+        }
+        res = new_res;
+        rnorm = new_norm;
+    }
+    SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+    SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    out.status = status;
+    out.iterations = total_inner;
+    out.residual = res;
+    out.ms = ms;
+    if (outer_steps) *outer_steps = outer;
+    return out;
+}
+
+}  // namespace svx

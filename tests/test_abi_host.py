@@ -1,0 +1,234 @@
+"""CPU tests of the C ABI library: it loads, exports every symbol the public
+header declares, and its host-side model resolution (svx_resolve, no GPU
+needed) matches the oracle's restatement of the reference's lookups and
+error order."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from solvix_b200 import abi
+from solvix_b200.marshal import FlatModel, model_desc
+from solvix_b200.model import (BoundaryCondition, ConcentratedLoad, ElemKind, Element,
+                               ElementSet, InvalidModel, Material, Mesh, Model, Node,
+                               NoConstraints, SolveError)
+from svx_cases import cantilever_deck, hex_mesh, load_golden, patch_deck, quad_mesh, steel_model
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "solvix_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(svx_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.load()
+    syms = header_symbols()
+    assert len(syms) >= 19
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    # and the ctypes signature table covers the same set
+    assert sorted(abi.SIGNATURES) == syms
+
+
+def test_version_string():
+    assert b"sm_100a" in abi.load().svx_version()
+
+
+def test_no_device_is_a_loud_error():
+    """Without a CUDA device the compute entry points refuse (no CPU path)."""
+    lib = abi.load()
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("a CUDA device is present")
+    h = C.c_void_p()
+    assert lib.svx_ctx_create(0, C.byref(h)) == abi.SVX_CUDA_ERROR
+    buf = C.create_string_buffer(512)
+    lib.svx_last_error(None, buf, 512)
+    assert buf.value
+
+
+def product_resolve(model):
+    """svx_resolve -> (FlatModel, pending status, pending message)."""
+    lib = abi.load()
+    desc, keep = model_desc(model)
+    res = C.c_void_p()
+    err = abi.SvxError()
+    st = lib.svx_resolve(C.byref(desc), C.byref(res), C.byref(err))
+    if st != abi.SVX_OK:
+        return None, st, err.message.decode()
+    try:
+        flat = FlatModel.from_struct(lib.svx_resolved_flat(res).contents)
+    finally:
+        lib.svx_resolved_free(res)
+    return flat, st, ""
+
+
+def oracle_resolve(model):
+    try:
+        flat, pending = oracle.resolve(model)
+    except SolveError as e:
+        code = abi.SVX_NO_CONSTRAINTS if isinstance(e, NoConstraints) else abi.SVX_INVALID_MODEL
+        return None, code, str(e)
+    return flat, pending, None
+
+
+def assert_same_flat(a: FlatModel, b: FlatModel):
+    assert a.ndof == b.ndof and a.thickness == b.thickness
+    for name in ("xyz", "kind", "conn_ptr", "conn", "youngs", "poisson", "f", "no_material",
+                 "node_id", "elem_id"):
+        x, y = getattr(a, name), getattr(b, name)
+        assert np.array_equal(np.asarray(x), np.asarray(y)), name
+
+
+@pytest.mark.parametrize("name", ["cantilever", "cantilever3d", "plate_hole"])
+def test_resolve_matches_oracle_on_golden_decks(name):
+    model, _ = load_golden(name)
+    fp, st, _ = product_resolve(model)
+    fo, pending, _ = oracle_resolve(model)
+    assert st == abi.SVX_OK and pending is None
+    assert_same_flat(fp, fo)
+    assert np.array_equal(fp.fixed_row, fo.fixed_row)
+
+
+def test_resolve_duplicate_ids_and_first_assignment_wins():
+    """node_index takes the first node with an id (lib.rs:106-108); the first
+    assignment whose set holds the element decides, even with no material
+    of that name (lib.rs:357-367)."""
+    m = steel_model(quad_mesh(3, 1, 3.0, 1.0))
+    m.materials = [Material("a", 1e9, 0.2), Material("b", 2e9, 0.3), Material("a", 5e9, 0.1)]
+    m.elsets = [ElementSet("s1", [2]), ElementSet("s2", [1, 2, 3]), ElementSet("s1", [3]),
+                ElementSet("ghost", [1])]
+    m.mat_assignments = [("s1", "missing"), ("s2", "b"), ("nope", "a")]
+    m.boundary_conditions = [BoundaryCondition([1, 5], [1, 2])]
+    m.cloads = [ConcentratedLoad(4, 2, -1.0), ConcentratedLoad(4, 2, -2.0)]
+    fp, st, _ = product_resolve(m)
+    fo, pending, _ = oracle_resolve(m)
+    assert st == abi.SVX_OK and pending is None
+    assert_same_flat(fp, fo)
+    assert list(fp.no_material) == [0, 1, 0]
+    assert fp.f[(4 - 1) * 2 + 1] == -3.0
+
+
+ERROR_CASES = []
+
+
+def _case(fn):
+    ERROR_CASES.append(fn)
+    return fn
+
+
+@_case
+def free_body():
+    return steel_model(quad_mesh(2, 1, 2.0, 1.0))
+
+
+@_case
+def empty_mesh():
+    m = Model(materials=[Material("s", 1.0, 0.3)])
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def no_material():
+    m = steel_model(quad_mesh(2, 1, 2.0, 1.0))
+    m.materials = []
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def malformed_element():
+    mesh = Mesh([Node(1, (0, 0, 0)), Node(2, (1, 0, 0)), Node(3, (1, 1, 0))],
+                [Element(7, ElemKind.Cps4, [1, 2, 3])])
+    m = steel_model(mesh)
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def unknown_node():
+    mesh = Mesh([Node(1, (0, 0, 0)), Node(2, (1, 0, 0)), Node(3, (1, 1, 0))],
+                [Element(1, ElemKind.Cps3, [1, 2, 42])])
+    m = steel_model(mesh)
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def bad_thickness():
+    m = steel_model(quad_mesh(1, 1, 1.0, 1.0), thickness=0.0)
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def mixed_dimensionality():
+    mesh = hex_mesh(1, 1, 1, 1, 1, 1)
+    quad = Mesh([Node(100, (0, 0, 5)), Node(101, (1, 0, 5)), Node(102, (1, 1, 5)),
+                 Node(103, (0, 1, 5))], [Element(50, ElemKind.Cps4, [100, 101, 102, 103])])
+    mesh = Mesh(mesh.nodes + quad.nodes, mesh.elements + quad.elements)
+    m = steel_model(mesh)
+    m.boundary_conditions = [BoundaryCondition([1], [1])]
+    return m
+
+
+@_case
+def cload_bad_dof():
+    m = cantilever_deck(4, 1)
+    m.cloads = [ConcentratedLoad(5, 3, 1.0)]
+    return m
+
+
+@_case
+def cload_unknown_node():
+    m = cantilever_deck(4, 1)
+    m.cloads = [ConcentratedLoad(500, 1, 1.0)]
+    return m
+
+
+@_case
+def bc_unknown_node():
+    m = cantilever_deck(4, 1)
+    m.boundary_conditions = [BoundaryCondition([1, 600], [1])]
+    return m
+
+
+@_case
+def bc_bad_dof():
+    m = cantilever_deck(4, 1)
+    m.boundary_conditions = [BoundaryCondition([1], [1, 0])]
+    return m
+
+
+@pytest.mark.parametrize("case", ERROR_CASES, ids=[f.__name__ for f in ERROR_CASES])
+def test_resolve_errors_match_oracle(case):
+    model = case()
+    fp, st, msg = product_resolve(model)
+    fo, ost, omsg = oracle_resolve(model)
+    if fo is None:  # raised before assembly
+        assert st == ost and msg == omsg
+    else:
+        assert st == abi.SVX_OK
+        if ost is None:
+            assert_same_flat(fp, fo)
+    if fo is not None and ost is not None:
+        # pending error: the oracle raises it after assembly
+        with pytest.raises(InvalidModel) as ei:
+            oracle.solve(model)
+        assert str(ei.value) == str(ost.err)
+
+
+def test_patch_deck_resolves():
+    fp, st, _ = product_resolve(patch_deck())
+    assert st == abi.SVX_OK and list(fp.fixed_row) == [0, 14, 6, 1]
