@@ -96,6 +96,13 @@ __device__ __forceinline__ double row_dot(const int32_t* __restrict__ col_idx,
     return acc0 + acc1;
 }
 
+// First row of this warp's 32/G row groups in the block-strided loop; it is
+// the same for all lanes of the warp.
+template <int G>
+__device__ __forceinline__ int64_t warp_first_row(int64_t groups_per_block) {
+    return int64_t(blockIdx.x) * groups_per_block + int64_t(threadIdx.x >> 5) * (32 / G);
+}
+
 // q = K p and per-block partial of p.q; the last block forms pap and alpha.
 template <int G, class V>
 __global__ void __launch_bounds__(BLOCK)
@@ -108,12 +115,15 @@ spmv_dot_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
     const int gl = threadIdx.x & (G - 1);
     const int64_t groups_per_block = BLOCK / G;
     double dot = 0.0;
-    for (int64_t r = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; r < n;
-         r += int64_t(gridDim.x) * groups_per_block) {
-        double v = row_dot<G, V>(col_idx, vals, p, row_ptr[r], row_ptr[r + 1], gl);
+    // warp-uniform trip count: every lane reaches the shuffles together
+    for (int64_t rb = warp_first_row<G>(groups_per_block); rb < n;
+         rb += int64_t(gridDim.x) * groups_per_block) {
+        const int64_t r = rb + ((threadIdx.x & 31) / G);
+        const bool valid = r < n;
+        double v = valid ? row_dot<G, V>(col_idx, vals, p, row_ptr[r], row_ptr[r + 1], gl) : 0.0;
 #pragma unroll
         for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (gl == 0) {
+        if (valid && gl == 0) {
             V qv = V(v);
             q[r] = qv;
             dot += double(p[r]) * double(qv);
@@ -255,12 +265,15 @@ spmv_kernel(int64_t n, const int32_t* __restrict__ row_ptr, const int32_t* __res
             double* __restrict__ y) {
     const int gl = threadIdx.x & (G - 1);
     const int64_t groups_per_block = BLOCK / G;
-    for (int64_t r = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; r < n;
-         r += int64_t(gridDim.x) * groups_per_block) {
-        double v = row_dot<G, double>(col_idx, vals, x, row_ptr[r], row_ptr[r + 1], gl);
+    for (int64_t rb = warp_first_row<G>(groups_per_block); rb < n;
+         rb += int64_t(gridDim.x) * groups_per_block) {
+        const int64_t r = rb + ((threadIdx.x & 31) / G);
+        const bool valid = r < n;
+        double v =
+            valid ? row_dot<G, double>(col_idx, vals, x, row_ptr[r], row_ptr[r + 1], gl) : 0.0;
 #pragma unroll
         for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (gl == 0) y[r] = v;
+        if (valid && gl == 0) y[r] = v;
     }
 }
 
@@ -276,12 +289,15 @@ residual_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
     const int gl = threadIdx.x & (G - 1);
     const int64_t groups_per_block = BLOCK / G;
     double rr = 0.0;
-    for (int64_t i = int64_t(blockIdx.x) * groups_per_block + threadIdx.x / G; i < n;
-         i += int64_t(gridDim.x) * groups_per_block) {
-        double v = row_dot<G, double>(col_idx, vals, u, row_ptr[i], row_ptr[i + 1], gl);
+    for (int64_t rb = warp_first_row<G>(groups_per_block); rb < n;
+         rb += int64_t(gridDim.x) * groups_per_block) {
+        const int64_t i = rb + ((threadIdx.x & 31) / G);
+        const bool valid = i < n;
+        double v =
+            valid ? row_dot<G, double>(col_idx, vals, u, row_ptr[i], row_ptr[i + 1], gl) : 0.0;
 #pragma unroll
         for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (gl == 0) {
+        if (valid && gl == 0) {
             double ri = f[i] - v;
             r[i] = ri;
             rr += ri * ri;
