@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the linear-static hot path on B200.
+
+One step is one full linear-static solve of the 160 x 16 x 16 C3D8
+cantilever (139,587 DOF, 10,393,929 nonzeros, seeded interior jitter): element
+integration, CSR assembly, Dirichlet, FP64 Jacobi-PCG to a relative residual
+of 1e-10 and von Mises / reaction recovery.
+
+* ``value`` - PCG DOF.iterations per second of whole solves whose inputs are
+  already resident in HBM (svx_op_reassemble + svx_op_solve on the device
+  copy of the model), timed with CUDA events on the library's stream.
+* ``e2e`` - the same metric through the public C ABI call a user makes
+  (svx_solve_flat) from pinned host buffers: the model's H2D copy and the
+  D2H read of u, displacements, von Mises and reactions are inside the
+  timed region.
+* ``roofline`` - the SpMV kernel (spmv_dot) against the measured HBM copy
+  peak, from its algorithmic bytes and its live CUDA-event duration.
+* ``cpu_baseline`` - the oracle (the C++ restatement of the reference's
+  Rust path) solving the same model on the host cores.
+
+``--impl reference`` times only the oracle port on the host cores (rank 0).
+Multi-GPU runs (torchrun) solve independent replicas per GPU ("replicas
+only": the plain solve does not shard); ``value`` sums all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PCG DOF-iters/s & solves/s: mixed/batched vs FP64 at 1e-8 err; p50/p99 ms"
+UNIT = "DOF*iter/s"
+HBM_FALLBACK_GBS = 6650.0
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_dot_fp64_c3d8_160x16x16.txt")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from solvix_b200 import workloads
+    return workloads.cantilever_c3d8(160, 16, 16)
+
+
+WORKLOAD_NAME = ("C3D8 cantilever 160x16x16 over 2.0x0.2x0.2 m (46,529 nodes, 139,587 DOF, "
+                 "10,393,929 nnz), jitter +-0.1h seed 2, E=70e9, nu=0.33, x=0 clamped, -5 kN "
+                 "in z over the x=L face; FP64 assembly + Jacobi-PCG to 1e-10 + stress")
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per spmv_dot launch from the committed ncu summary."""
+    try:
+        with open(TRAFFIC_FILE) as fh:
+            for line in fh:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return int(float(line.split(":", 1)[1].strip()))
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if r[4 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(flat, iterations_hint=None):
+    """The oracle's full solve of the same model on min(8, cores) threads."""
+    from oracle import oracle
+    threads = oracle.default_threads()
+    t0 = time.perf_counter()
+    ref = oracle.solve_flat(flat, threads=threads)
+    dt = time.perf_counter() - t0
+    n = flat.n_dof
+    return {
+        "value": n * ref.iterations / dt, "unit": UNIT, "cores": threads, "kind": "port",
+        "sample": (f"one full oracle solve of the same model (assembly, {ref.iterations} "
+                   f"PCG iterations, stress) on {threads} threads in {dt:.2f} s "
+                   f"(host: {os.cpu_count()} cores)"),
+        "solves_per_s": 1.0 / dt,
+    }
+
+
+def pinned_like(a):
+    import numpy as np
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    out = t.numpy().view(a.dtype).reshape(a.shape)
+    np.copyto(out, a)
+    return out, t
+
+
+def run_reference(args, rank):
+    """--impl reference: the oracle port on the host cores, rank 0 only."""
+    if rank != 0:
+        return None
+    flat = workload()
+    from oracle import oracle
+    oracle.build()
+    for _ in range(max(0, args.warmup)):
+        cpu_baseline(flat)
+    vals, times = [], []
+    for _ in range(args.steps):
+        cb = cpu_baseline(flat)
+        vals.append(cb["value"])
+        times.append(1.0 / cb["solves_per_s"])
+    value = len(times) * flat.n_dof * (vals[0] * times[0] / flat.n_dof) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": WORKLOAD_NAME, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solves_per_s": 1.0 / (sum(times) / len(times)),
+        "note": ("the reference is Rust and no Rust toolchain exists here or on the GPU box; "
+                 "the arm times the C++ restatement (oracle/) that reproduces the reference's "
+                 "published iteration counts and residuals bit for bit"),
+    }
+    return line
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, abi
+    from solvix_b200.marshal import FlatModel
+
+    torch.cuda.set_device(local_rank)
+    precision = abi.SVX_MIXED if args.precision == "mixed" else abi.SVX_FP64
+    flat = workload()
+    n = flat.n_dof
+    ctx = Context(local_rank)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
+    op = ctx.assemble(flat)
+    nnz = op.nnz
+
+    def step():
+        op.reassemble()
+        return op.solve_device(precision=precision, want_stress=True)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    # flush L2 before the timed region (the per-step working set, K + Ke
+    # ~ 315 MB, is larger than the 126 MB L2 on its own)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    with torch.cuda.stream(stream):
+        flush.fill_(1)
+    del flush
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = lib.svx_launch_count()
+    ev0.record(stream)
+    iters = []
+    ms_parts = np.zeros(3)
+    for _ in range(args.steps):
+        it, res, ms_s, ms_st, ms_a = step()
+        iters.append(it)
+        ms_parts += [ms_a, ms_s, ms_st]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.svx_launch_count() - launches0
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    ms_max = float(ms_t.item())
+    dof_iters = float(np.sum(iters)) * n
+    value = world * dof_iters / (ms_max / 1000.0)
+
+    # roofline of the SpMV: algorithmic bytes / live CUDA-event duration
+    kms = op.time_kernels(reps=50)
+    spmv_bytes = nnz * (8 + 4) + 4 * (n + 1) + 2 * 8 * n
+    achieved = spmv_bytes / (kms[0] / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic()
+
+    # e2e: the public C ABI call from pinned host memory
+    keep = []
+    pinned = {}
+    for name in ("xyz", "kind", "conn_ptr", "conn", "youngs", "poisson", "fixed_row", "f",
+                 "node_id", "elem_id"):
+        a = getattr(flat, name)
+        if a is None:
+            continue
+        pa, t = pinned_like(np.ascontiguousarray(a))
+        keep.append(t)
+        pinned[name] = pa
+    pflat = FlatModel(thickness=flat.thickness, ndof=flat.ndof, **pinned)
+    outs = {}
+    for name, shape in (("u", (n,)), ("disp", (flat.n_nodes, 3)), ("vm", (flat.n_elem,)),
+                        ("vmn", (flat.n_nodes,)), ("react", (flat.fixed_row.shape[0],))):
+        pa, t = pinned_like(np.zeros(shape))
+        keep.append(t)
+        outs[name] = pa
+    sol = abi.SvxSolution()
+    sol.u = abi.ptr(outs["u"], C.c_double)
+    sol.displacements = abi.ptr(outs["disp"], C.c_double)
+    sol.von_mises = abi.ptr(outs["vm"], C.c_double)
+    sol.nodal_von_mises = abi.ptr(outs["vmn"], C.c_double)
+    sol.reactions = abi.ptr(outs["react"], C.c_double)
+    opts = abi.default_opts(precision=precision)
+    err = abi.SvxError()
+    s = pflat.as_struct()
+    h2d = pflat.nbytes()
+    d2h = sum(a.nbytes for a in outs.values())
+
+    def e2e_step():
+        st = lib.svx_solve_flat(ctx.handle, C.byref(s), C.byref(opts), C.byref(sol),
+                                C.byref(err))
+        if st != abi.SVX_OK:
+            raise RuntimeError(err.message.decode())
+        return int(sol.iterations)
+
+    e2e_step()
+    e2e_steps = max(3, min(args.steps, 10))
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e_iters = 0
+    for _ in range(e2e_steps):
+        e_iters += e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if world > 1:
+        torch.distributed.all_reduce(e_ms, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * e_iters * n / (float(e_ms.item()) / 1000.0)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32/f64",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": WORKLOAD_NAME, "n_dof": n, "nnz": nnz,
+                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (K 125 MB + Ke 189 MB per step vs 126 MB L2); "
+                         "L2 flushed before the timed region"},
+        "solves_per_s": world * args.steps / (ms_max / 1000.0),
+        "iterations": int(iters[-1]),
+        "ms_breakdown": {"assemble": ms_parts[0] / args.steps, "pcg": ms_parts[1] / args.steps,
+                         "stress": ms_parts[2] / args.steps},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                "solves_per_s": world * e2e_steps / (float(e_ms.item()) / 1000.0)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "spmv_dot (FP64 CSR SpMV + p.Kp)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": int(spmv_bytes),
+                     "launch_ms": float(kms[0]),
+                     "traffic": traffic,
+                     "other_kernels_ms": {"update": float(kms[1]), "p_update": float(kms[2])}},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(flat)
+        line["cpu_baseline"].pop("solves_per_s", None)
+    op.free()
+    ctx.close()
+    return line
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -201,6 +201,9 @@ void svx_default_opts(svx_solve_opts_t* opts);
 /* ---- context ----------------------------------------------------- */
 int svx_ctx_create(int device, svx_ctx_t** out);
 int svx_ctx_destroy(svx_ctx_t* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own
+ * work or timing events with the library's. */
+void* svx_ctx_stream(svx_ctx_t* ctx);
 /* Copies the last error message of `ctx` (or of the calling thread when
  * ctx is NULL) into buf. */
 int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len);
@@ -228,6 +231,10 @@ enum svx_assemble_flags {
 int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, uint32_t flags,
                  svx_op_t** out, svx_error_t* err);
 int svx_op_free(svx_op_t* op);
+/* Re-runs element integration, assembly and Dirichlet from the operator's
+ * device-resident model (the pattern is kept): the whole K1-K4 path with
+ * no host traffic. */
+int svx_op_reassemble(svx_op_t* op, svx_error_t* err);
 /* CSR sizes of an assembled operator. */
 int svx_op_dims(const svx_op_t* op, int64_t* n_rows, int64_t* nnz);
 /* Copies the CSR to host arrays of n+1 / nnz / nnz entries (any may be
@@ -245,15 +252,28 @@ int svx_op_spmv(svx_op_t* op, const double* x, double* y);
 int svx_op_set_solution(svx_op_t* op, const double* u);
 
 /* ---- K5-K7: PCG --------------------------------------------------- */
-/* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644). */
+/* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644);
+ * with opts->want_stress also K9-K10 (device-side, copied to the non-NULL
+ * arrays of sol). */
 int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol,
                  svx_error_t* err);
 
 /* ---- K9-K10: stress + reactions ----------------------------------- */
-/* Uses the operator's last solution (svx_op_solve).  Replaces
+/* svx_op_solve with opts->want_stress = 1 also recovers the stresses into
+ * device buffers (copied out only where sol's arrays are non-NULL).
+ * svx_op_stress uses the operator's last solution (svx_op_solve).  Replaces
  * stress::{von_mises_at_centroids, nodal_von_mises, reactions}
  * (stress.rs:22-118) and the displacement packaging of lib.rs:689-698. */
 int svx_op_stress(svx_op_t* op, svx_solution_t* sol);
+
+/* ---- measurement --------------------------------------------------- */
+/* Kernels this process has launched through the library (graph nodes count
+ * when their graph is launched). */
+int64_t svx_launch_count(void);
+/* Average device time in ms of the three FP64 PCG iteration kernels of an
+ * operator (ms3[0] = SpMV + p.Kp, ms3[1] = u/r update + dots, ms3[2] = p
+ * update), each over `reps` back-to-back launches on the context stream. */
+int svx_op_time_kernels(svx_op_t* op, int reps, double* ms3);
 
 /* ---- one-call pipelines -------------------------------------------- */
 /* Whole linear-static path for a flat model: lib.rs:614-703. */

@@ -154,6 +154,10 @@ SIGNATURES = {
     "svx_default_opts": (None, [C.POINTER(SvxSolveOpts)]),
     "svx_ctx_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
     "svx_ctx_destroy": (C.c_int, [_VP]),
+    "svx_ctx_stream": (C.c_void_p, [_VP]),
+    "svx_op_reassemble": (C.c_int, [_VP, C.POINTER(SvxError)]),
+    "svx_launch_count": (C.c_int64, []),
+    "svx_op_time_kernels": (C.c_int, [_VP, C.c_int, c_double_p]),
     "svx_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
     "svx_resolve": (C.c_int, [C.POINTER(SvxModelDesc), C.POINTER(_VP), C.POINTER(SvxError)]),
     "svx_resolved_flat": (C.POINTER(SvxFlatModel), [_VP]),

@@ -49,6 +49,11 @@ class Context:
         self.handle = h
         self.device = device
 
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        return int(self.lib.svx_ctx_stream(self.handle) or 0)
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.svx_ctx_destroy(self.handle)
@@ -215,13 +220,44 @@ class Operator:
         if st != abi.SVX_OK:
             _raise(st, None, "svx_op_set_solution failed")
 
+    def time_kernels(self, reps: int = 50):
+        """(spmv_dot, update, p_update) average device ms per launch."""
+        ms = np.zeros(3)
+        st = self.lib.svx_op_time_kernels(self.handle, int(reps), abi.ptr(ms, C.c_double))
+        if st != abi.SVX_OK:
+            _raise(st, None, "svx_op_time_kernels failed")
+        return ms
+
+    def reassemble(self):
+        """Re-run K1-K4 from the device-resident model (no host traffic)."""
+        err = abi.SvxError()
+        st = self.lib.svx_op_reassemble(self.handle, C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+
+    def solve_device(self, tol=1e-10, max_iter=0, precision=abi.SVX_FP64, inner_tol=1e-5,
+                     want_stress=True, check_every=0):
+        """Solve (and recover stresses) leaving every result on the device;
+        returns (iterations, residual, ms_solve, ms_stress, ms_assemble) with
+        ms_assemble the device time of the operator's last assembly."""
+        sol = abi.SvxSolution()
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
+                                inner_tol=inner_tol, check_every=check_every,
+                                want_stress=int(want_stress))
+        err = abi.SvxError()
+        st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        return int(sol.iterations), float(sol.final_residual), float(sol.ms_solve), \
+            float(sol.ms_stress), float(sol.ms_assemble)
+
     def solve(self, tol=1e-10, max_iter=0, precision=abi.SVX_FP64, inner_tol=1e-5,
               check_every=0):
         u = np.zeros(self.n)
         sol = abi.SvxSolution()
         sol.u = abi.ptr(u, C.c_double)
         opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
-                                inner_tol=inner_tol, check_every=check_every)
+                                inner_tol=inner_tol, check_every=check_every, want_stress=0)
         err = abi.SvxError()
         st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
         if st != abi.SVX_OK:

@@ -230,6 +230,37 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
+// K1-K4 from the operator's device-resident model: element integration,
+// pattern, fixed-order assembly and Dirichlet.  Needs no host model.
+void device_assemble(svx_ctx* ctx, svx_op* op) {
+    cudaStream_t st = ctx->stream;
+    SVX_CUDA(cudaEventRecord(ctx->ev[2], st));
+    DBuf<double> ke;
+    ke.alloc(ctx->pool, size_t(op->n_elem) * op->pat.ke_stride + 1);
+    uint64_t g = integrate_elements(ctx, op, ke.p, op->pat.ke_stride);
+    if (g != ~uint64_t(0)) {
+        int64_t g_fail = int64_t(g >> 8);
+        int g_reason = int(g & 0xff);
+        throw ModelFail{SVX_INVALID_MODEL, g_reason, g_fail,
+                        "element " + std::to_string(op->h_elem_id[g_fail]) + ": " +
+                            reason_text(g_reason)};
+    }
+    if (!op->pat.row_ptr.p) build_pattern(ctx, op);
+    op->vals.alloc(ctx->pool, op->pat.nnz + 1);
+    assemble_values(ctx, op, ke.p, op->pat.ke_stride, op->vals.p);
+    ke.reset();
+    if (op->flags & SVX_KEEP_ORIGINAL) {
+        op->vals_orig.alloc(ctx->pool, op->pat.nnz + 1);
+        SVX_CUDA(cudaMemcpyAsync(op->vals_orig.p, op->vals.p, op->pat.nnz * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st));
+    }
+    op->vals32.reset();
+    apply_dirichlet(ctx, op);
+    op->spmv_group = choose_spmv_group(op);
+    SVX_CUDA(cudaEventRecord(ctx->ev[3], st));
+    op->ms_assemble = elapsed_ms(ctx->ev[2], ctx->ev[3]);
+}
+
 // K1-K4 for a validated flat model; throws ModelFail for element errors.
 svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
     SVX_CUDA(cudaSetDevice(ctx->device));
@@ -267,8 +298,9 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
     op->ndof = m->ndof;
     op->n = m->n_nodes * m->ndof;
     op->thickness = m->thickness;
+    op->flags = flags;
     cudaStream_t st = ctx->stream;
-    SVX_CUDA(cudaEventRecord(ctx->ev[2], st));
+    SVX_CUDA(cudaEventRecord(ctx->ev[6], st));
     upload(ctx, op->xyz, m->xyz, size_t(3 * m->n_nodes));
     upload(ctx, op->kind, m->kind, size_t(op->n_elem));
     upload(ctx, op->conn_ptr, m->conn_ptr, size_t(op->n_elem + 1));
@@ -280,28 +312,20 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
     op->pat.max_nn = std::max(max_nn, 1);
     const int max_N = max_nn * m->ndof;
     op->pat.ke_stride = std::max(1, max_N * max_N);
-
-    // K1: element integration (only up to a material failure)
-    DBuf<double> ke;
-    ke.alloc(ctx->pool, size_t(op->n_elem) * op->pat.ke_stride + 1);
-    uint64_t g = integrate_elements(ctx, op.get(), ke.p, op->pat.ke_stride);
-    int64_t g_fail = (g == ~uint64_t(0)) ? -1 : int64_t(g >> 8);
-    int g_reason = int(g & 0xff);
-    if (g_fail >= 0) {
-        throw ModelFail{SVX_INVALID_MODEL, g_reason, g_fail, element_message(m, g_fail, g_reason)};
-    }
+    op->h_elem_id.resize(size_t(op->n_elem));
+    for (int64_t e = 0; e < op->n_elem; ++e) op->h_elem_id[e] = elem_id_of(m, e);
     if (m_fail >= 0) {
+        // only the elements before the first material failure can fail first
+        DBuf<double> ke;
+        ke.alloc(ctx->pool, size_t(op->n_elem) * op->pat.ke_stride + 1);
+        uint64_t g = integrate_elements(ctx, op.get(), ke.p, op->pat.ke_stride);
+        if (g != ~uint64_t(0)) {
+            int64_t g_fail = int64_t(g >> 8);
+            int g_reason = int(g & 0xff);
+            throw ModelFail{SVX_INVALID_MODEL, g_reason, g_fail,
+                            element_message(m, g_fail, g_reason)};
+        }
         throw ModelFail{SVX_INVALID_MODEL, m_reason, m_fail, element_message(m, m_fail, m_reason)};
-    }
-    // K3 pattern, K2 fixed-order assembly
-    build_pattern(ctx, op.get());
-    op->vals.alloc(ctx->pool, op->pat.nnz + 1);
-    assemble_values(ctx, op.get(), ke.p, op->pat.ke_stride, op->vals.p);
-    ke.reset();
-    if (flags & SVX_KEEP_ORIGINAL) {
-        op->vals_orig.alloc(ctx->pool, op->pat.nnz + 1);
-        SVX_CUDA(cudaMemcpyAsync(op->vals_orig.p, op->vals.p, op->pat.nnz * sizeof(double),
-                                 cudaMemcpyDeviceToDevice, st));
     }
     // loads and constraints
     std::vector<double> f(size_t(op->n), 0.0);
@@ -313,12 +337,35 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
     op->h_node_id.resize(size_t(m->n_nodes));
     for (int64_t i = 0; i < m->n_nodes; ++i)
         op->h_node_id[i] = m->node_id ? m->node_id[i] : uint32_t(i + 1);
-    // K4
-    apply_dirichlet(ctx, op.get());
-    op->spmv_group = choose_spmv_group(op.get());
-    SVX_CUDA(cudaEventRecord(ctx->ev[3], st));
-    op->ms_assemble = elapsed_ms(ctx->ev[2], ctx->ev[3]);
+    device_assemble(ctx, op.get());
+    SVX_CUDA(cudaEventRecord(ctx->ev[7], st));
+    op->ms_upload_assemble = elapsed_ms(ctx->ev[6], ctx->ev[7]);
     return op.release();
+}
+
+void stress_to_device(svx_op* op) {
+    svx_ctx* ctx = op->ctx;
+    if (!op->vm_elem.p) op->vm_elem.alloc(ctx->pool, op->n_elem + 1);
+    if (!op->vm_node.p) op->vm_node.alloc(ctx->pool, op->n_nodes + 1);
+    if (!op->react.p) op->react.alloc(ctx->pool, op->n_fixed + 1);
+    if (!op->disp3.p) op->disp3.alloc(ctx->pool, 3 * op->n_nodes + 1);
+    recover_stress(ctx, op, op->u.p, op->vm_elem.p, op->vm_node.p, op->react.p, op->disp3.p);
+}
+
+void copy_stress_out(svx_op* op, svx_solution_t* sol) {
+    cudaStream_t st = op->ctx->stream;
+    if (sol->von_mises && op->n_elem)
+        SVX_CUDA(cudaMemcpyAsync(sol->von_mises, op->vm_elem.p, op->n_elem * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    if (sol->nodal_von_mises && op->n_nodes)
+        SVX_CUDA(cudaMemcpyAsync(sol->nodal_von_mises, op->vm_node.p,
+                                 op->n_nodes * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (sol->reactions && op->n_fixed)
+        SVX_CUDA(cudaMemcpyAsync(sol->reactions, op->react.p, op->n_fixed * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    if (sol->displacements && op->n_nodes)
+        SVX_CUDA(cudaMemcpyAsync(sol->displacements, op->disp3.p,
+                                 3 * op->n_nodes * sizeof(double), cudaMemcpyDeviceToHost, st));
 }
 
 long long default_max_iter(int64_t n) { return std::max<long long>(1000, 10 * (long long)n); }
@@ -361,29 +408,14 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
         ctx->last_error = msg;
         return SVX_NOT_CONVERGED;
     }
-    if (sol && opts.want_stress) {
+    if (opts.want_stress) {
         SVX_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
-        DBuf<double> vm_e, vm_n, react, disp;
-        if (sol->von_mises) vm_e.alloc(ctx->pool, op->n_elem + 1);
-        if (sol->nodal_von_mises) vm_n.alloc(ctx->pool, op->n_nodes + 1);
-        if (sol->reactions) react.alloc(ctx->pool, op->n_fixed + 1);
-        if (sol->displacements) disp.alloc(ctx->pool, 3 * op->n_nodes + 1);
-        recover_stress(ctx, op, op->u.p, vm_e.p, vm_n.p, react.p, disp.p);
+        stress_to_device(op);
         SVX_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
-        cudaStream_t st = ctx->stream;
-        if (sol->von_mises && op->n_elem)
-            SVX_CUDA(cudaMemcpyAsync(sol->von_mises, vm_e.p, op->n_elem * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->nodal_von_mises && op->n_nodes)
-            SVX_CUDA(cudaMemcpyAsync(sol->nodal_von_mises, vm_n.p, op->n_nodes * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->reactions && op->n_fixed)
-            SVX_CUDA(cudaMemcpyAsync(sol->reactions, react.p, op->n_fixed * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->displacements && op->n_nodes)
-            SVX_CUDA(cudaMemcpyAsync(sol->displacements, disp.p, 3 * op->n_nodes * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        sol->ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+        if (sol) {
+            copy_stress_out(op, sol);
+            sol->ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+        }
     }
     SVX_CUDA(cudaStreamSynchronize(ctx->stream));
     clear_error(err);
@@ -458,6 +490,31 @@ int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, uint32_t flags, 
     *out = nullptr;
     return guarded(ctx, err, [&]() -> int {
         *out = assemble_impl(ctx, model, flags);
+        clear_error(err);
+        return SVX_OK;
+    });
+}
+
+void* svx_ctx_stream(svx_ctx_t* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t svx_launch_count(void) { return int64_t(g_launches.load()); }
+
+int svx_op_time_kernels(svx_op_t* op, int reps, double* ms3) {
+    if (!op || !ms3 || reps <= 0) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, nullptr, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        time_iteration_kernels(ctx, op, reps, ms3);
+        return SVX_OK;
+    });
+}
+
+int svx_op_reassemble(svx_op_t* op, svx_error_t* err) {
+    if (!op) return SVX_BAD_ARGUMENT;
+    svx_ctx* ctx = op->ctx;
+    return guarded(ctx, err, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        device_assemble(ctx, op);
         clear_error(err);
         return SVX_OK;
     });
@@ -561,24 +618,7 @@ int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol
                  svx_error_t* err) {
     if (!op) return SVX_BAD_ARGUMENT;
     svx_ctx* ctx = op->ctx;
-    return guarded(ctx, err, [&]() -> int {
-        svx_solve_opts_t o;
-        svx_default_opts(&o);
-        if (opts) o = *opts;
-        o.want_stress = 0;
-        svx_solution_t tmp{};
-        if (sol) tmp = *sol;
-        int st = solve_impl(op, &o, sol ? &tmp : nullptr, err);
-        if (sol) {
-            sol->iterations = tmp.iterations;
-            sol->outer_iterations = tmp.outer_iterations;
-            sol->final_residual = tmp.final_residual;
-            sol->cond_estimate = tmp.cond_estimate;
-            sol->ms_assemble = tmp.ms_assemble;
-            sol->ms_solve = tmp.ms_solve;
-        }
-        return st;
-    });
+    return guarded(ctx, err, [&]() -> int { return solve_impl(op, opts, sol, err); });
 }
 
 int svx_op_stress(svx_op_t* op, svx_solution_t* sol) {
@@ -590,25 +630,9 @@ int svx_op_stress(svx_op_t* op, svx_solution_t* sol) {
         SVX_CUDA(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         SVX_CUDA(cudaEventRecord(ctx->ev[4], st));
-        DBuf<double> vm_e, vm_n, react, disp;
-        if (sol->von_mises) vm_e.alloc(ctx->pool, op->n_elem + 1);
-        if (sol->nodal_von_mises) vm_n.alloc(ctx->pool, op->n_nodes + 1);
-        if (sol->reactions) react.alloc(ctx->pool, op->n_fixed + 1);
-        if (sol->displacements) disp.alloc(ctx->pool, 3 * op->n_nodes + 1);
-        recover_stress(ctx, op, op->u.p, vm_e.p, vm_n.p, react.p, disp.p);
+        stress_to_device(op);
         SVX_CUDA(cudaEventRecord(ctx->ev[5], st));
-        if (sol->von_mises && op->n_elem)
-            SVX_CUDA(cudaMemcpyAsync(sol->von_mises, vm_e.p, op->n_elem * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->nodal_von_mises && op->n_nodes)
-            SVX_CUDA(cudaMemcpyAsync(sol->nodal_von_mises, vm_n.p, op->n_nodes * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->reactions && op->n_fixed)
-            SVX_CUDA(cudaMemcpyAsync(sol->reactions, react.p, op->n_fixed * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
-        if (sol->displacements && op->n_nodes)
-            SVX_CUDA(cudaMemcpyAsync(sol->displacements, disp.p, 3 * op->n_nodes * sizeof(double),
-                                     cudaMemcpyDeviceToHost, st));
+        copy_stress_out(op, sol);
         if (sol->u)
             SVX_CUDA(cudaMemcpyAsync(sol->u, op->u.p, op->n * sizeof(double),
                                      cudaMemcpyDeviceToHost, st));

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -28,7 +30,15 @@ struct CudaFail {
                                                          __FILE__ ":" + std::to_string(__LINE__)}; \
     } while (0)
 
-#define SVX_LAUNCH_CHECK() SVX_CUDA(cudaGetLastError())
+// Kernels launched by this process through the library (graph nodes are
+// counted when their graph is launched).
+extern std::atomic<long long> g_launches;
+
+#define SVX_LAUNCH_CHECK()                                     \
+    do {                                                       \
+        ::svx::g_launches.fetch_add(1, std::memory_order_relaxed); \
+        SVX_CUDA(cudaGetLastError());                          \
+    } while (0)
 
 // Error thrown for model / argument problems (carries the svx_error_t).
 struct ModelFail {
@@ -180,6 +190,11 @@ struct svx_op {
     svx::DBuf<double> kc_val;
     std::vector<int64_t> h_fixed_row;
     std::vector<uint32_t> h_node_id;
+    std::vector<uint32_t> h_elem_id;
+    uint32_t flags = 0;
+    double ms_upload_assemble = 0.0;
+    // recovered fields (device)
+    svx::DBuf<double> vm_elem, vm_node, react, disp3;
     // solution state
     svx::DBuf<double> u;
     bool has_solution = false;
@@ -222,6 +237,9 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
                     int check_every, double* u_dev, long long* outer_steps);
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y);
 int choose_spmv_group(const svx_op* op);
+// Average device time (ms) of the three FP64 PCG iteration kernels
+// (spmv_dot, update, p_update) over `reps` back-to-back launches each.
+void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3);
 
 // Generic device helpers (svx_pattern.cu).
 void exclusive_scan_i64(svx_ctx* ctx, const int64_t* in, int64_t* out, int64_t n,

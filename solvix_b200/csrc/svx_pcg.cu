@@ -412,6 +412,7 @@ struct PcgRun {
                     throw ModelFail{SVX_CUDA_ERROR, 0, -1,
                                     "PCG status did not leave RUNNING within max_iter"};
                 SVX_CUDA(cudaGraphLaunch(exec, st));
+                g_launches.fetch_add(3LL * check_every, std::memory_order_relaxed);
                 SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
                 SVX_CUDA(cudaStreamSynchronize(st));
                 status = h_s->status;
@@ -446,6 +447,55 @@ int auto_check_every(int64_t n, int64_t nnz) {
 }
 
 }  // namespace
+
+std::atomic<long long> g_launches{0};
+
+void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
+    const int64_t n = op->n;
+    cudaStream_t st = ctx->stream;
+    DBuf<double> u, r, p, q, partials;
+    DBuf<PcgScalars> s;
+    u.alloc(ctx->pool, n + 1);
+    r.alloc(ctx->pool, n + 1);
+    p.alloc(ctx->pool, n + 1);
+    q.alloc(ctx->pool, n + 1);
+    const int G = op->spmv_group;
+    const unsigned grid_r = grid_rows(ctx, n, G), grid_v = grid_vec(ctx, n);
+    partials.alloc(ctx->pool, 2 * size_t(std::max(grid_r, grid_v)) + 2);
+    s.alloc(ctx->pool, 1);
+    // a running state that never stops: tol 0, unbounded budget
+    PcgScalars init{};
+    init.tol = 0.0;
+    init.max_iter = (1LL << 62);
+    init.bnorm = 1.0;
+    init.status = PCG_RUNNING;
+    SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    SVX_CUDA(cudaMemcpyAsync(p.p, op->f.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    SVX_CUDA(cudaMemcpyAsync(r.p, op->f.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    SVX_CUDA(cudaMemsetAsync(u.p, 0, n * sizeof(double), st));
+    auto timed = [&](auto&& launch) -> double {
+        launch();  // warm
+        SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+        for (int k = 0; k < reps; ++k) launch();
+        SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+        SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
+        float ms = 0.f;
+        SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        g_launches.fetch_add(reps + 1, std::memory_order_relaxed);
+        return double(ms) / reps;
+    };
+    ms3[0] = timed([&] {
+        launch_spmv_dot<double>(G, grid_r, st, n, op, op->vals.p, p.p, q.p, partials.p, s.p);
+    });
+    ms3[1] = timed([&] {
+        update_kernel<double, double><<<grid_v, BLOCK, 0, st>>>(n, u.p, r.p, p.p, q.p,
+                                                                op->inv_diag.p, partials.p, s.p);
+    });
+    ms3[2] = timed([&] {
+        p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p.p, r.p, op->inv_diag.p, s.p);
+    });
+    SVX_CUDA(cudaGetLastError());
+}
 
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y) {
     const int G = op->spmv_group;

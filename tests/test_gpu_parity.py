@@ -63,8 +63,9 @@ def orphan_and_collapsed():
     xyz = np.vstack([flat.xyz, [[9.0, 9.0, 0.0]]])  # orphan node, index n
     n_nodes = xyz.shape[0]
     conn = flat.conn.reshape(-1, 4).copy()
-    # collapse the last element's third node onto its fourth (triangle-shaped quad)
-    conn[-1, 2] = conn[-1, 3]
+    # collapse the first element's third node onto its fourth (triangle-shaped
+    # quad); the dropped corner stays in use by the neighbouring elements
+    conn[0, 2] = conn[0, 3]
     f = np.zeros(n_nodes * 2)
     f[: flat.f.shape[0]] = flat.f
     return FlatModel(xyz=xyz, kind=flat.kind, conn_ptr=flat.conn_ptr, conn=conn.ravel(),
