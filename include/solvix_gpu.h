@@ -275,6 +275,40 @@ int64_t svx_launch_count(void);
  * update), each over `reps` back-to-back launches on the context stream. */
 int svx_op_time_kernels(svx_op_t* op, int reps, double* ms3);
 
+/* ---- PCG without device allocation ---------------------------------- */
+/* Largest system (rows) svx_pcg_solve_noalloc accepts. */
+#define SVX_NOALLOC_MAX_DOF 262144
+
+/* Jacobi-preconditioned CG on a CSR system that already lives on the
+ * device, for callers that cannot let a library allocate device memory:
+ * an application that manages all device memory through its own arena, or
+ * a latency-bounded loop that cannot absorb the implicit synchronisation of
+ * cudaMalloc / cudaFree.  This entry point has no counterpart in the
+ * reference; it runs the same kernels, launch geometry and stopping rule as
+ * svx_op_solve (FP64).
+ *
+ * Every pointer but `iterations` / `residual` (host) is a device pointer of
+ * the current device: row_ptr [n + 1] and col_idx [nnz] (int32, sorted
+ * columns, the diagonal present), vals [nnz], f [n], u [n] (output).  tol is
+ * the relative residual tolerance; max_iter <= 0 means max(1000, 10 n).
+ * stream is a cudaStream_t (NULL = the legacy default stream); the call
+ * returns after the solve has finished on it.
+ *
+ * Nothing is allocated: the work vectors (4 x SVX_NOALLOC_MAX_DOF doubles,
+ * about 8 MB) live in one static device array that every GPU loading this
+ * library holds until the process exits.  All calls on a device share that
+ * array and it keeps the previous call's contents, so calls whose work
+ * overlaps on the GPU (other threads, other streams) race; serialise them.
+ * The first call on each device looks up the array's device address, so
+ * make that first call before any stream capture.
+ *
+ * Returns SVX_OK, SVX_NOT_CONVERGED (iterations / residual filled),
+ * SVX_BAD_ARGUMENT (null pointer, n <= 0 or n > SVX_NOALLOC_MAX_DOF) or
+ * SVX_CUDA_ERROR. */
+int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col_idx,
+                          const double* vals, const double* f, double tol, int64_t max_iter,
+                          double* u, int64_t* iterations, double* residual, void* stream);
+
 /* ---- one-call pipelines -------------------------------------------- */
 /* Whole linear-static path for a flat model: lib.rs:614-703. */
 int svx_solve_flat(svx_ctx_t* ctx, const svx_flat_model_t* model,

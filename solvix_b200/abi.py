@@ -32,6 +32,7 @@ SVX_QUEUE_EMPTY = 8
 SVX_CPS3, SVX_CPS4, SVX_CPS8, SVX_CPE4, SVX_CPE8, SVX_C3D8, SVX_C3D4, SVX_B31 = range(8)
 
 SVX_KEEP_ORIGINAL = 1
+SVX_NOALLOC_MAX_DOF = 262144
 
 # enum svx_precision
 SVX_FP64 = 0
@@ -158,6 +159,8 @@ SIGNATURES = {
     "svx_op_reassemble": (C.c_int, [_VP, C.POINTER(SvxError)]),
     "svx_launch_count": (C.c_int64, []),
     "svx_op_time_kernels": (C.c_int, [_VP, C.c_int, c_double_p]),
+    "svx_pcg_solve_noalloc": (C.c_int, [C.c_int64, _VP, _VP, _VP, _VP, C.c_double, C.c_int64,
+                                        _VP, c_int64_p, c_double_p, _VP]),
     "svx_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
     "svx_resolve": (C.c_int, [C.POINTER(SvxModelDesc), C.POINTER(_VP), C.POINTER(SvxError)]),
     "svx_resolved_flat": (C.POINTER(SvxFlatModel), [_VP]),

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace svx {
@@ -701,3 +702,173 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
 }
 
 }  // namespace svx
+
+// ---------------------------------------------------------------------------
+// Jacobi-PCG on a caller-owned device CSR that allocates no memory.
+//
+// Some callers cannot let a library allocate device memory: a host
+// application that owns the whole device-memory budget through its own
+// arena (a cudaMalloc behind its back fragments that arena and synchronises
+// the device), or a caller running a latency-bounded loop in which the
+// implicit synchronisation and unpredictable latency of cudaMalloc /
+// cudaFree are not acceptable.  For them svx_pcg_solve_noalloc takes every
+// input and output as a device pointer and keeps all of its work vectors in
+// the file-scope array below, which every GPU that loads the library holds
+// until the process exits.
+// ---------------------------------------------------------------------------
+namespace svx {
+namespace {
+
+constexpr int64_t NOALLOC_MAX_N = SVX_NOALLOC_MAX_DOF;
+constexpr int64_t NOALLOC_PARTIALS = 4096;  // >= 2 * the largest grid used
+constexpr int64_t NOALLOC_SCALARS = 16;     // doubles holding a PcgScalars
+constexpr int64_t NOALLOC_DOUBLES = 4 * NOALLOC_MAX_N + NOALLOC_PARTIALS + NOALLOC_SCALARS;
+static_assert(sizeof(PcgScalars) <= NOALLOC_SCALARS * sizeof(double), "scalar slot too small");
+
+// r | p | q | inv_diag | block partials | PcgScalars.  Shared by every call
+// on a device; its contents are whatever the previous call left.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+int g_noalloc_sms[NOALLOC_MAX_DEVICES] = {};
+
+// 1 / K_ii (0 for a zero or missing diagonal), as the PCG's Jacobi step.
+__global__ void noalloc_inv_diag_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
+                                        const int32_t* __restrict__ col_idx,
+                                        const double* __restrict__ vals,
+                                        double* __restrict__ inv_diag) {
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    for (int32_t j = row_ptr[i]; j < row_ptr[i + 1]; ++j)
+        if (col_idx[j] == i) {
+            d = vals[j];
+            break;
+        }
+    inv_diag[i] = (d == 0.0) ? 0.0 : 1.0 / d;
+}
+
+void launch_spmv_dot_raw(int G, unsigned grid, cudaStream_t st, int64_t n, const int32_t* rp,
+                         const int32_t* ci, const double* vals, const double* p, double* q,
+                         double* partials, PcgScalars* s) {
+    switch (G) {
+        case 2: spmv_dot_kernel<2, double><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 4: spmv_dot_kernel<4, double><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 8: spmv_dot_kernel<8, double><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        case 16: spmv_dot_kernel<16, double><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+        default: spmv_dot_kernel<32, double><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
+    }
+}
+
+// Device address of the scratch array and the SM count of the current
+// device, looked up once per device (the array's name is only a host-side
+// stand-in; the kernels need the address cudaGetSymbolAddress returns).
+cudaError_t noalloc_setup(int* device, double** scratch, int* sms) {
+    cudaError_t e = cudaGetDevice(device);
+    if (e != cudaSuccess) return e;
+    if (*device < 0 || *device >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[*device]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        int count = 0;
+        e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, *device);
+        if (e != cudaSuccess) return e;
+        g_noalloc_sms[*device] = count;
+        g_noalloc_ptr[*device] = static_cast<double*>(p);
+    }
+    *scratch = g_noalloc_ptr[*device];
+    *sms = g_noalloc_sms[*device];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+}  // namespace svx
+
+extern "C" int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col_idx,
+                                     const double* vals, const double* f, double tol,
+                                     int64_t max_iter, double* u, int64_t* iterations,
+                                     double* residual, void* stream) {
+    using namespace svx;
+    if (n <= 0 || !row_ptr || !col_idx || !vals || !f || !u) return SVX_BAD_ARGUMENT;
+    if (n > NOALLOC_MAX_N) return SVX_BAD_ARGUMENT;  // beyond the static scratch
+    int device = 0, sms = 0;
+    double* scratch = nullptr;
+    if (noalloc_setup(&device, &scratch, &sms) != cudaSuccess) {
+        cudaGetLastError();
+        return SVX_CUDA_ERROR;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* r = scratch;
+    double* p = r + NOALLOC_MAX_N;
+    double* q = p + NOALLOC_MAX_N;
+    double* inv_diag = q + NOALLOC_MAX_N;
+    double* partials = inv_diag + NOALLOC_MAX_N;
+    PcgScalars* s = reinterpret_cast<PcgScalars*>(partials + NOALLOC_PARTIALS);
+
+    // nnz and the launch geometry of the allocating path
+    int32_t nnz = 0;
+    if (cudaMemcpyAsync(&nnz, row_ptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return SVX_CUDA_ERROR;
+    }
+    const int G = pick_group(double(nnz) / double(n));
+    const int64_t per_block = BLOCK / G;
+    const unsigned grid_r =
+        unsigned(std::max<int64_t>(1, std::min<int64_t>((n + per_block - 1) / per_block,
+                                                        int64_t(sms) * 8)));
+    const unsigned grid_v = unsigned(
+        std::max<int64_t>(1, std::min<int64_t>((n + BLOCK - 1) / BLOCK, int64_t(sms) * 8)));
+    if (2 * int64_t(std::max(grid_r, grid_v)) + 2 > NOALLOC_PARTIALS) return SVX_BAD_ARGUMENT;
+    if (max_iter <= 0) max_iter = std::max<int64_t>(1000, 10 * n);
+    const int check_every = auto_check_every(n, nnz);
+
+    // the scalars must start from a clean state every call
+    PcgScalars init{};
+    init.tol = tol;
+    init.max_iter = max_iter;
+    init.status = PCG_RUNNING;
+    PcgScalars h{};
+    cudaError_t e = cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        noalloc_inv_diag_kernel<<<unsigned((n + 255) / 256), 256, 0, st>>>(n, row_ptr, col_idx,
+                                                                           vals, inv_diag);
+        init_kernel<double, double><<<grid_v, BLOCK, 0, st>>>(n, f, 1.0, u, r, p, inv_diag,
+                                                             partials, s);
+        g_launches.fetch_add(2, std::memory_order_relaxed);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, s, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    // the device stops at max_iter; the launch bound only guards the host loop
+    const long long launches_max = max_iter / check_every + 2;
+    for (long long launch = 0; e == cudaSuccess && h.status == PCG_RUNNING; ++launch) {
+        if (launch >= launches_max) {
+            e = cudaErrorUnknown;
+            break;
+        }
+        for (int k = 0; k < check_every; ++k) {
+            launch_spmv_dot_raw(G, grid_r, st, n, row_ptr, col_idx, vals, p, q, partials, s);
+            update_kernel<double, double><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag,
+                                                                    partials, s);
+            p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
+        }
+        g_launches.fetch_add(3LL * check_every, std::memory_order_relaxed);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, s, sizeof(h), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return SVX_CUDA_ERROR;
+    }
+    if (iterations) *iterations = h.it;
+    if (residual) *residual = h.res;
+    return h.status == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
+}
