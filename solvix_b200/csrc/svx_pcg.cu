@@ -148,6 +148,166 @@ spmv_dot_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
     }
 }
 
+
+// ------------------------------------------------------------ node-block SpMV
+// The pattern is node adjacency x dense ndof blocks, so the ND rows of node i
+// share one column list: adj[adj_ptr[i] .. adj_ptr[i+1]).  These kernels read
+// the column of each ND x ND block once from adj (4 B per block instead of
+// 4 B per nonzero) and the values in the CSR order of the node's rows:
+//   y[i*ND + da] = sum_k sum_db vals[node_base[i] + da*ND*d + k*ND + db]
+//                                * x[adj[k]*ND + db]
+// G lanes own one node and split its d blocks; lane k loads one index, ND
+// x values and ND*ND matrix values, all independent of each other.
+template <int ND, int G, class V>
+__device__ __forceinline__ void node_rows(const int64_t* __restrict__ adj_ptr,
+                                          const int32_t* __restrict__ adj,
+                                          const int64_t* __restrict__ node_base,
+                                          const V* __restrict__ vals, const V* __restrict__ x,
+                                          int64_t i, int gl, double* acc) {
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const V* __restrict__ v = vals + node_base[i];
+    if (d == 0) {  // an unreferenced node: rows of length 1 (the diagonal)
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = double(v[da]) * double(x[i * ND + da]);
+        return;
+    }
+    const int rowlen = ND * d;
+    for (int k = gl; k < d; k += G) {
+        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xv[db] = double(x[c + db]);
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                acc[da] += double(__ldg(v + da * rowlen + k * ND + db)) * xv[db];
+    }
+}
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// q = K p (node blocks) and the per-block partial of p.q; the last block
+// forms pap and alpha exactly like spmv_dot_kernel.
+template <int ND, int G, class V>
+__global__ void __launch_bounds__(BLOCK)
+spmv_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                     const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                     const V* __restrict__ vals, const V* __restrict__ p, V* __restrict__ q,
+                     double* __restrict__ partials, PcgScalars* __restrict__ s) {
+    __shared__ double sh[32];
+    if (s->status != PCG_RUNNING) return;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t nodes_per_block = BLOCK / G;
+    double dot = 0.0;
+    for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
+         nb += int64_t(gridDim.x) * nodes_per_block) {
+        const int64_t i = nb + ((threadIdx.x & 31) / G);
+        double acc[ND];
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+        if (i < n_nodes) node_rows<ND, G, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+        if (i < n_nodes && gl == 0) {
+#pragma unroll
+            for (int da = 0; da < ND; ++da) {
+                V qv = V(acc[da]);
+                q[i * ND + da] = qv;
+                dot += double(p[i * ND + da]) * double(qv);
+            }
+        }
+    }
+    double bs = block_sum(dot, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+    if (last_block(&s->count_a)) {
+        double pap = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            s->count_a = 0;
+            s->pap = pap;
+            if (pap <= 0.0 || isnan(pap)) {
+                s->status = PCG_BREAKDOWN;
+                s->it = s->it + 1;
+                s->res = sqrt(s->rr) / s->bnorm;
+            } else {
+                s->alpha = s->rz / pap;
+            }
+        }
+    }
+}
+
+// y = K x (FP64, node blocks).
+template <int ND, int G>
+__global__ void __launch_bounds__(BLOCK)
+spmv_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                 const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                 const double* __restrict__ vals, const double* __restrict__ x,
+                 double* __restrict__ y) {
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t nodes_per_block = BLOCK / G;
+    for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
+         nb += int64_t(gridDim.x) * nodes_per_block) {
+        const int64_t i = nb + ((threadIdx.x & 31) / G);
+        double acc[ND];
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+        if (i < n_nodes) node_rows<ND, G, double>(adj_ptr, adj, node_base, vals, x, i, gl, acc);
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+        if (i < n_nodes && gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) y[i * ND + da] = acc[da];
+    }
+}
+
+// r = f - K u (FP64, node blocks) and r.r, for the defect correction.
+template <int ND, int G>
+__global__ void __launch_bounds__(BLOCK)
+residual_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                     const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                     const double* __restrict__ vals, const double* __restrict__ u,
+                     const double* __restrict__ f, double* __restrict__ r,
+                     double* __restrict__ partials, unsigned int* counter,
+                     double* __restrict__ out_rr) {
+    __shared__ double sh[32];
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t nodes_per_block = BLOCK / G;
+    double rr = 0.0;
+    for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
+         nb += int64_t(gridDim.x) * nodes_per_block) {
+        const int64_t i = nb + ((threadIdx.x & 31) / G);
+        double acc[ND];
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+        if (i < n_nodes) node_rows<ND, G, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+        if (i < n_nodes && gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) {
+                double ri = f[i * ND + da] - acc[da];
+                r[i * ND + da] = ri;
+                rr += ri * ri;
+            }
+    }
+    double b = block_sum(rr, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = b;
+    if (last_block(counter)) {
+        double t = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            *counter = 0;
+            *out_rr = t;
+        }
+    }
+}
+
 // u += alpha p ; r -= alpha q ; partials of r.r and r.z (z = r * inv_diag).
 template <class V, class U>
 __global__ void __launch_bounds__(BLOCK)
@@ -365,6 +525,44 @@ void launch_spmv_dot(int G, unsigned grid, cudaStream_t st, int64_t n, const svx
     }
 }
 
+// Lanes per node for the node-block kernels: the smallest of 8 / 16 / 32
+// that covers the largest node degree (27 for interior C3D8 nodes).
+int pick_node_group(int max_deg) {
+    if (max_deg <= 8) return 8;
+    if (max_deg <= 16) return 16;
+    return 32;
+}
+
+unsigned grid_nodes(const svx_ctx* ctx, int64_t n_nodes, int G) {
+    int64_t per_block = BLOCK / G;
+    int64_t need = (n_nodes + per_block - 1) / per_block;
+    int64_t cap = int64_t(ctx->sm_count) * 8;
+    return unsigned(std::max<int64_t>(1, std::min(need, cap)));
+}
+
+#define SVX_NODE_DISPATCH(ND_, G_, KERNEL_CALL)                         \
+    do {                                                                \
+        if ((ND_) == 3) {                                               \
+            if ((G_) == 8) { constexpr int ND = 3, GG = 8; KERNEL_CALL; } \
+            else if ((G_) == 16) { constexpr int ND = 3, GG = 16; KERNEL_CALL; } \
+            else { constexpr int ND = 3, GG = 32; KERNEL_CALL; }        \
+        } else {                                                        \
+            if ((G_) == 8) { constexpr int ND = 2, GG = 8; KERNEL_CALL; } \
+            else if ((G_) == 16) { constexpr int ND = 2, GG = 16; KERNEL_CALL; } \
+            else { constexpr int ND = 2, GG = 32; KERNEL_CALL; }        \
+        }                                                               \
+    } while (0)
+
+template <class V>
+void launch_spmv_node_dot(const svx_op* op, int G, unsigned grid, cudaStream_t st,
+                          const V* vals, const V* p, V* q, double* partials, PcgScalars* s) {
+    const Pattern& P = op->pat;
+    SVX_NODE_DISPATCH(op->ndof, G,
+                      (spmv_node_dot_kernel<ND, GG, V><<<grid, BLOCK, 0, st>>>(
+                          op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, vals, p, q,
+                          partials, s)));
+}
+
 // One PCG run in value type V (the vectors and K) with solution type U.
 template <class V, class U>
 struct PcgRun {
@@ -382,7 +580,7 @@ struct PcgRun {
     PcgScalars* h_s;  // pinned
 
     void enqueue_iteration(cudaStream_t st) {
-        launch_spmv_dot<V>(G, grid_r, st, n, op, vals, p, q, partials, s);
+        launch_spmv_node_dot<V>(op, G, grid_r, st, vals, p, q, partials, s);
         update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
         p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
     }
@@ -460,8 +658,8 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
-    const int G = op->spmv_group;
-    const unsigned grid_r = grid_rows(ctx, n, G), grid_v = grid_vec(ctx, n);
+    const int G = pick_node_group(op->pat.max_deg);
+    const unsigned grid_r = grid_nodes(ctx, op->n_nodes, G), grid_v = grid_vec(ctx, n);
     partials.alloc(ctx->pool, 2 * size_t(std::max(grid_r, grid_v)) + 2);
     s.alloc(ctx->pool, 1);
     // a running state that never stops: tol 0, unbounded budget
@@ -486,7 +684,7 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
         return double(ms) / reps;
     };
     ms3[0] = timed([&] {
-        launch_spmv_dot<double>(G, grid_r, st, n, op, op->vals.p, p.p, q.p, partials.p, s.p);
+        launch_spmv_node_dot<double>(op, G, grid_r, st, op->vals.p, p.p, q.p, partials.p, s.p);
     });
     ms3[1] = timed([&] {
         update_kernel<double, double><<<grid_v, BLOCK, 0, st>>>(n, u.p, r.p, p.p, q.p,
@@ -499,18 +697,13 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
 }
 
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y) {
-    const int G = op->spmv_group;
-    unsigned grid = grid_rows(ctx, op->n, G);
+    const int G = pick_node_group(op->pat.max_deg);
+    const unsigned grid = grid_nodes(ctx, op->n_nodes, G);
     cudaStream_t st = ctx->stream;
-    const int32_t* rp = op->pat.row_ptr.p;
-    const int32_t* ci = op->pat.col_idx.p;
-    switch (G) {
-        case 2: spmv_kernel<2><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
-        case 4: spmv_kernel<4><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
-        case 8: spmv_kernel<8><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
-        case 16: spmv_kernel<16><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
-        default: spmv_kernel<32><<<grid, BLOCK, 0, st>>>(op->n, rp, ci, vals, x, y); break;
-    }
+    const Pattern& P = op->pat;
+    SVX_NODE_DISPATCH(op->ndof, G,
+                      (spmv_node_kernel<ND, GG><<<grid, BLOCK, 0, st>>>(
+                          op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, vals, x, y)));
     SVX_LAUNCH_CHECK();
 }
 
@@ -530,13 +723,13 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
-    const int G = op->spmv_group;
+    const int G = pick_node_group(op->pat.max_deg);
     PcgRun<double, double> run;
     run.ctx = ctx;
     run.op = op;
     run.n = n;
     run.G = G;
-    run.grid_r = grid_rows(ctx, n, G);
+    run.grid_r = grid_nodes(ctx, op->n_nodes, G);
     run.grid_v = grid_vec(ctx, n);
     partials.alloc(ctx->pool, 2 * size_t(std::max(run.grid_r, run.grid_v)) + 2);
     s.alloc(ctx->pool, 1);
@@ -579,7 +772,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
     if (check_every <= 0) check_every = auto_check_every(n, op->pat.nnz);
-    const int G = op->spmv_group;
+    const int G = pick_node_group(op->pat.max_deg);
     // FP32 copies of K and the Jacobi diagonal
     if (!op->vals32.p) {
         op->vals32.alloc(ctx->pool, op->pat.nnz + 1);
@@ -627,16 +820,12 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     // ||f||
     double* h_rr = &hs.h->rr;  // scratch slot of the pinned struct
     auto true_residual = [&]() -> double {
-        unsigned grid = grid_rows(ctx, n, G);
-        const int32_t* rp = op->pat.row_ptr.p;
-        const int32_t* ci = op->pat.col_idx.p;
-        switch (G) {
-            case 2: residual_kernel<2><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
-            case 4: residual_kernel<4><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
-            case 8: residual_kernel<8><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
-            case 16: residual_kernel<16><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
-            default: residual_kernel<32><<<grid, BLOCK, 0, st>>>(n, rp, ci, op->vals.p, u_dev, op->f.p, r64.p, partials.p, counter.p, rr_dev.p); break;
-        }
+        const unsigned grid = grid_nodes(ctx, op->n_nodes, G);
+        const Pattern& P = op->pat;
+        SVX_NODE_DISPATCH(op->ndof, G,
+                          (residual_node_kernel<ND, GG><<<grid, BLOCK, 0, st>>>(
+                              op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p, u_dev,
+                              op->f.p, r64.p, partials.p, counter.p, rr_dev.p)));
         SVX_LAUNCH_CHECK();
         SVX_CUDA(cudaMemcpyAsync(h_rr, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         SVX_CUDA(cudaStreamSynchronize(st));
