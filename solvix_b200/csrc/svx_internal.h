@@ -135,6 +135,14 @@ struct PcgScalars {
 
 enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_BREAKDOWN = 2, PCG_MAXITER = 3 };
 
+// State of the bounded grid-wide barrier of the persistent PCG kernel.
+struct GridBarrier {
+    unsigned int count;  // blocks arrived at the current barrier
+    unsigned int gen;    // barrier generation
+    int error;           // 1 after a bounded spin gave up
+    int pad;
+};
+
 // Mesh pattern: node -> incident element slots and node adjacency.
 struct Pattern {
     int64_t n_nodes = 0, n_elem = 0;

@@ -34,6 +34,9 @@ namespace svx {
 namespace {
 
 constexpr int BLOCK = 256;
+// Resident blocks per SM the node-block SpMV kernels are compiled for; their
+// grids are exactly one wave of that many blocks per SM.
+constexpr int NODE_BLOCKS_PER_SM = 5;
 
 // ------------------------------------------------------------ reductions
 __device__ __forceinline__ double warp_sum(double v) {
@@ -197,7 +200,7 @@ __device__ __forceinline__ double group_sum(double v) {
 // q = K p (node blocks) and the per-block partial of p.q; the last block
 // forms pap and alpha exactly like spmv_dot_kernel.
 template <int ND, int G, class V>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, NODE_BLOCKS_PER_SM)
 spmv_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                      const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
                      const V* __restrict__ vals, const V* __restrict__ p, V* __restrict__ q,
@@ -245,7 +248,7 @@ spmv_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
 
 // y = K x (FP64, node blocks).
 template <int ND, int G>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, NODE_BLOCKS_PER_SM)
 spmv_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                  const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
                  const double* __restrict__ vals, const double* __restrict__ x,
@@ -269,7 +272,7 @@ spmv_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
 
 // r = f - K u (FP64, node blocks) and r.r, for the defect correction.
 template <int ND, int G>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, NODE_BLOCKS_PER_SM)
 residual_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                      const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
                      const double* __restrict__ vals, const double* __restrict__ u,
@@ -489,6 +492,205 @@ __global__ void to_float_kernel(int64_t n, const double* __restrict__ a, float* 
         b[i] = float(a[i]);
 }
 
+
+// ------------------------------------------------------------ persistent PCG
+// One cooperative launch runs up to `chunk` whole PCG iterations.  Block b
+// owns the nodes [n_nodes*b/B, n_nodes*(b+1)/B) for the SpMV and the rows of
+// those nodes for the vector updates, so an iteration is
+//   A: q = K p on own nodes, partial p.q          -> grid barrier
+//   B: alpha; u, r update on own rows, partials    -> grid barrier
+//   C: beta; p = z + beta p on own rows            -> grid barrier
+// Every block sums the same partials in the same order, so all blocks hold
+// bitwise identical scalars and take the same exit (converged, breakdown,
+// budget) without a broadcast.  Data written by other blocks during the
+// launch (p, q, partials) is read with ld.global.cg (L2), never through L1.
+// The barrier spins are bounded: on timeout the kernel raises an error flag
+// and returns, and the host reports a device error.
+constexpr int PBLOCK = 512;
+constexpr long long BARRIER_SPIN_LIMIT = 1LL << 25;
+
+template <int ND, int G, class V>
+__device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr,
+                                             const int32_t* __restrict__ adj,
+                                             const int64_t* __restrict__ node_base,
+                                             const V* __restrict__ vals, const V* x,
+                                             int64_t i, int gl, double* acc) {
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const V* __restrict__ v = vals + node_base[i];
+    if (d == 0) {
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = double(v[da]) * double(__ldcg(x + i * ND + da));
+        return;
+    }
+    const int rowlen = ND * d;
+#pragma unroll 2
+    for (int k = gl; k < d; k += G) {
+        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xv[db] = double(__ldcg(x + c + db));
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                acc[da] += double(__ldg(v + da * rowlen + k * ND + db)) * xv[db];
+    }
+}
+
+// Bounded grid-wide barrier (all blocks co-resident: cooperative launch).
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks) {
+    __shared__ int ok;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* vgen = &gb->gen;
+        const unsigned int g = *vgen;
+        int good = 1;
+        const unsigned int arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == nblocks - 1) {
+            gb->count = 0;
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*vgen == g) {
+                if (++spins > BARRIER_SPIN_LIMIT) {
+                    atomicExch(&gb->error, 1);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        ok = good && (*((volatile int*)&gb->error) == 0);
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Fixed-order sum of n partials (stride `stride`, offset `off`) read from L2.
+__device__ __forceinline__ double sum_partials_cg(const double* partials, int n, int stride,
+                                                  int off, double* sh) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) v += __ldcg(partials + k * stride + off);
+    return block_sum(v, sh);
+}
+
+template <int ND, int G, class V, class U>
+__global__ void __launch_bounds__(PBLOCK, 2)
+pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                      const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                      const V* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
+                      V* p, V* q, double* part_a, double* part_b, PcgScalars* s,
+                      GridBarrier* gb, int chunk) {
+    __shared__ double sh[32];
+    const unsigned int B = gridDim.x;
+    const int64_t nb0 = n_nodes * int64_t(blockIdx.x) / B;
+    const int64_t nb1 = n_nodes * int64_t(blockIdx.x + 1) / B;
+    const int64_t r0 = nb0 * ND, r1 = nb1 * ND;
+    volatile PcgScalars* vs = s;
+    if (vs->status != PCG_RUNNING) return;
+    double rz = vs->rz, rr = vs->rr, res = vs->res;
+    const double bnorm = vs->bnorm, tol = vs->tol;
+    long long it = vs->it;
+    const long long max_iter = vs->max_iter;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t warp_nodes = 32 / G;
+    const int64_t step = int64_t(PBLOCK / 32) * warp_nodes;
+    const bool writer = (blockIdx.x == 0 && threadIdx.x == 0);
+    for (int c = 0; c < chunk; ++c) {
+        // A: q = K p on own nodes, p.q
+        double dot = 0.0;
+        for (int64_t nb = nb0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < nb1; nb += step) {
+            const int64_t i = nb + ((threadIdx.x & 31) / G);
+            double acc[ND];
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+            if (i < nb1) node_rows_cg<ND, G, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+            if (i < nb1 && gl == 0) {
+#pragma unroll
+                for (int da = 0; da < ND; ++da) {
+                    V qv = V(acc[da]);
+                    q[i * ND + da] = qv;
+                    dot += double(__ldcg(p + i * ND + da)) * double(qv);
+                }
+            }
+        }
+        double bs = block_sum(dot, sh);
+        if (threadIdx.x == 0) part_a[blockIdx.x] = bs;
+        if (!grid_sync(gb, B)) return;
+        const double pap = sum_partials_cg(part_a, int(B), 1, 0, sh);
+        if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
+            if (writer) {
+                s->pap = pap;
+                s->it = it + 1;
+                s->res = sqrt(rr) / bnorm;
+                s->rr = rr;
+                s->rz = rz;
+                __threadfence();
+                s->status = PCG_BREAKDOWN;
+            }
+            return;
+        }
+        const double alpha = rz / pap;
+        // B: u += alpha p, r -= alpha q on own rows; r.r, r.z
+        const V a = V(alpha);
+        double lrr = 0.0, lrz = 0.0;
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += PBLOCK) {
+            const V pi = __ldcg(p + row);
+            u[row] = U(u[row] + U(a) * U(pi));
+            const V ri = __ldcg(r + row) - a * __ldcg(q + row);
+            r[row] = ri;
+            const V zi = ri * inv_diag[row];
+            lrr += double(ri) * double(ri);
+            lrz += double(ri) * double(zi);
+        }
+        const double brr = block_sum(lrr, sh);
+        const double brz = block_sum(lrz, sh);
+        if (threadIdx.x == 0) {
+            part_b[2 * blockIdx.x] = brr;
+            part_b[2 * blockIdx.x + 1] = brz;
+        }
+        if (!grid_sync(gb, B)) return;
+        const double rr_new = sum_partials_cg(part_b, int(B), 2, 0, sh);
+        const double rz_new = sum_partials_cg(part_b, int(B), 2, 1, sh);
+        it += 1;
+        rr = rr_new;
+        res = sqrt(rr) / bnorm;
+        if (res <= tol || it >= max_iter) {
+            if (writer) {
+                s->it = it;
+                s->res = res;
+                s->rr = rr;
+                s->rz = rz;
+                s->pap = pap;
+                s->alpha = alpha;
+                __threadfence();
+                s->status = (res <= tol) ? PCG_CONVERGED : PCG_MAXITER;
+            }
+            return;
+        }
+        const double beta = rz_new / rz;
+        rz = rz_new;
+        // C: p = z + beta p on own rows
+        const V bt = V(beta);
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += PBLOCK)
+            p[row] = __ldcg(r + row) * inv_diag[row] + bt * __ldcg(p + row);
+        if (!grid_sync(gb, B)) return;
+    }
+    if (writer) {
+        s->it = it;
+        s->res = res;
+        s->rr = rr;
+        s->rz = rz;
+    }
+}
+
 // ------------------------------------------------------------ host side
 int pick_group(double mean_row) {
     if (mean_row < 6) return 2;
@@ -536,7 +738,7 @@ int pick_node_group(int max_deg) {
 unsigned grid_nodes(const svx_ctx* ctx, int64_t n_nodes, int G) {
     int64_t per_block = BLOCK / G;
     int64_t need = (n_nodes + per_block - 1) / per_block;
-    int64_t cap = int64_t(ctx->sm_count) * 8;
+    int64_t cap = int64_t(ctx->sm_count) * NODE_BLOCKS_PER_SM;
     return unsigned(std::max<int64_t>(1, std::min(need, cap)));
 }
 
@@ -583,6 +785,63 @@ struct PcgRun {
         launch_spmv_node_dot<V>(op, G, grid_r, st, vals, p, q, partials, s);
         update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
         p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
+    }
+
+    // Persistent form: cooperative launches of up to `chunk` iterations each
+    // until the device status leaves RUNNING.  Returns -1 when a cooperative
+    // launch is not possible on this device (the caller falls back to the
+    // graph form).
+    int iterate_persistent(int chunk) {
+        cudaStream_t st = ctx->stream;
+        const int ND = op->ndof;
+        const int PG = (op->pat.max_deg <= 8) ? 8 : 16;
+        void* fn = nullptr;
+        if (ND == 3) fn = PG == 8 ? (void*)pcg_persistent_kernel<3, 8, V, U>
+                                  : (void*)pcg_persistent_kernel<3, 16, V, U>;
+        else fn = PG == 8 ? (void*)pcg_persistent_kernel<2, 8, V, U>
+                          : (void*)pcg_persistent_kernel<2, 16, V, U>;
+        int coop = 0, bps = 0;
+        SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+        SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, PBLOCK, 0));
+        if (!coop || bps <= 0) return -1;
+        const unsigned int B = unsigned(std::min(bps, 2) * ctx->sm_count);
+        DBuf<double> part_a, part_b;
+        DBuf<GridBarrier> gb;
+        part_a.alloc(ctx->pool, B + 1);
+        part_b.alloc(ctx->pool, 2 * size_t(B) + 2);
+        gb.alloc(ctx->pool, 1);
+        SVX_CUDA(cudaMemsetAsync(gb.p, 0, sizeof(GridBarrier), st));
+        int64_t n_nodes = op->n_nodes;
+        const int64_t* a_ptr = op->pat.adj_ptr.p;
+        const int32_t* a_idx = op->pat.adj.p;
+        const int64_t* nbase = op->pat.node_base.p;
+        GridBarrier* gbp = gb.p;
+        double* pa = part_a.p;
+        double* pb = part_b.p;
+        void* args[] = {&n_nodes, (void*)&a_ptr, (void*)&a_idx, (void*)&nbase, (void*)&vals,
+                        (void*)&inv_diag, (void*)&u, (void*)&r, (void*)&p, (void*)&q,
+                        (void*)&pa, (void*)&pb, (void*)&s, (void*)&gbp, (void*)&chunk};
+        SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        const long long launches_max = h_s->max_iter / chunk + 2;
+        GridBarrier hgb{};
+        int status = h_s->status;
+        for (long long launch = 0; status == PCG_RUNNING; ++launch) {
+            if (launch >= launches_max)
+                throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                "PCG status did not leave RUNNING within max_iter"};
+            SVX_CUDA(cudaLaunchCooperativeKernel(fn, dim3(B), dim3(PBLOCK), args, 0, st));
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            SVX_CUDA(cudaMemcpyAsync(&hgb, gbp, sizeof(GridBarrier), cudaMemcpyDeviceToHost, st));
+            SVX_CUDA(cudaStreamSynchronize(st));
+            if (hgb.error)
+                throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                "persistent PCG: a grid barrier wait ran out (blocks not "
+                                "co-resident)"};
+            status = h_s->status;
+        }
+        return status;
     }
 
     // Runs until the device status leaves RUNNING; returns the status.
@@ -635,6 +894,14 @@ struct PinnedScalars {
         if (h) cudaFreeHost(h);
     }
 };
+
+// Iterations per persistent launch: a few to tens of milliseconds of work,
+// so the host sees progress and a long solve is not one unbounded launch.
+int persistent_chunk(int64_t nnz) {
+    if (nnz > 100000000) return 64;
+    if (nnz > 10000000) return 256;
+    return 1024;
+}
 
 int auto_check_every(int64_t n, int64_t nnz) {
     // ~30 us per iteration at C3D8 3.5M dofs vs ~5 us at 10k dofs: keep one
@@ -755,7 +1022,10 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     SVX_CUDA(cudaMemcpyAsync(hs.h, s.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     SVX_CUDA(cudaStreamSynchronize(st));
     int status = hs.h->status;
-    if (status == PCG_RUNNING) status = run.iterate(check_every);
+    if (status == PCG_RUNNING) {
+        status = run.iterate_persistent(persistent_chunk(op->pat.nnz));
+        if (status < 0) status = run.iterate(check_every);
+    }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
     SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
     float ms = 0.f;
@@ -858,7 +1128,8 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         init_kernel<float, double><<<run.grid_v, BLOCK, 0, st>>>(
             n, r64.p, 1.0 / rnorm, d32.p, r32.p, p32.p, inv32.p, partials.p, s.p);
         SVX_LAUNCH_CHECK();
-        int inner_status = run.iterate(check_every);
+        int inner_status = run.iterate_persistent(persistent_chunk(op->pat.nnz));
+        if (inner_status < 0) inner_status = run.iterate(check_every);
         total_inner += hs.h->it;
         if (inner_status == PCG_BREAKDOWN && hs.h->it <= 1) {
             status = PCG_BREAKDOWN;
