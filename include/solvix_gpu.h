@@ -200,6 +200,7 @@ void svx_default_opts(svx_solve_opts_t* opts);
 
 /* ---- context ----------------------------------------------------- */
 int svx_ctx_create(int device, svx_ctx_t** out);
+/* Free every operator of a context (svx_op_free) before destroying it. */
 int svx_ctx_destroy(svx_ctx_t* ctx);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work or timing events with the library's. */

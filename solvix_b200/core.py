@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -48,6 +49,7 @@ class Context:
             raise DeviceError(buf.value.decode() or f"svx_ctx_create failed ({st})")
         self.handle = h
         self.device = device
+        self._ops = weakref.WeakSet()
 
     @property
     def stream(self) -> int:
@@ -55,7 +57,10 @@ class Context:
         return int(self.lib.svx_ctx_stream(self.handle) or 0)
 
     def close(self):
+        """Free every live operator of this context, then the context."""
         if getattr(self, "handle", None):
+            for op in list(getattr(self, "_ops", ())):
+                op.free()
             self.lib.svx_ctx_destroy(self.handle)
             self.handle = None
 
@@ -80,7 +85,9 @@ class Context:
         st = self.lib.svx_assemble(self.handle, C.byref(s), flags, C.byref(h), C.byref(err))
         if st != abi.SVX_OK:
             _raise(st, err)
-        return Operator(self, h, flat)
+        op = Operator(self, h, flat)
+        self._ops.add(op)
+        return op
 
     def solve_flat(self, flat: FlatModel, tol: float = 1e-10, max_iter: int = 0,
                    precision: int = abi.SVX_FP64, inner_tol: float = 1e-5,
@@ -178,7 +185,8 @@ class Operator:
 
     def free(self):
         if getattr(self, "handle", None):
-            self.lib.svx_op_free(self.handle)
+            if getattr(self.ctx, "handle", None):
+                self.lib.svx_op_free(self.handle)
             self.handle = None
 
     def __del__(self):
