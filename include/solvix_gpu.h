@@ -160,15 +160,19 @@ typedef struct svx_resolved svx_resolved_t;
 
 /* Precision forms of the PCG solve. */
 enum svx_precision {
-    SVX_FP64 = 0,   /* FP64 K, FP64 PCG: the plain form */
-    SVX_MIXED = 1   /* FP32-stored K, FP32 inner PCG, FP64 defect correction */
+    SVX_FP64 = 0,      /* FP64 K, FP64 PCG: the plain form */
+    SVX_MIXED = 1      /* FP32-stored K streamed by the PCG, FP64 vectors, u, dots and
+                          true residual (reliable-update defect correction, finishing
+                          with the FP64 operator once the FP32 one stops gaining) */
 };
 
 typedef struct svx_solve_opts {
     double tol;            /* relative residual tolerance (reference: 1e-10) */
     int64_t max_iter;      /* <= 0: max(1000, 10 * ndof_total) like lib.rs:632 */
     int32_t precision;     /* enum svx_precision */
-    double inner_tol;      /* mixed: inner FP32 PCG tolerance (default 1e-5) */
+    double inner_tol;      /* mixed: residual reduction of each FP32 segment between two
+                              FP64 true-residual updates; values outside (0.01, 1)
+                              select 0.1 */
     int32_t check_every;   /* iterations per graph launch between host checks (0: auto) */
     int32_t want_stress;   /* 1: compute von Mises + reactions */
 } svx_solve_opts_t;

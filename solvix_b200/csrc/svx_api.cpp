@@ -381,8 +381,8 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
     PcgResult r;
     long long outer = 0;
     if (opts.precision == SVX_MIXED)
-        r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol > 0 ? opts.inner_tol : 1e-5,
-                      opts.check_every, op->u.p, &outer);
+        r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol, opts.check_every, op->u.p,
+                      &outer);
     else
         r = pcg_fp64(ctx, op, opts.tol, max_iter, opts.check_every, op->u.p);
     op->has_solution = true;

@@ -125,6 +125,7 @@ struct PcgScalars {
     double bnorm;    // ||f||
     double tol;
     double res;      // ||r|| / ||f|| of the current iterate
+    double rr_stop;  // stop with PCG_RELIABLE once r.r <= rr_stop (< 0: never)
     long long it;        // iterations completed
     long long max_iter;
     int status;          // PCG_RUNNING / PCG_CONVERGED / PCG_BREAKDOWN / PCG_MAXITER
@@ -133,7 +134,8 @@ struct PcgScalars {
     unsigned int count_c;
 };
 
-enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_BREAKDOWN = 2, PCG_MAXITER = 3 };
+enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_BREAKDOWN = 2, PCG_MAXITER = 3,
+       PCG_RELIABLE = 4 };
 
 // State of the bounded grid-wide barrier of the persistent PCG kernel.
 struct GridBarrier {
@@ -213,6 +215,7 @@ struct svx_op {
     svx::DBuf<double> vals_orig;
     // PCG tuning picked for this operator
     int spmv_group = 8;
+    long long mixed_sloppy_iters = 0;  // FP32-operator iterations of the last mixed solve
     int spmv_block = 256;
 };
 

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace svx {
@@ -377,9 +378,9 @@ p_update_kernel(int64_t n, V* __restrict__ p, const V* __restrict__ r,
 }
 
 // r = b ; u = 0 ; p = z = r * inv_diag ; partials of b.b and r.z.
-template <class V, class B>
+template <class V, class B, class U = V>
 __global__ void __launch_bounds__(BLOCK)
-init_kernel(int64_t n, const B* __restrict__ b, double b_scale, V* __restrict__ u,
+init_kernel(int64_t n, const B* __restrict__ b, double b_scale, U* __restrict__ u,
             V* __restrict__ r, V* __restrict__ p, const V* __restrict__ inv_diag,
             double* __restrict__ partials, PcgScalars* __restrict__ s) {
     __shared__ double sh[32];
@@ -387,7 +388,7 @@ init_kernel(int64_t n, const B* __restrict__ b, double b_scale, V* __restrict__ 
     for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * BLOCK) {
         V ri = V(double(b[i]) * b_scale);
-        u[i] = V(0);
+        u[i] = U(0);
         r[i] = ri;
         V zi = ri * inv_diag[i];
         p[i] = zi;
@@ -509,15 +510,15 @@ __global__ void to_float_kernel(int64_t n, const double* __restrict__ a, float* 
 constexpr int PBLOCK = 512;
 constexpr long long BARRIER_SPIN_LIMIT = 1LL << 25;
 
-template <int ND, int G, class V>
+template <int ND, int G, class M, class V>
 __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr,
                                              const int32_t* __restrict__ adj,
                                              const int64_t* __restrict__ node_base,
-                                             const V* __restrict__ vals, const V* x,
+                                             const M* __restrict__ vals, const V* x,
                                              int64_t i, int gl, double* acc) {
     const int64_t a0 = adj_ptr[i];
     const int d = int(adj_ptr[i + 1] - a0);
-    const V* __restrict__ v = vals + node_base[i];
+    const M* __restrict__ v = vals + node_base[i];
     if (d == 0) {
         if (gl == 0)
 #pragma unroll
@@ -579,11 +580,11 @@ __device__ __forceinline__ double sum_partials_cg(const double* partials, int n,
     return block_sum(v, sh);
 }
 
-template <int ND, int G, class V, class U>
+template <int ND, int G, class M, class V, class U>
 __global__ void __launch_bounds__(PBLOCK, 2)
 pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                       const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
-                      const V* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
+                      const M* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
                       V* p, V* q, double* part_a, double* part_b, PcgScalars* s,
                       GridBarrier* gb, int chunk) {
     __shared__ double sh[32];
@@ -594,7 +595,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
     volatile PcgScalars* vs = s;
     if (vs->status != PCG_RUNNING) return;
     double rz = vs->rz, rr = vs->rr, res = vs->res;
-    const double bnorm = vs->bnorm, tol = vs->tol;
+    const double bnorm = vs->bnorm, tol = vs->tol, rr_stop = vs->rr_stop;
     long long it = vs->it;
     const long long max_iter = vs->max_iter;
     const int gl = threadIdx.x & (G - 1);
@@ -609,7 +610,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
             double acc[ND];
 #pragma unroll
             for (int da = 0; da < ND; ++da) acc[da] = 0.0;
-            if (i < nb1) node_rows_cg<ND, G, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+            if (i < nb1) node_rows_cg<ND, G, M, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
 #pragma unroll
             for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
             if (i < nb1 && gl == 0) {
@@ -662,16 +663,17 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         it += 1;
         rr = rr_new;
         res = sqrt(rr) / bnorm;
-        if (res <= tol || it >= max_iter) {
+        if (res <= tol || it >= max_iter || rr <= rr_stop) {
             if (writer) {
                 s->it = it;
                 s->res = res;
                 s->rr = rr;
-                s->rz = rz;
-                s->pap = pap;
+                s->rz = rz;         // r.z of the previous iterate (beta's denominator)
+                s->pap = rz_new;    // r.z of this iterate
                 s->alpha = alpha;
                 __threadfence();
-                s->status = (res <= tol) ? PCG_CONVERGED : PCG_MAXITER;
+                s->status = (res <= tol) ? PCG_CONVERGED
+                                         : (it >= max_iter ? PCG_MAXITER : PCG_RELIABLE);
             }
             return;
         }
@@ -766,14 +768,14 @@ void launch_spmv_node_dot(const svx_op* op, int G, unsigned grid, cudaStream_t s
 }
 
 // One PCG run in value type V (the vectors and K) with solution type U.
-template <class V, class U>
+template <class M, class V, class U>
 struct PcgRun {
     svx_ctx* ctx;
     const svx_op* op;
     int64_t n;
     int G;
     unsigned grid_r, grid_v;
-    const V* vals;
+    const M* vals;
     const V* inv_diag;
     U* u;
     V *r, *p, *q;
@@ -782,9 +784,14 @@ struct PcgRun {
     PcgScalars* h_s;  // pinned
 
     void enqueue_iteration(cudaStream_t st) {
-        launch_spmv_node_dot<V>(op, G, grid_r, st, vals, p, q, partials, s);
-        update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
-        p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
+        if constexpr (std::is_same<M, V>::value) {
+            launch_spmv_node_dot<V>(op, G, grid_r, st, vals, p, q, partials, s);
+            update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
+            p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
+        } else {
+            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                            "mixed precision needs cooperative launch (persistent PCG)"};
+        }
     }
 
     // Persistent form: cooperative launches of up to `chunk` iterations each
@@ -796,10 +803,10 @@ struct PcgRun {
         const int ND = op->ndof;
         const int PG = (op->pat.max_deg <= 8) ? 8 : 16;
         void* fn = nullptr;
-        if (ND == 3) fn = PG == 8 ? (void*)pcg_persistent_kernel<3, 8, V, U>
-                                  : (void*)pcg_persistent_kernel<3, 16, V, U>;
-        else fn = PG == 8 ? (void*)pcg_persistent_kernel<2, 8, V, U>
-                          : (void*)pcg_persistent_kernel<2, 16, V, U>;
+        if (ND == 3) fn = PG == 8 ? (void*)pcg_persistent_kernel<3, 8, M, V, U>
+                                  : (void*)pcg_persistent_kernel<3, 16, M, V, U>;
+        else fn = PG == 8 ? (void*)pcg_persistent_kernel<2, 8, M, V, U>
+                          : (void*)pcg_persistent_kernel<2, 16, M, V, U>;
         int coop = 0, bps = 0;
         SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
         SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, PBLOCK, 0));
@@ -991,7 +998,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
     const int G = pick_node_group(op->pat.max_deg);
-    PcgRun<double, double> run;
+    PcgRun<double, double, double> run;
     run.ctx = ctx;
     run.op = op;
     run.n = n;
@@ -1004,6 +1011,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     PcgScalars init{};
     init.tol = tol;
     init.max_iter = max_iter;
+    init.rr_stop = -1.0;
     init.status = PCG_RUNNING;
     SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
     SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
@@ -1037,126 +1045,187 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     return out;
 }
 
+// r = V(r64); partials of r.z; the last block forms beta = r.z / rz_old for
+// the reliable update (the search direction p is kept).
+template <class V>
+__global__ void __launch_bounds__(BLOCK)
+reliable_resume_kernel(int64_t n, const double* __restrict__ r64, V* __restrict__ r,
+                       const V* __restrict__ inv_diag, double* __restrict__ partials,
+                       PcgScalars* __restrict__ s) {
+    __shared__ double sh[32];
+    double rz = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * BLOCK) {
+        const V ri = V(r64[i]);
+        r[i] = ri;
+        rz += double(ri) * double(ri * inv_diag[i]);
+    }
+    const double b = block_sum(rz, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = b;
+    if (last_block(&s->count_c)) {
+        const double t = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            s->count_c = 0;
+            s->beta = t / s->rz;
+            s->rz = t;
+        }
+    }
+}
+
+// Mixed precision: FP32-stored K inside an FP64 defect correction, run as a
+// single Jacobi-PCG with reliable updates.  The sloppy segments stream the
+// FP32 copy of K (vectors, u and dots stay FP64).  A segment ends when its
+// recursive residual has dropped by `delta` or after `seg_cap` iterations;
+// the host then computes the true residual r = f - K64 u with the FP64
+// operator, replaces the recursive one with it and resumes with the same
+// search direction (the Krylov space is kept).  The FP32 operator differs
+// from K by ~1e-7 per entry, so on an ill-conditioned system the true
+// residual stops improving well above 1e-10; once it fails to halve over two
+// segments the same CG continues with the FP64 operator to the tolerance.
+// The bulk of the iterations stream 4 B instead of 8 B per nonzero.
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps) {
+    (void)check_every;
+    const double delta = (inner_tol > 0.01 && inner_tol < 1.0) ? inner_tol : 0.1;
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
-    if (check_every <= 0) check_every = auto_check_every(n, op->pat.nnz);
-    const int G = pick_node_group(op->pat.max_deg);
-    // FP32 copies of K and the Jacobi diagonal
     if (!op->vals32.p) {
         op->vals32.alloc(ctx->pool, op->pat.nnz + 1);
         to_float_kernel<<<grid_vec(ctx, op->pat.nnz), BLOCK, 0, st>>>(op->pat.nnz, op->vals.p,
                                                                        op->vals32.p);
         SVX_LAUNCH_CHECK();
     }
-    DBuf<float> inv32, r32, p32, q32, d32;
-    DBuf<double> r64, partials, rr_dev;
+    const int G = pick_node_group(op->pat.max_deg);
+    DBuf<double> r, p, q, r64, partials, rr_dev;
     DBuf<PcgScalars> s;
     DBuf<unsigned int> counter;
-    inv32.alloc(ctx->pool, n + 1);
-    r32.alloc(ctx->pool, n + 1);
-    p32.alloc(ctx->pool, n + 1);
-    q32.alloc(ctx->pool, n + 1);
-    d32.alloc(ctx->pool, n + 1);
+    r.alloc(ctx->pool, n + 1);
+    p.alloc(ctx->pool, n + 1);
+    q.alloc(ctx->pool, n + 1);
     r64.alloc(ctx->pool, n + 1);
     rr_dev.alloc(ctx->pool, 1);
     counter.alloc(ctx->pool, 1);
     SVX_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned int), st));
-    to_float_kernel<<<grid_vec(ctx, n), BLOCK, 0, st>>>(n, op->inv_diag.p, inv32.p);
-    SVX_LAUNCH_CHECK();
-    PcgRun<float, float> run;
-    run.ctx = ctx;
-    run.op = op;
-    run.n = n;
-    run.G = G;
-    run.grid_r = grid_rows(ctx, n, G);
-    run.grid_v = grid_vec(ctx, n);
-    partials.alloc(ctx->pool, 2 * size_t(std::max(run.grid_r, run.grid_v)) + 2);
+    const unsigned grid_r = grid_nodes(ctx, op->n_nodes, G), grid_v = grid_vec(ctx, n);
+    partials.alloc(ctx->pool, 2 * size_t(std::max(grid_r, grid_v)) + 2);
     s.alloc(ctx->pool, 1);
     PinnedScalars hs;
-    run.vals = op->vals32.p;
-    run.inv_diag = inv32.p;
-    run.u = d32.p;
-    run.r = r32.p;
-    run.p = p32.p;
-    run.q = q32.p;
-    run.partials = partials.p;
-    run.s = s.p;
-    run.h_s = hs.h;
+    PcgRun<float, double, double> sloppy;
+    PcgRun<double, double, double> exact;
+    auto wire = [&](auto& run) {
+        run.ctx = ctx;
+        run.op = op;
+        run.n = n;
+        run.G = G;
+        run.grid_r = grid_r;
+        run.grid_v = grid_v;
+        run.inv_diag = op->inv_diag.p;
+        run.u = u_dev;
+        run.r = r.p;
+        run.p = p.p;
+        run.q = q.p;
+        run.partials = partials.p;
+        run.s = s.p;
+        run.h_s = hs.h;
+    };
+    wire(sloppy);
+    wire(exact);
+    sloppy.vals = op->vals32.p;
+    exact.vals = op->vals.p;
 
-    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
-    SVX_CUDA(cudaMemsetAsync(u_dev, 0, n * sizeof(double), st));
-    // ||f||
-    double* h_rr = &hs.h->rr;  // scratch slot of the pinned struct
     auto true_residual = [&]() -> double {
-        const unsigned grid = grid_nodes(ctx, op->n_nodes, G);
         const Pattern& P = op->pat;
         SVX_NODE_DISPATCH(op->ndof, G,
-                          (residual_node_kernel<ND, GG><<<grid, BLOCK, 0, st>>>(
+                          (residual_node_kernel<ND, GG><<<grid_r, BLOCK, 0, st>>>(
                               op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p, u_dev,
                               op->f.p, r64.p, partials.p, counter.p, rr_dev.p)));
         SVX_LAUNCH_CHECK();
-        SVX_CUDA(cudaMemcpyAsync(h_rr, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        double h = 0.0;
+        SVX_CUDA(cudaMemcpyAsync(&h, rr_dev.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         SVX_CUDA(cudaStreamSynchronize(st));
-        return *h_rr;
+        return h;
     };
-    double ff = true_residual();  // u = 0: r = f
-    double bnorm = std::sqrt(ff);
-    PcgResult out{PCG_CONVERGED, 0, 0.0, 0.0};
-    long long total_inner = 0, outer = 0;
-    double res = bnorm == 0.0 ? 0.0 : 1.0;
-    double rnorm = bnorm;
-    int status = PCG_CONVERGED;
-    const int max_outer = 200;
-    while (bnorm != 0.0) {
+    auto set_field = [&](auto PcgScalars::*field, auto value) {
+        SVX_CUDA(cudaMemcpyAsync(&(s.p->*field), &value, sizeof(value), cudaMemcpyHostToDevice,
+                                 st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+    };
+
+    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+    PcgScalars init{};
+    init.tol = tol;
+    init.max_iter = max_iter;
+    init.status = PCG_RUNNING;
+    SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    init_kernel<double, double, double><<<grid_v, BLOCK, 0, st>>>(
+        n, op->f.p, 1.0, u_dev, r.p, p.p, op->inv_diag.p, partials.p, s.p);
+    SVX_LAUNCH_CHECK();
+    SVX_CUDA(cudaMemcpyAsync(hs.h, s.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    SVX_CUDA(cudaStreamSynchronize(st));
+    const double bnorm = hs.h->bnorm;
+    const long long seg_cap = 500;
+    int status = hs.h->status;
+    long long outer = 0, sloppy_iters = 0;
+    double res = hs.h->res;
+    double best_true = 1.0;
+    int stagnant = 0;
+    bool fp64_phase = false;
+    set_field(&PcgScalars::rr_stop, delta * delta * hs.h->rr);
+    set_field(&PcgScalars::max_iter, std::min(max_iter, seg_cap));
+    const int chunk = persistent_chunk(op->pat.nnz);
+    while (status == PCG_RUNNING) {
+        if (fp64_phase) {
+            status = exact.iterate_persistent(chunk);
+            res = hs.h->res;
+            break;
+        }
+        status = sloppy.iterate_persistent(chunk);
+        if (status < 0)
+            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                            "mixed precision needs cooperative launch (persistent PCG)"};
+        sloppy_iters = hs.h->it;
+        if (status == PCG_BREAKDOWN) break;
+        // segment ended (reduced by delta, capped, or sloppy-converged):
+        // true FP64 residual and reliable update
+        ++outer;
+        const double rr_true = true_residual();
+        res = std::sqrt(rr_true) / bnorm;
         if (res <= tol) {
             status = PCG_CONVERGED;
             break;
         }
-        if (outer >= max_outer || total_inner >= max_iter) {
+        if (hs.h->it >= max_iter) {
             status = PCG_MAXITER;
             break;
         }
-        ++outer;
-        // inner solve K32 d = r / ||r|| in FP32 with FP64 dots
-        PcgScalars init{};
-        init.tol = inner_tol;
-        init.max_iter = std::max<long long>(1, max_iter - total_inner);
-        init.status = PCG_RUNNING;
-        SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
-        init_kernel<float, double><<<run.grid_v, BLOCK, 0, st>>>(
-            n, r64.p, 1.0 / rnorm, d32.p, r32.p, p32.p, inv32.p, partials.p, s.p);
-        SVX_LAUNCH_CHECK();
-        int inner_status = run.iterate_persistent(persistent_chunk(op->pat.nnz));
-        if (inner_status < 0) inner_status = run.iterate(check_every);
-        total_inner += hs.h->it;
-        if (inner_status == PCG_BREAKDOWN && hs.h->it <= 1) {
-            status = PCG_BREAKDOWN;
-            break;
+        if (res < 0.5 * best_true) {
+            best_true = res;
+            stagnant = 0;
+        } else {
+            ++stagnant;
         }
-        correct_kernel<<<run.grid_v, BLOCK, 0, st>>>(n, u_dev, d32.p, rnorm);
+        fp64_phase = stagnant >= 2;
+        reliable_resume_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, r64.p, r.p, op->inv_diag.p,
+                                                                partials.p, s.p);
         SVX_LAUNCH_CHECK();
-        double rr = true_residual();
-        double new_norm = std::sqrt(rr);
-        double new_res = new_norm / bnorm;
-        if (!(new_res < res)) {  // no progress: the FP32 operator cannot refine further
-            res = new_res;
-            rnorm = new_norm;
-            status = (new_res <= tol) ? PCG_CONVERGED : PCG_BREAKDOWN;
-            break;
-        }
-        res = new_res;
-        rnorm = new_norm;
+        set_field(&PcgScalars::rr, rr_true);
+        set_field(&PcgScalars::res, res);
+        set_field(&PcgScalars::rr_stop, fp64_phase ? -1.0 : delta * delta * rr_true);
+        set_field(&PcgScalars::max_iter,
+                  fp64_phase ? max_iter : std::min(max_iter, hs.h->it + seg_cap));
+        set_field(&PcgScalars::status, int(PCG_RUNNING));
+        p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p.p, r.p, op->inv_diag.p, s.p);
+        SVX_LAUNCH_CHECK();
+        status = PCG_RUNNING;
     }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
     SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
     float ms = 0.f;
     SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-    out.status = status;
-    out.iterations = total_inner;
-    out.residual = res;
-    out.ms = ms;
+    SVX_CUDA(cudaMemcpyAsync(hs.h, s.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    SVX_CUDA(cudaStreamSynchronize(st));
+    PcgResult out{status, hs.h->it, res, ms};
+    op->mixed_sloppy_iters = sloppy_iters;
     if (outer_steps) *outer_steps = outer;
     return out;
 }
