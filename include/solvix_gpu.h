@@ -271,6 +271,40 @@ int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol
  * (stress.rs:22-118) and the displacement packaging of lib.rs:689-698. */
 int svx_op_stress(svx_op_t* op, svx_solution_t* sol);
 
+/* ---- batched solves (many independent models in one launch) -------- */
+typedef struct svx_batch_result {
+    int64_t iterations;    /* PCG iterations of this model */
+    double residual;       /* recursive ||r||/||f|| at exit */
+    int32_t status;        /* SVX_OK or SVX_NOT_CONVERGED */
+    int32_t pad;
+    double cond_estimate;  /* max|diag| / min|diag| of this model's modified K */
+} svx_batch_result_t;
+
+typedef struct svx_batch_stats {
+    double ms_assemble;    /* device time: all models' K1-K4 */
+    double ms_solve;       /* device time of the batched PCG launch */
+    double ms_stress;      /* device time of the centroid von Mises */
+    int32_t threads_per_cta;  /* autotuned CTA size of the batched PCG */
+    int32_t lanes_per_node;   /* autotuned lanes per node of its SpMV */
+    int64_t total_iterations; /* sum over models */
+    int64_t total_dof;        /* sum over models */
+    int32_t not_converged;    /* models that missed tol within their budget */
+    int32_t pad;
+} svx_batch_stats_t;
+
+/* Solves `count` independent models of equal ndof (FP64 form).  They are
+ * assembled as one block-diagonal operator; one persistent launch then runs
+ * every model's Jacobi-PCG with its own scalars, convergence test and
+ * iteration budget (max(1000, 10 n_model) unless opts->max_iter > 0), one
+ * CTA per model at a time, largest models first.  The CTA size and lanes
+ * per node are autotuned once per context and ndof, and kept.  Per model
+ * outputs: u[k] (n_nodes*ndof) and von_mises[k] (n_elem), host arrays, any
+ * may be NULL.  A model that fails assembly rejects the batch (InvalidModel,
+ * message prefixed with "model k: "). */
+int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* models,
+                    const svx_solve_opts_t* opts, double* const* u, double* const* von_mises,
+                    svx_batch_result_t* results, svx_batch_stats_t* stats, svx_error_t* err);
+
 /* ---- measurement --------------------------------------------------- */
 /* Kernels this process has launched through the library (graph nodes count
  * when their graph is launched). */

@@ -140,6 +140,30 @@ class SvxSolution(C.Structure):
     ]
 
 
+class SvxBatchResult(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int64),
+        ("residual", C.c_double),
+        ("status", C.c_int32),
+        ("pad", C.c_int32),
+        ("cond_estimate", C.c_double),
+    ]
+
+
+class SvxBatchStats(C.Structure):
+    _fields_ = [
+        ("ms_assemble", C.c_double),
+        ("ms_solve", C.c_double),
+        ("ms_stress", C.c_double),
+        ("threads_per_cta", C.c_int32),
+        ("lanes_per_node", C.c_int32),
+        ("total_iterations", C.c_int64),
+        ("total_dof", C.c_int64),
+        ("not_converged", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
 def ptr(a: np.ndarray | None, ctype):
     """Pointer to a contiguous numpy array (or NULL)."""
     if a is None:
@@ -176,6 +200,10 @@ SIGNATURES = {
     "svx_op_solve": (C.c_int, [_VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),
                                C.POINTER(SvxError)]),
     "svx_op_stress": (C.c_int, [_VP, C.POINTER(SvxSolution)]),
+    "svx_batch_solve": (C.c_int, [_VP, C.c_int32, C.POINTER(SvxFlatModel),
+                                  C.POINTER(SvxSolveOpts), C.POINTER(c_double_p),
+                                  C.POINTER(c_double_p), C.POINTER(SvxBatchResult),
+                                  C.POINTER(SvxBatchStats), C.POINTER(SvxError)]),
     "svx_solve_flat": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.POINTER(SvxSolveOpts),
                                  C.POINTER(SvxSolution), C.POINTER(SvxError)]),
     "svx_solve_resolved": (C.c_int, [_VP, _VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),

@@ -104,6 +104,38 @@ class Context:
             _raise(st, err)
         return out.solution(flat, precision)
 
+    def solve_batch(self, flats, tol: float = 1e-10, max_iter: int = 0, want_u: bool = True,
+                    want_stress: bool = True):
+        """Solve many independent FlatModels (equal ndof) in one batched launch.
+
+        Returns (list of per-model dicts with u / von_mises / iterations /
+        residual / converged / cond_estimate, stats dict).
+        """
+        flats = list(flats)
+        count = len(flats)
+        structs = (abi.SvxFlatModel * count)(*[f.as_struct() for f in flats])
+        us = [np.zeros(f.n_dof) if want_u else None for f in flats]
+        vms = [np.zeros(f.n_elem) if want_stress else None for f in flats]
+        u_ptrs = (abi.c_double_p * count)(*[abi.ptr(a, C.c_double) for a in us])
+        vm_ptrs = (abi.c_double_p * count)(*[abi.ptr(a, C.c_double) for a in vms])
+        results = (abi.SvxBatchResult * count)()
+        stats = abi.SvxBatchStats()
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, want_stress=int(want_stress))
+        err = abi.SvxError()
+        st = self.lib.svx_batch_solve(self.handle, count, structs, C.byref(opts),
+                                      u_ptrs if want_u else None,
+                                      vm_ptrs if want_stress else None, results,
+                                      C.byref(stats), C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        out = [{"u": us[k], "von_mises": vms[k], "iterations": int(results[k].iterations),
+                "residual": float(results[k].residual),
+                "converged": results[k].status == abi.SVX_OK,
+                "cond_estimate": float(results[k].cond_estimate)} for k in range(count)]
+        st_d = {name: getattr(stats, name) for name, _ in abi.SvxBatchStats._fields_
+                if name != "pad"}
+        return out, st_d
+
     def solve_model(self, model: Model, tol: float = 1e-10, precision: int = abi.SVX_FP64,
                     inner_tol: float = 1e-5) -> Solution:
         """The reference-shaped path: resolve ids / sets on the host (C++),

@@ -262,7 +262,8 @@ void device_assemble(svx_ctx* ctx, svx_op* op) {
 }
 
 // K1-K4 for a validated flat model; throws ModelFail for element errors.
-svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
+svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags,
+                      const double* thick_elem = nullptr) {
     SVX_CUDA(cudaSetDevice(ctx->device));
     check_flat(m);
     // ndof_per_node (lib.rs:725-752) runs before assembly
@@ -307,6 +308,7 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags) {
     upload(ctx, op->conn, m->conn, size_t(op->n_elem > 0 ? m->conn_ptr[op->n_elem] : 0));
     upload(ctx, op->youngs, m->youngs, size_t(op->n_elem));
     upload(ctx, op->poisson, m->poisson, size_t(op->n_elem));
+    if (thick_elem) upload(ctx, op->thick_elem, thick_elem, size_t(op->n_elem));
     int max_nn = 0;
     for (int64_t e = 0; e < op->n_elem; ++e) max_nn = std::max(max_nn, node_count(m->kind[e]));
     op->pat.max_nn = std::max(max_nn, 1);
@@ -638,6 +640,144 @@ int svx_op_stress(svx_op_t* op, svx_solution_t* sol) {
                                      cudaMemcpyDeviceToHost, st));
         sol->ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
         SVX_CUDA(cudaStreamSynchronize(st));
+        return SVX_OK;
+    });
+}
+
+int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* models,
+                    const svx_solve_opts_t* opts, double* const* u, double* const* von_mises,
+                    svx_batch_result_t* results, svx_batch_stats_t* stats, svx_error_t* err) {
+    if (!ctx || count <= 0 || !models) return SVX_BAD_ARGUMENT;
+    return guarded(ctx, err, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        svx_solve_opts_t o;
+        svx_default_opts(&o);
+        if (opts) o = *opts;
+        if (o.precision != SVX_FP64)
+            throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "batched solves run the FP64 form"};
+        const int ndof = models[0].ndof;
+        // concatenate into one block-diagonal model
+        int64_t nn = 0, ne = 0, nc = 0, nf = 0;
+        for (int32_t k = 0; k < count; ++k) {
+            const svx_flat_model_t& m = models[k];
+            try {
+                check_flat(&m);
+            } catch (const ModelFail& f) {
+                throw ModelFail{f.code, f.reason, f.elem_index,
+                                "model " + std::to_string(k) + ": " + f.message};
+            }
+            if (m.ndof != ndof)
+                throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "models of one batch share ndof"};
+            for (int64_t e = 0; e < m.n_elem; ++e) {
+                const int r = material_reason(&m, e);
+                if (r)
+                    throw ModelFail{SVX_INVALID_MODEL, r, e,
+                                    "model " + std::to_string(k) + ": " +
+                                        element_message(&m, e, r)};
+            }
+            nn += m.n_nodes;
+            ne += m.n_elem;
+            nc += m.n_elem ? m.conn_ptr[m.n_elem] : 0;
+            nf += m.n_fixed;
+        }
+        const size_t une = static_cast<size_t>(ne);
+        std::vector<double> xyz(static_cast<size_t>(3 * nn)), E(une), nu(une), th(une);
+        std::vector<double> f(static_cast<size_t>(nn * ndof), 0.0);
+        std::vector<uint8_t> kind(une);
+        std::vector<int64_t> conn_ptr(une + 1, 0), fixed;
+        std::vector<int32_t> conn(static_cast<size_t>(nc));
+        std::vector<int64_t> node_off(static_cast<size_t>(count) + 1, 0);
+        std::vector<int64_t> elem_off(static_cast<size_t>(count) + 1, 0);
+        fixed.reserve(size_t(nf));
+        for (int32_t k = 0; k < count; ++k) {
+            const svx_flat_model_t& m = models[k];
+            const int64_t n0 = node_off[k], e0 = elem_off[k];
+            std::memcpy(xyz.data() + 3 * n0, m.xyz, sizeof(double) * 3 * m.n_nodes);
+            if (m.f) std::memcpy(f.data() + n0 * ndof, m.f, sizeof(double) * m.n_nodes * ndof);
+            const int64_t c0 = conn_ptr[e0];
+            for (int64_t e = 0; e < m.n_elem; ++e) {
+                kind[e0 + e] = m.kind[e];
+                E[e0 + e] = m.youngs[e];
+                nu[e0 + e] = m.poisson[e];
+                th[e0 + e] = m.thickness;
+                conn_ptr[e0 + e + 1] = c0 + m.conn_ptr[e + 1];
+            }
+            for (int64_t q = 0; q < (m.n_elem ? m.conn_ptr[m.n_elem] : 0); ++q)
+                conn[c0 + q] = int32_t(m.conn[q] + n0);
+            for (int64_t j = 0; j < m.n_fixed; ++j) fixed.push_back(m.fixed_row[j] + n0 * ndof);
+            node_off[k + 1] = n0 + m.n_nodes;
+            elem_off[k + 1] = e0 + m.n_elem;
+        }
+        svx_flat_model_t all{};
+        all.n_nodes = nn;
+        all.xyz = xyz.data();
+        all.n_elem = ne;
+        all.kind = kind.data();
+        all.conn_ptr = conn_ptr.data();
+        all.conn = conn.data();
+        all.youngs = E.data();
+        all.poisson = nu.data();
+        all.thickness = 1.0;
+        all.ndof = ndof;
+        all.n_fixed = int64_t(fixed.size());
+        all.fixed_row = fixed.data();
+        all.f = f.data();
+        std::unique_ptr<svx_op> op(assemble_impl(ctx, &all, 0, th.data()));
+        std::vector<double> tol(static_cast<size_t>(count), o.tol);
+        std::vector<int64_t> mi(static_cast<size_t>(count));
+        for (int32_t k = 0; k < count; ++k)
+            mi[k] = o.max_iter > 0 ? o.max_iter
+                                   : default_max_iter((node_off[k + 1] - node_off[k]) * ndof);
+        std::vector<int64_t> it;
+        std::vector<double> res, cond;
+        std::vector<int32_t> status;
+        BatchStats bs;
+        batch_pcg(ctx, op.get(), count, node_off, tol, mi, it, res, status, cond, &bs);
+        cudaStream_t st = ctx->stream;
+        double ms_stress = 0.0;
+        if (von_mises && o.want_stress) {
+            SVX_CUDA(cudaEventRecord(ctx->ev[4], st));
+            if (!op->vm_elem.p) op->vm_elem.alloc(ctx->pool, op->n_elem + 1);
+            recover_stress(ctx, op.get(), op->u.p, op->vm_elem.p, nullptr, nullptr, nullptr);
+            SVX_CUDA(cudaEventRecord(ctx->ev[5], st));
+            ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+            for (int32_t k = 0; k < count; ++k)
+                if (von_mises[k] && elem_off[k + 1] > elem_off[k])
+                    SVX_CUDA(cudaMemcpyAsync(von_mises[k], op->vm_elem.p + elem_off[k],
+                                             (elem_off[k + 1] - elem_off[k]) * sizeof(double),
+                                             cudaMemcpyDeviceToHost, st));
+        }
+        if (u)
+            for (int32_t k = 0; k < count; ++k)
+                if (u[k])
+                    SVX_CUDA(cudaMemcpyAsync(u[k], op->u.p + node_off[k] * ndof,
+                                             (node_off[k + 1] - node_off[k]) * ndof *
+                                                 sizeof(double),
+                                             cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        int64_t total_it = 0;
+        int failed = 0;
+        for (int32_t k = 0; k < count; ++k) {
+            if (results) {
+                results[k].iterations = it[k];
+                results[k].residual = res[k];
+                results[k].status = status[k] == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
+                results[k].cond_estimate = cond[k];
+            }
+            total_it += it[k];
+            failed += status[k] != PCG_CONVERGED;
+        }
+        if (stats) {
+            stats->ms_assemble = op->ms_assemble;
+            stats->ms_solve = bs.ms_solve;
+            stats->ms_stress = ms_stress;
+            stats->threads_per_cta = bs.threads_per_cta;
+            stats->lanes_per_node = bs.lanes_per_node;
+            stats->total_iterations = total_it;
+            stats->total_dof = nn * ndof;
+            stats->not_converged = failed;
+        }
+        clear_error(err);
         return SVX_OK;
     });
 }

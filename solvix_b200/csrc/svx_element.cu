@@ -214,7 +214,8 @@ __global__ void __launch_bounds__(WARPS * 32)
 integrate_kernel(int64_t n_elem, const uint8_t* __restrict__ kind,
                  const int64_t* __restrict__ conn_ptr, const int32_t* __restrict__ conn,
                  const double* __restrict__ xyz, const double* __restrict__ youngs,
-                 const double* __restrict__ poisson, double thickness,
+                 const double* __restrict__ poisson, double thickness_all,
+                 const double* __restrict__ thick_elem,
                  double* __restrict__ ke_out, int ke_stride,
                  unsigned long long* __restrict__ first_fail) {
     __shared__ ElemSmem smem[WARPS];
@@ -230,6 +231,7 @@ integrate_kernel(int64_t n_elem, const uint8_t* __restrict__ kind,
         if (lane < nn * 3) sm.xyz[lane] = xyz[int64_t(conn[q0 + lane / 3]) * 3 + lane % 3];
         __syncwarp();
         const double E = youngs[e], nu = poisson[e];
+        const double thickness = thick_elem ? thick_elem[e] : thickness_all;
         const int N = (k == SVX_C3D8) ? 24 : nn * 2;
         const int n_pairs = N * (N + 1) / 2;
         int pa[MAX_PAIRS_PER_LANE], pc[MAX_PAIRS_PER_LANE];
@@ -651,7 +653,7 @@ uint64_t integrate_elements(svx_ctx* ctx, svx_op* op, double* ke, int ke_stride)
         if (blocks > cap) blocks = cap;
         integrate_kernel<<<unsigned(blocks), WARPS * 32, 0, ctx->stream>>>(
             op->n_elem, op->kind.p, op->conn_ptr.p, op->conn.p, op->xyz.p, op->youngs.p,
-            op->poisson.p, op->thickness, ke, ke_stride, fail.p);
+            op->poisson.p, op->thickness, op->thick_elem.p, ke, ke_stride, fail.p);
         SVX_LAUNCH_CHECK();
     }
     unsigned long long h = 0;

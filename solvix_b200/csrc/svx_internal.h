@@ -107,6 +107,7 @@ struct DBuf {
 struct svx_ctx {
     int device = 0;
     int sm_count = 0;
+    int batch_choice[2] = {-1, -1};  // autotuned batched-PCG config per ndof (2, 3)
     cudaStream_t stream = nullptr;
     svx::DevicePool* pool = nullptr;
     std::string last_error;
@@ -182,6 +183,7 @@ struct svx_op {
     svx::DBuf<int64_t> conn_ptr;
     svx::DBuf<int32_t> conn;
     svx::DBuf<double> youngs, poisson;
+    svx::DBuf<double> thick_elem;  // per-element thickness (batched models), else empty
     svx::Pattern pat;
     // assembled system
     svx::DBuf<double> vals;        // K after Dirichlet (the PCG operator)
@@ -251,6 +253,18 @@ int choose_spmv_group(const svx_op* op);
 // Average device time (ms) of the three FP64 PCG iteration kernels
 // (spmv_dot, update, p_update) over `reps` back-to-back launches each.
 void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3);
+
+// Batched PCG over a block-diagonal concatenation of independent models
+// (svx_pcg.cu).  node_off[count + 1] delimits each instance's nodes.
+struct BatchStats {
+    double ms_solve = 0.0;
+    int threads_per_cta = 0;
+    int lanes_per_node = 0;
+};
+void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& node_off,
+               const std::vector<double>& tol, const std::vector<int64_t>& max_iter,
+               std::vector<int64_t>& it, std::vector<double>& res, std::vector<int32_t>& status,
+               std::vector<double>& cond, BatchStats* stats);
 
 // Generic device helpers (svx_pattern.cu).
 void exclusive_scan_i64(svx_ctx* ctx, const int64_t* in, int64_t* out, int64_t n,

@@ -693,6 +693,178 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
     }
 }
 
+
+// ------------------------------------------------------------ batched PCG
+// Thousands of independent models concatenated into one block-diagonal
+// operator.  One launch; each CTA takes the next instance from an atomic
+// queue (instances ordered by size, largest first) and runs that instance's
+// whole Jacobi-PCG with CTA-local reductions, so every instance has its own
+// alpha/beta, its own convergence test and its own iteration count, and no
+// CTA ever waits for another.  An instance is always computed by one CTA of
+// the same shape, so its result does not depend on what else is in the
+// batch.
+template <int ND, int G, class M>
+__device__ __forceinline__ void node_rows_mv(const int64_t* __restrict__ adj_ptr,
+                                             const int32_t* __restrict__ adj,
+                                             const int64_t* __restrict__ node_base,
+                                             const M* __restrict__ vals, const double* x,
+                                             int64_t i, int gl, double* acc) {
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const M* __restrict__ v = vals + node_base[i];
+    if (d == 0) {
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = double(v[da]) * x[i * ND + da];
+        return;
+    }
+    const int rowlen = ND * d;
+    for (int k = gl; k < d; k += G) {
+        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xv[db] = x[c + db];
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                acc[da] += double(__ldg(v + da * rowlen + k * ND + db)) * xv[db];
+    }
+}
+
+template <int ND, int G, int BS, class M>
+__global__ void __launch_bounds__(BS)
+batch_pcg_kernel(int count, const int32_t* __restrict__ order, const int64_t* __restrict__ node_off,
+                 const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj,
+                 const int64_t* __restrict__ node_base, const M* __restrict__ vals,
+                 const double* __restrict__ inv_diag, const double* __restrict__ f, double* u,
+                 double* r, double* p, double* q, const double* __restrict__ tol,
+                 const int64_t* __restrict__ max_iter, int64_t* __restrict__ out_it,
+                 double* __restrict__ out_res, int32_t* __restrict__ out_status,
+                 unsigned int* queue) {
+    __shared__ double sh[32];
+    __shared__ int next;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t warp_nodes = 32 / G;
+    const int64_t step = int64_t(BS / 32) * warp_nodes;
+    for (;;) {
+        if (threadIdx.x == 0) next = int(atomicAdd(queue, 1u));
+        __syncthreads();
+        const int k = next;
+        __syncthreads();
+        if (k >= count) return;
+        const int inst = order[k];
+        const int64_t n0 = node_off[inst], n1 = node_off[inst + 1];
+        const int64_t r0 = n0 * ND, r1 = n1 * ND;
+        const double tl = tol[inst];
+        const int64_t mi = max_iter[inst];
+        double rr = 0.0, rz = 0.0;
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+            const double ri = f[row];
+            u[row] = 0.0;
+            r[row] = ri;
+            const double zi = ri * inv_diag[row];
+            p[row] = zi;
+            rr += ri * ri;
+            rz += ri * zi;
+        }
+        rr = block_sum(rr, sh);
+        rz = block_sum(rz, sh);
+        const double bnorm = sqrt(rr);
+        int64_t it = 0;
+        int status = (bnorm == 0.0) ? PCG_CONVERGED : PCG_RUNNING;
+        double res = (bnorm == 0.0) ? 0.0 : 1.0;
+        while (status == PCG_RUNNING) {
+            double dot = 0.0;
+            for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1; nb += step) {
+                const int64_t i = nb + ((threadIdx.x & 31) / G);
+                double acc[ND];
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                if (i < n1) node_rows_mv<ND, G, M>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                if (i < n1 && gl == 0) {
+#pragma unroll
+                    for (int da = 0; da < ND; ++da) {
+                        q[i * ND + da] = acc[da];
+                        dot += p[i * ND + da] * acc[da];
+                    }
+                }
+            }
+            const double pap = block_sum(dot, sh);
+            if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
+                status = PCG_BREAKDOWN;
+                it += 1;
+                res = sqrt(rr) / bnorm;
+                break;
+            }
+            const double alpha = rz / pap;
+            double lrr = 0.0, lrz = 0.0;
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+                u[row] += alpha * p[row];
+                const double ri = r[row] - alpha * q[row];
+                r[row] = ri;
+                const double zi = ri * inv_diag[row];
+                lrr += ri * ri;
+                lrz += ri * zi;
+            }
+            rr = block_sum(lrr, sh);
+            const double rz_new = block_sum(lrz, sh);
+            it += 1;
+            res = sqrt(rr) / bnorm;
+            if (res <= tl) {
+                status = PCG_CONVERGED;
+                break;
+            }
+            if (it >= mi) {
+                status = PCG_MAXITER;
+                break;
+            }
+            const double beta = rz_new / rz;
+            rz = rz_new;
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS)
+                p[row] = r[row] * inv_diag[row] + beta * p[row];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            out_it[inst] = it;
+            out_res[inst] = res;
+            out_status[inst] = status;
+        }
+    }
+}
+
+// Extreme |K_ii| of each instance (its cond_estimate), one CTA per instance.
+__global__ void instance_diag_kernel(int ndof, const int64_t* __restrict__ node_off,
+                                     const int32_t* __restrict__ diag_pos,
+                                     const double* __restrict__ vals, double* __restrict__ hi,
+                                     double* __restrict__ lo) {
+    __shared__ double shi[256], slo[256];
+    const int inst = blockIdx.x;
+    const int64_t r0 = node_off[inst] * ndof, r1 = node_off[inst + 1] * ndof;
+    double h = 0.0, l = INFINITY;
+    for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+        const double a = fabs(vals[diag_pos[row]]);
+        h = fmax(h, a);
+        l = fmin(l, a);
+    }
+    shi[threadIdx.x] = h;
+    slo[threadIdx.x] = l;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            shi[threadIdx.x] = fmax(shi[threadIdx.x], shi[threadIdx.x + off]);
+            slo[threadIdx.x] = fmin(slo[threadIdx.x], slo[threadIdx.x + off]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        hi[inst] = shi[0];
+        lo[inst] = slo[0];
+    }
+}
+
 // ------------------------------------------------------------ host side
 int pick_group(double mean_row) {
     if (mean_row < 6) return 2;
@@ -1401,3 +1573,144 @@ extern "C" int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const in
     if (residual) *residual = h.res;
     return h.status == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
 }
+
+namespace svx {
+
+// ------------------------------------------------------------ batched host
+namespace {
+
+using BatchFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*, const int32_t*,
+                         const int64_t*, const double*, const double*, const double*, double*,
+                         double*, double*, double*, const double*, const int64_t*, int64_t*,
+                         double*, int32_t*, unsigned int*);
+
+struct BatchConfig {
+    int nd, g, bs;
+    BatchFn fn;
+};
+
+template <int ND, int G, int BS>
+BatchConfig batch_config() {
+    return BatchConfig{ND, G, BS, &batch_pcg_kernel<ND, G, BS, double>};
+}
+
+std::vector<BatchConfig> batch_candidates(int ndof) {
+    if (ndof == 3)
+        return {batch_config<3, 16, 128>(), batch_config<3, 16, 256>(), batch_config<3, 16, 512>(),
+                batch_config<3, 32, 256>(), batch_config<3, 32, 512>()};
+    return {batch_config<2, 8, 128>(), batch_config<2, 8, 256>(), batch_config<2, 8, 512>(),
+            batch_config<2, 16, 256>(), batch_config<2, 16, 512>()};
+}
+
+}  // namespace
+
+void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& node_off,
+               const std::vector<double>& tol, const std::vector<int64_t>& max_iter,
+               std::vector<int64_t>& it, std::vector<double>& res, std::vector<int32_t>& status,
+               std::vector<double>& cond, BatchStats* stats) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = op->n;
+    const Pattern& P = op->pat;
+    // largest instances first (longest-processing-time order for the queue)
+    std::vector<int32_t> order(count);
+    for (int k = 0; k < count; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return node_off[a + 1] - node_off[a] > node_off[b + 1] - node_off[b];
+    });
+    DBuf<int32_t> d_order, d_status;
+    DBuf<int64_t> d_off, d_maxit, d_it, d_cap;
+    DBuf<double> d_tol, d_res, r, p, q, d_hi, d_lo;
+    DBuf<unsigned int> queue;
+    d_order.alloc(ctx->pool, count + 1);
+    d_off.alloc(ctx->pool, count + 1);
+    d_maxit.alloc(ctx->pool, count + 1);
+    d_cap.alloc(ctx->pool, count + 1);
+    d_it.alloc(ctx->pool, count + 1);
+    d_tol.alloc(ctx->pool, count + 1);
+    d_res.alloc(ctx->pool, count + 1);
+    d_status.alloc(ctx->pool, count + 1);
+    d_hi.alloc(ctx->pool, count + 1);
+    d_lo.alloc(ctx->pool, count + 1);
+    queue.alloc(ctx->pool, 1);
+    r.alloc(ctx->pool, n + 1);
+    p.alloc(ctx->pool, n + 1);
+    q.alloc(ctx->pool, n + 1);
+    op->u.alloc(ctx->pool, n + 1);
+    SVX_CUDA(cudaMemcpyAsync(d_order.p, order.data(), count * sizeof(int32_t),
+                             cudaMemcpyHostToDevice, st));
+    SVX_CUDA(cudaMemcpyAsync(d_off.p, node_off.data(), (count + 1) * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, st));
+    SVX_CUDA(cudaMemcpyAsync(d_maxit.p, max_iter.data(), count * sizeof(int64_t),
+                             cudaMemcpyHostToDevice, st));
+    SVX_CUDA(cudaMemcpyAsync(d_tol.p, tol.data(), count * sizeof(double), cudaMemcpyHostToDevice,
+                             st));
+    auto launch = [&](const BatchConfig& c, const int64_t* maxit, int n_inst) {
+        int bps = 0;
+        SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)c.fn, c.bs, 0));
+        const int grid = std::max(1, std::min(bps * ctx->sm_count, n_inst));
+        SVX_CUDA(cudaMemsetAsync(queue.p, 0, sizeof(unsigned int), st));
+        c.fn<<<grid, c.bs, 0, st>>>(n_inst, d_order.p, d_off.p, P.adj_ptr.p, P.adj.p,
+                                    P.node_base.p, op->vals.p, op->inv_diag.p, op->f.p, op->u.p,
+                                    r.p, p.p, q.p, d_tol.p, maxit, d_it.p, d_res.p, d_status.p,
+                                    queue.p);
+        SVX_LAUNCH_CHECK();
+    };
+    // autotune (once per context and ndof): threads per CTA and lanes per
+    // node, timed on the largest instances with a short iteration budget
+    int& choice = ctx->batch_choice[op->ndof == 3 ? 1 : 0];
+    const std::vector<BatchConfig> cands = batch_candidates(op->ndof);
+    if (choice < 0) {
+        const int sample = std::min(count, 2 * ctx->sm_count);
+        std::vector<int64_t> cap(count, 40);
+        SVX_CUDA(cudaMemcpyAsync(d_cap.p, cap.data(), count * sizeof(int64_t),
+                                 cudaMemcpyHostToDevice, st));
+        float best = 0.f;
+        for (size_t c = 0; c < cands.size(); ++c) {
+            launch(cands[c], d_cap.p, sample);  // warm
+            SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+            launch(cands[c], d_cap.p, sample);
+            SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+            SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
+            float ms = 0.f;
+            SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+            if (choice < 0 || ms < best) {
+                best = ms;
+                choice = int(c);
+            }
+        }
+    }
+    const BatchConfig& cfg = cands[choice];
+    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+    launch(cfg, d_maxit.p, count);
+    SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+    instance_diag_kernel<<<count, 256, 0, st>>>(op->ndof, d_off.p, P.diag_pos.p, op->vals.p,
+                                                d_hi.p, d_lo.p);
+    SVX_LAUNCH_CHECK();
+    it.resize(count);
+    res.resize(count);
+    status.resize(count);
+    cond.resize(count);
+    std::vector<double> hi(count), lo(count);
+    SVX_CUDA(cudaMemcpyAsync(it.data(), d_it.p, count * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                             st));
+    SVX_CUDA(cudaMemcpyAsync(res.data(), d_res.p, count * sizeof(double), cudaMemcpyDeviceToHost,
+                             st));
+    SVX_CUDA(cudaMemcpyAsync(status.data(), d_status.p, count * sizeof(int32_t),
+                             cudaMemcpyDeviceToHost, st));
+    SVX_CUDA(cudaMemcpyAsync(hi.data(), d_hi.p, count * sizeof(double), cudaMemcpyDeviceToHost,
+                             st));
+    SVX_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, count * sizeof(double), cudaMemcpyDeviceToHost,
+                             st));
+    SVX_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    for (int k = 0; k < count; ++k) cond[k] = hi[k] / lo[k];
+    op->has_solution = true;
+    if (stats) {
+        stats->ms_solve = ms;
+        stats->threads_per_cta = cfg.bs;
+        stats->lanes_per_node = cfg.g;
+    }
+}
+
+}  // namespace svx
