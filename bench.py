@@ -50,6 +50,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=["plain", "batched", "precision"], default="plain",
+                    help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
+                         "2D plates in one launch; precision: FP64 vs mixed on the "
+                         "480x48x48 heterogeneous C3D8 model")
     return ap.parse_args()
 
 
@@ -347,6 +351,175 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+
+BATCH_NAME = ("4,096 independent 2D plates (nx~U{10..160}, ny~U{4..40}, h=1, CPS4 or CPS3 "
+              "p=0.5, E=10^U(9,log10 3e11), nu~U(0.15,0.45), t~U(0.001,0.05), left edge "
+              "clamped, one CLOAD U(100,1e4) N at a random right-edge node; seed 4), FP64 "
+              "Jacobi-PCG to 1e-10 per model, centroid von Mises")
+
+
+def run_batched(args, rank, world, local_rank):
+    """C4: the whole plate mix per step through svx_batch_solve; models are
+    sharded over ranks (greedy on estimated work, no collective)."""
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, workloads
+    from solvix_b200.sharding import shard_instances
+
+    torch.cuda.set_device(local_rank)
+    flats = workloads.plate_batch(4096, seed=4)
+    mine = shard_instances([f.n_dof for f in flats], world)[rank]
+    sub = [flats[k] for k in mine]
+    ctx = Context(local_rank)
+    lib = ctx.lib
+    for _ in range(max(args.warmup, 0)):
+        ctx.solve_batch(sub)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = lib.svx_launch_count()
+    dev_ms, wall_s, dof_it, bytes_alg = [], [], 0.0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out, st = ctx.solve_batch(sub)
+        wall_s.append(time.perf_counter() - t0)
+        dev_ms.append(st["ms_assemble"] + st["ms_solve"] + st["ms_stress"])
+        solve_ms = st["ms_solve"]
+        dof_it = float(sum(f.n_dof * o["iterations"] for f, o in zip(sub, out)))
+        # node-block SpMV (8 B value + 4 B per 2x2 / 3x3 block index) and the
+        # 13 FP64 vector streams, per iteration of each model
+        nd = sub[0].ndof
+        bytes_alg = float(sum(o["iterations"] * (o["nnz"] * (8 + 4 / (nd * nd)) + 104 * f.n_dof)
+                              for f, o in zip(sub, out)))
+    launches = lib.svx_launch_count() - launches0
+    clk = clocks.stop()
+    vals = torch.tensor([sum(dev_ms), sum(wall_s), dof_it], dtype=torch.float64,
+                        device=f"cuda:{local_rank}")
+    if world > 1:
+        mx = vals[:2].clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        tot = vals[2:].clone()
+        torch.distributed.all_reduce(tot, op=torch.distributed.ReduceOp.SUM)
+        vals = torch.cat([mx, tot])
+    ms_max, wall_max, dof_it_all = (float(v) for v in vals.tolist())
+    value = args.steps * dof_it_all / (ms_max / 1000.0)
+    e2e_value = args.steps * dof_it_all / wall_max
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_alg / (solve_ms / 1000.0) / 1e9
+    iters = np.array([o["iterations"] for o in out])
+    line = {
+        "metric": METRIC, "form": "batched", "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": BATCH_NAME, "models": len(flats),
+                   "total_dof": int(sum(f.n_dof for f in flats)),
+                   "parallelism": f"instances sharded over {world} GPU(s), no collective",
+                   "autotuned": {"threads_per_cta": st["threads_per_cta"],
+                                 "lanes_per_node": st["lanes_per_node"]}},
+        "solves_per_s": world * len(sub) * args.steps / (ms_max / 1000.0),
+        "iterations": {"min": int(iters.min()), "mean": float(iters.mean()),
+                       "max": int(iters.max())},
+        "ms_breakdown": {"assemble": st["ms_assemble"], "pcg": st["ms_solve"],
+                         "stress": st["ms_stress"]},
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "solves_per_s": len(flats) * args.steps / wall_max,
+                "h2d_bytes_per_step": int(sum(f.nbytes() for f in sub)),
+                "d2h_bytes_per_step": int(sum(8 * (f.n_dof + f.n_elem) for f in sub)),
+                "note": "svx_batch_solve from pageable host arrays, wall clock per call"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel (one launch per step)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": int(bytes_alg),
+                     "launch_ms": solve_ms, "traffic": None},
+        "clocks": clk,
+    }
+    if rank == 0:
+        # the one-at-a-time plain GPU path on a sample of the same models
+        rng = np.random.default_rng(0)
+        idx = rng.choice(len(flats), 64, replace=False)
+        ctx.solve_flat(flats[int(idx[0])])
+        t0 = time.perf_counter()
+        for k in idx:
+            ctx.solve_flat(flats[int(k)])
+        per = (time.perf_counter() - t0) / len(idx)
+        line["one_at_a_time"] = {
+            "solves_per_s": 1.0 / per,
+            "sample": "64 models of the mix through svx_solve_flat one after another "
+                      "(wall clock), projected to the set",
+            "speedup_device": line["solves_per_s"] * per,
+            "speedup_e2e": line["e2e"]["solves_per_s"] * per}
+    ctx.close()
+    return line
+
+
+PRECISION_NAME = ("C3D8 cantilever 480x48x48 over 2.0x0.2x0.2 m (1,154,881 nodes, 3,464,643 "
+                  "DOF, 272,673,225 nnz), per-element E=10^U(9,11) seed 3, nu=0.3, x=0 "
+                  "clamped, -5 kN in z over the x=L face; relative residual 1e-10")
+
+
+def run_precision(args, rank, world, local_rank):
+    """C3: plain FP64 and mixed solves of the heterogeneous model, from the
+    device-resident operator; error of mixed against FP64."""
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, abi, workloads
+
+    torch.cuda.set_device(local_rank)
+    flat = workloads.heterogeneous_c3d8(480, 48, 48, seed=3)
+    n = flat.n_dof
+    ctx = Context(local_rank)
+    op = ctx.assemble(flat)
+    res = {}
+    for name, prec in (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED)):
+        times, its = [], []
+        u = None
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            op.reassemble()
+            u, it, r, _c = op.solve(precision=prec, max_iter=200000)
+            times.append(time.perf_counter() - t0)
+            its.append(it)
+        res[name] = {"u": u, "iterations": its[-1], "s_per_solve": float(np.mean(times)),
+                     "residual": r}
+    kms = op.time_kernels(reps=10)
+    err = float(np.linalg.norm(res["mixed"]["u"] - res["fp64"]["u"]) /
+                np.linalg.norm(res["fp64"]["u"]))
+    peak, peak_kind = measured_peaks()
+    nnz = op.nnz
+    spmv_bytes = nnz * (8 + 4 / 9) + 16 * (flat.n_nodes + 1) + 16 * n
+    f64 = res["fp64"]
+    line = {
+        "metric": METRIC, "form": "precision", "value": n * f64["iterations"] / f64["s_per_solve"],
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": 0,
+        "ms_per_step": 1000 * f64["s_per_solve"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": PRECISION_NAME, "n_dof": n, "nnz": nnz},
+        "fp64": {"iterations": f64["iterations"], "s_per_solve": f64["s_per_solve"],
+                 "solves_per_s": 1 / f64["s_per_solve"], "residual": f64["residual"]},
+        "mixed": {"iterations": res["mixed"]["iterations"],
+                  "s_per_solve": res["mixed"]["s_per_solve"],
+                  "solves_per_s": 1 / res["mixed"]["s_per_solve"],
+                  "residual_fp64_true": res["mixed"]["residual"],
+                  "rel_err_vs_fp64": err,
+                  "speed_vs_fp64": f64["s_per_solve"] / res["mixed"]["s_per_solve"]},
+        "roofline": {"bound": "hbm", "kernel": "node-block FP64 SpMV (spmv_node_dot)",
+                     "achieved": spmv_bytes / (kms[0] / 1000) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": spmv_bytes / (kms[0] / 1000) / 1e9 / peak,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": int(spmv_bytes),
+                     "launch_ms": float(kms[0]), "traffic": None},
+    }
+    op.free()
+    ctx.close()
+    return line
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -364,12 +537,17 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        line = run_ours(args, rank, world, local_rank)
+        if args.form == "batched":
+            line = run_batched(args, rank, world, local_rank)
+        elif args.form == "precision":
+            line = run_precision(args, rank, world, local_rank) if rank == 0 else None
+        else:
+            line = run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch
             torch.distributed.destroy_process_group()
-    if rank == 0:
+    if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
 
 

@@ -278,6 +278,7 @@ typedef struct svx_batch_result {
     int32_t status;        /* SVX_OK or SVX_NOT_CONVERGED */
     int32_t pad;
     double cond_estimate;  /* max|diag| / min|diag| of this model's modified K */
+    int64_t nnz;           /* nonzeros of this model's K */
 } svx_batch_result_t;
 
 typedef struct svx_batch_stats {

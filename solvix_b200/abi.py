@@ -147,6 +147,7 @@ class SvxBatchResult(C.Structure):
         ("status", C.c_int32),
         ("pad", C.c_int32),
         ("cond_estimate", C.c_double),
+        ("nnz", C.c_int64),
     ]
 
 

@@ -131,7 +131,8 @@ class Context:
         out = [{"u": us[k], "von_mises": vms[k], "iterations": int(results[k].iterations),
                 "residual": float(results[k].residual),
                 "converged": results[k].status == abi.SVX_OK,
-                "cond_estimate": float(results[k].cond_estimate)} for k in range(count)]
+                "cond_estimate": float(results[k].cond_estimate),
+                "nnz": int(results[k].nnz)} for k in range(count)]
         st_d = {name: getattr(stats, name) for name, _ in abi.SvxBatchStats._fields_
                 if name != "pad"}
         return out, st_d

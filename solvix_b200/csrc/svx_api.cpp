@@ -755,6 +755,11 @@ int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* model
                                                  sizeof(double),
                                              cudaMemcpyDeviceToHost, st));
         SVX_CUDA(cudaStreamSynchronize(st));
+        std::vector<int64_t> nb(static_cast<size_t>(count) + 1);
+        for (int32_t k = 0; k <= count; ++k)
+            SVX_CUDA(cudaMemcpyAsync(&nb[k], op->pat.node_base.p + node_off[k], sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
         int64_t total_it = 0;
         int failed = 0;
         for (int32_t k = 0; k < count; ++k) {
@@ -763,6 +768,7 @@ int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* model
                 results[k].residual = res[k];
                 results[k].status = status[k] == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
                 results[k].cond_estimate = cond[k];
+                results[k].nnz = nb[k + 1] - nb[k];
             }
             total_it += it[k];
             failed += status[k] != PCG_CONVERGED;
