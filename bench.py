@@ -50,10 +50,17 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batched", "precision"], default="plain",
+    ap.add_argument("--form", choices=["plain", "batched", "precision", "served"],
+                    default="plain",
                     help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
                          "2D plates in one launch; precision: FP64 vs mixed on the "
-                         "480x48x48 heterogeneous C3D8 model")
+                         "480x48x48 heterogeneous C3D8 model; served: Poisson request "
+                         "stream through the continuous-batching server")
+    ap.add_argument("--requests", type=int, default=20000,
+                    help="served form: requests per rate point")
+    ap.add_argument("--rates", type=str, default="",
+                    help="served form: comma-separated arrival rates (requests/s); default "
+                         "fractions of the measured saturation throughput")
     return ap.parse_args()
 
 
@@ -520,6 +527,161 @@ def run_precision(args, rank, world, local_rank):
     return line
 
 
+SERVED_NAME = ("Poisson stream of solve requests: 70% 2D plates of the batched mix, 30% "
+               "C3D8 cantilevers nx~U{20..120}, ny=nz~U{4..16}, E=70e9, nu=0.33, tip load "
+               "U(1e3,1e4) N (seed 5); mixed precision to relative residual 1e-10; 40 GiB "
+               "admission budget; 4 lanes")
+
+
+def _serve_run(srv, reqs, rate_scale, base_t):
+    """Submit reqs at base_t * rate_scale seconds after the start (0 scale:
+    all at once), collect every result; returns (results, wall_s)."""
+    results = {}
+    done = threading.Event()
+    count = len(reqs)
+
+    def collect():
+        while len(results) < count:
+            r = srv.poll(200)
+            if r is not None:
+                r.pop("u", None)
+                r.pop("von_mises", None)
+                results[r["tag"]] = r
+        done.set()
+
+    th = threading.Thread(target=collect, daemon=True)
+    th.start()
+    t0 = time.perf_counter()
+    for k, flat in enumerate(reqs):
+        due = t0 + base_t[k] * rate_scale
+        while True:
+            now = time.perf_counter()
+            if now >= due:
+                break
+            time.sleep(min(due - now, 0.002))
+        st, msg = srv.submit(flat, k)
+        if st != 0:
+            raise RuntimeError(f"request {k} refused: {msg}")
+    th.join()
+    return results, time.perf_counter() - t0
+
+
+def run_served(args, rank, world, local_rank):
+    """C5: the request stream through svx_serve_* (continuous batching), at
+    saturation and at a sweep of Poisson rates; latency from submit to
+    result on the host."""
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, abi, workloads
+    from solvix_b200.serve import Server
+
+    torch.cuda.set_device(local_rank)
+    count = max(16, args.requests)
+    stream = workloads.request_stream(count, 1.0, seed=5)  # unit-rate arrival times
+    mine = list(range(rank, count, world))  # round-robin keeps each rank's arrivals Poisson
+    reqs = [stream[k][1] for k in mine]
+    base_t = np.array([stream[k][0] for k in mine]) * world  # rank's own unit-rate clock
+    n_dof = {k: f.n_dof for k, f in enumerate(reqs)}
+    srv = Server(local_rank, precision=abi.SVX_MIXED)
+    # warm-up: compile-free, but the first batches size the memory pool
+    warm = [reqs[k] for k in range(min(len(reqs), 256))]
+    _serve_run(srv, warm, 0.0, np.zeros(len(warm)))
+
+    def summarize(results, wall):
+        lat = np.array([r["t_done_ms"] - r["t_submit_ms"] for r in results.values()])
+        ok = [r for r in results.values() if r["status"] == 0]
+        dof_it = float(sum(n_dof[r["tag"]] * r["iterations"] for r in results.values()))
+        return {"solves_per_s": len(ok) / wall, "dof_iter_per_s": dof_it / wall,
+                "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+                "p99_ms": float(np.percentile(lat, 99)), "failed": len(results) - len(ok),
+                "mean_batch": float(np.mean([r["batch_size"] for r in results.values()])),
+                "wall_s": wall}
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = srv.lib.svx_launch_count()
+    sat_res, sat_wall = _serve_run(srv, reqs, 0.0, base_t)
+    sat = summarize(sat_res, sat_wall)
+    sat["rate_per_s"] = "all at t=0"
+    cap = sat["solves_per_s"] * world
+    rates = ([float(x) for x in args.rates.split(",") if x] if args.rates
+             else [round(cap * f, 1) for f in (0.25, 0.5, 0.8)])
+    sweep = []
+    for rate in rates:
+        per_rank_rate = rate / world
+        res, wall = _serve_run(srv, reqs, 1.0 / per_rank_rate, base_t / world)
+        row = summarize(res, wall)
+        row["rate_per_s"] = rate
+        sweep.append(row)
+    clk = clocks.stop()
+    launches = srv.lib.svx_launch_count() - launches0
+    stats = srv.stats()
+    srv.close()
+    # error against FP64 and the one-at-a-time plain FP64 GPU path on a sample
+    ctx = Context(local_rank)
+    rng = np.random.default_rng(1)
+    idx = [int(i) for i in rng.choice(len(reqs), min(48, len(reqs)), replace=False)]
+    with Server(local_rank, lanes=1, precision=abi.SVX_MIXED) as one:
+        for k in idx:
+            one.submit(reqs[k], k)
+        mixed_u = {}
+        while len(mixed_u) < len(idx):
+            r = one.poll(200)
+            if r is not None:
+                mixed_u[r["tag"]] = r["u"]
+    ctx.solve_flat(reqs[idx[0]])
+    t0 = time.perf_counter()
+    errs = []
+    for k in idx:
+        ref = ctx.solve_flat(reqs[k])
+        errs.append(float(np.linalg.norm(mixed_u[k] - ref.u) / np.linalg.norm(ref.u)))
+    one_per = (time.perf_counter() - t0) / len(idx)
+    ctx.close()
+    rows = [sat] + sweep
+    if world > 1:
+        gathered = [None] * world
+        torch.distributed.all_gather_object(gathered, rows)
+        rows = [{"solves_per_s": sum(g[i]["solves_per_s"] for g in gathered),
+                 "dof_iter_per_s": sum(g[i]["dof_iter_per_s"] for g in gathered),
+                 "p50_ms": max(g[i]["p50_ms"] for g in gathered),
+                 "p95_ms": max(g[i]["p95_ms"] for g in gathered),
+                 "p99_ms": max(g[i]["p99_ms"] for g in gathered),
+                 "failed": sum(g[i]["failed"] for g in gathered),
+                 "mean_batch": float(np.mean([g[i]["mean_batch"] for g in gathered])),
+                 "wall_s": max(g[i]["wall_s"] for g in gathered),
+                 "rate_per_s": rows[i]["rate_per_s"]} for i in range(len(rows))]
+    sat = rows[0]
+    head = rows[-1] if len(rows) > 1 else sat
+    line = {
+        "metric": METRIC, "form": "served", "value": sat["dof_iter_per_s"], "unit": UNIT,
+        "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1000 * sat["wall_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": SERVED_NAME, "requests_per_point": count,
+                   "parallelism": f"requests round-robin over {world} GPU(s), no collective"},
+        "solves_per_s": sat["solves_per_s"],
+        "latency_ms": {"p50": head["p50_ms"], "p95": head["p95_ms"], "p99": head["p99_ms"],
+                       "at_rate_per_s": head["rate_per_s"]},
+        "sweep": rows,
+        "rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                            "sample": len(errs)},
+        "one_at_a_time": {"solves_per_s": 1.0 / one_per,
+                          "sample": f"{len(idx)} requests through svx_solve_flat (FP64) one "
+                                    "after another, wall clock",
+                          "speedup_served": sat["solves_per_s"] * one_per},
+        "server": {k: stats[k] for k in ("batches", "peak_bytes_admitted",
+                                         "peak_device_bytes")},
+        "e2e": {"value": sat["dof_iter_per_s"], "unit": UNIT,
+                "note": "submit of host models to results on the host, wall clock",
+                "h2d_bytes_per_step": int(sum(f.nbytes() for f in reqs)),
+                "d2h_bytes_per_step": int(sum(8 * (f.n_dof + f.n_elem) for f in reqs))},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    return line
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -539,6 +701,8 @@ def main():
     try:
         if args.form == "batched":
             line = run_batched(args, rank, world, local_rank)
+        elif args.form == "served":
+            line = run_served(args, rank, world, local_rank)
         elif args.form == "precision":
             line = run_precision(args, rank, world, local_rank) if rank == 0 else None
         else:

@@ -275,10 +275,13 @@ int svx_op_stress(svx_op_t* op, svx_solution_t* sol);
 typedef struct svx_batch_result {
     int64_t iterations;    /* PCG iterations of this model */
     double residual;       /* recursive ||r||/||f|| at exit */
-    int32_t status;        /* SVX_OK or SVX_NOT_CONVERGED */
-    int32_t pad;
+    int32_t status;        /* SVX_OK, SVX_NOT_CONVERGED, or why the model was
+                              rejected (SVX_EMPTY_MESH, SVX_NO_CONSTRAINTS,
+                              SVX_INVALID_MODEL, SVX_BAD_ARGUMENT) */
+    int32_t reason;        /* enum svx_elem_reason for SVX_INVALID_MODEL */
     double cond_estimate;  /* max|diag| / min|diag| of this model's modified K */
     int64_t nnz;           /* nonzeros of this model's K */
+    int64_t elem_index;    /* failing element (index within the model) or -1 */
 } svx_batch_result_t;
 
 typedef struct svx_batch_stats {
@@ -289,22 +292,114 @@ typedef struct svx_batch_stats {
     int32_t lanes_per_node;   /* autotuned lanes per node of its SpMV */
     int64_t total_iterations; /* sum over models */
     int64_t total_dof;        /* sum over models */
-    int32_t not_converged;    /* models that missed tol within their budget */
-    int32_t pad;
+    int32_t not_converged;    /* models that missed tol within their budget
+                                 or were rejected */
+    int32_t cluster_members;  /* models solved by a CTA cluster (3D >= 4096
+                                 rows, 2D >= 16384 rows) */
+    int64_t fp32_iterations;  /* mixed form: iterations on the FP32 operator */
 } svx_batch_stats_t;
 
-/* Solves `count` independent models of equal ndof (FP64 form).  They are
+/* Solves `count` independent models of equal ndof.  They are
  * assembled as one block-diagonal operator; one persistent launch then runs
  * every model's Jacobi-PCG with its own scalars, convergence test and
  * iteration budget (max(1000, 10 n_model) unless opts->max_iter > 0), one
  * CTA per model at a time, largest models first.  The CTA size and lanes
  * per node are autotuned once per context and ndof, and kept.  Per model
  * outputs: u[k] (n_nodes*ndof) and von_mises[k] (n_elem), host arrays, any
- * may be NULL.  A model that fails assembly rejects the batch (InvalidModel,
- * message prefixed with "model k: "). */
+ * may be NULL.  Each model is checked on its own: one that is rejected
+ * (empty mesh, no constraints, a bad element found on the host or by the
+ * element kernel) gets that status in its result and the others are solved
+ * as if it were absent.  Models of different ndof in one call are
+ * SVX_BAD_ARGUMENT for the call.  opts->precision selects the FP64 or the
+ * mixed form (FP32-stored K with FP64 residual replacement) per model. */
 int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* models,
                     const svx_solve_opts_t* opts, double* const* u, double* const* von_mises,
                     svx_batch_result_t* results, svx_batch_stats_t* stats, svx_error_t* err);
+
+/* ---- served solves (continuous batching) ---------------------------- */
+/* A request loop for `solvix serve --json`: decks are submitted as they
+ * arrive and solved in batches on the device while later ones keep
+ * arriving.  `lanes` dispatcher threads each own a CUDA stream; whenever a
+ * lane is free it takes every waiting request (arrival order, equal ndof,
+ * at most max_batch) whose device memory fits what is left of the budget,
+ * solves them as one batch (svx_batch_solve's per-model isolation and
+ * per-model convergence) and publishes each result as its batch completes.
+ * Batches of different lanes run concurrently on the device.  A request is
+ * admitted only while the estimated device bytes of all admitted, unfinished
+ * requests stay within hbm_budget_bytes.  The lanes share one device memory
+ * pool whose arena, the whole budget, is reserved at creation, so batches
+ * of any size make no cudaMalloc / cudaFree calls in steady state. */
+typedef struct svx_server svx_server_t;
+
+typedef struct svx_serve_opts {
+    int64_t hbm_budget_bytes;  /* admission budget; 0 = 40 GiB */
+    int32_t lanes;             /* concurrent batches (streams); 0 = 4 */
+    int32_t max_batch;         /* requests per batch at most; 0 = 4096 */
+    svx_solve_opts_t solve;    /* tolerance, precision, max_iter, want_stress */
+} svx_serve_opts_t;
+
+typedef struct svx_serve_result {
+    uint64_t tag;              /* the caller's tag from svx_serve_submit */
+    int32_t status;            /* as svx_batch_result_t.status */
+    int32_t ndof;
+    int64_t n_nodes;
+    int64_t n_elem;
+    int64_t iterations;
+    double residual;
+    double cond_estimate;
+    double t_submit_ms;        /* server clock (ms since svx_serve_create) */
+    double t_start_ms;         /* its batch was taken by a lane */
+    double t_done_ms;          /* its batch's results were on the host */
+    int32_t batch_size;        /* requests in its batch */
+    int32_t lane;
+    const double* u;           /* [n_nodes * ndof], owned by the result */
+    const double* von_mises;   /* [n_elem] centroid von Mises (NULL if off) */
+    svx_error_t error;         /* why a request failed (status != SVX_OK) */
+} svx_serve_result_t;
+
+typedef struct svx_serve_stats {
+    int64_t submitted;
+    int64_t rejected;          /* refused by svx_serve_submit */
+    int64_t completed;         /* results published (any status) */
+    int64_t batches;
+    int64_t pending;           /* waiting for admission */
+    int64_t in_flight;         /* admitted, not yet published */
+    int64_t bytes_admitted;    /* estimated device bytes of in-flight work */
+    int64_t peak_bytes_admitted;
+    int64_t device_bytes;      /* device memory the lanes' pool holds: its
+                                  arena (the budget, reserved at creation) or,
+                                  if more, the blocks in use + cached */
+    int64_t peak_device_bytes;
+    /* summed over batches, ms of host wall clock per phase: member checks
+     * and concatenation, upload + assembly, batched PCG, result copies;
+     * and the device time of the batched PCG launches */
+    double prep_ms, assemble_ms, solve_ms, output_ms, device_solve_ms;
+    double pool_ms;            /* wall clock inside cudaMalloc / cudaFree */
+    int64_t pool_mallocs;      /* cudaMalloc calls of the shared pool */
+} svx_serve_stats_t;
+
+void svx_serve_default_opts(svx_serve_opts_t* opts);
+int svx_serve_create(int device, const svx_serve_opts_t* opts, svx_server_t** out,
+                     svx_error_t* err);
+/* Queues a copy of `model`.  Refused at once (not queued, no result) with
+ * SVX_OOM when its estimated device bytes exceed the whole budget, and with
+ * the reference's error for a deck the host can reject (bad sizes, empty
+ * mesh, no constraints, a bad material); elements with a non-positive
+ * Jacobian are found on the device and come back as a failed result. */
+int svx_serve_submit(svx_server_t* srv, const svx_flat_model_t* model, uint64_t tag,
+                     svx_error_t* err);
+/* Estimated device bytes the server charges against the budget for a model. */
+int64_t svx_serve_estimate_bytes(const svx_flat_model_t* model);
+/* Next completed result (completion order), waiting up to wait_ms
+ * (< 0: until one exists).  SVX_QUEUE_EMPTY when none arrived in time. */
+int svx_serve_poll(svx_server_t* srv, int32_t wait_ms, svx_serve_result_t** out);
+void svx_serve_result_free(svx_serve_result_t* res);
+int svx_serve_stats(svx_server_t* srv, svx_serve_stats_t* stats);
+/* Milliseconds on the server clock. */
+double svx_serve_now_ms(const svx_server_t* srv);
+/* Finishes every submitted request, then stops the lanes and frees the
+ * server (results not yet polled are freed too). */
+int svx_serve_destroy(svx_server_t* srv);
 
 /* ---- measurement --------------------------------------------------- */
 /* Kernels this process has launched through the library (graph nodes count

@@ -145,9 +145,10 @@ class SvxBatchResult(C.Structure):
         ("iterations", C.c_int64),
         ("residual", C.c_double),
         ("status", C.c_int32),
-        ("pad", C.c_int32),
+        ("reason", C.c_int32),
         ("cond_estimate", C.c_double),
         ("nnz", C.c_int64),
+        ("elem_index", C.c_int64),
     ]
 
 
@@ -161,8 +162,48 @@ class SvxBatchStats(C.Structure):
         ("total_iterations", C.c_int64),
         ("total_dof", C.c_int64),
         ("not_converged", C.c_int32),
-        ("pad", C.c_int32),
+        ("cluster_members", C.c_int32),
+        ("fp32_iterations", C.c_int64),
     ]
+
+
+class SvxServeOpts(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_int64),
+        ("lanes", C.c_int32),
+        ("max_batch", C.c_int32),
+        ("solve", SvxSolveOpts),
+    ]
+
+
+class SvxServeResult(C.Structure):
+    _fields_ = [
+        ("tag", C.c_uint64),
+        ("status", C.c_int32),
+        ("ndof", C.c_int32),
+        ("n_nodes", C.c_int64),
+        ("n_elem", C.c_int64),
+        ("iterations", C.c_int64),
+        ("residual", C.c_double),
+        ("cond_estimate", C.c_double),
+        ("t_submit_ms", C.c_double),
+        ("t_start_ms", C.c_double),
+        ("t_done_ms", C.c_double),
+        ("batch_size", C.c_int32),
+        ("lane", C.c_int32),
+        ("u", C.POINTER(C.c_double)),
+        ("von_mises", C.POINTER(C.c_double)),
+        ("error", SvxError),
+    ]
+
+
+class SvxServeStats(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in (
+        "submitted", "rejected", "completed", "batches", "pending", "in_flight",
+        "bytes_admitted", "peak_bytes_admitted", "device_bytes", "peak_device_bytes")] + \
+        [(name, C.c_double) for name in (
+            "prep_ms", "assemble_ms", "solve_ms", "output_ms", "device_solve_ms", "pool_ms")] + \
+        [("pool_mallocs", C.c_int64)]
 
 
 def ptr(a: np.ndarray | None, ctype):
@@ -205,6 +246,17 @@ SIGNATURES = {
                                   C.POINTER(SvxSolveOpts), C.POINTER(c_double_p),
                                   C.POINTER(c_double_p), C.POINTER(SvxBatchResult),
                                   C.POINTER(SvxBatchStats), C.POINTER(SvxError)]),
+    "svx_serve_default_opts": (None, [C.POINTER(SvxServeOpts)]),
+    "svx_serve_create": (C.c_int, [C.c_int, C.POINTER(SvxServeOpts), C.POINTER(_VP),
+                                   C.POINTER(SvxError)]),
+    "svx_serve_submit": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.c_uint64,
+                                   C.POINTER(SvxError)]),
+    "svx_serve_estimate_bytes": (C.c_int64, [C.POINTER(SvxFlatModel)]),
+    "svx_serve_poll": (C.c_int, [_VP, C.c_int32, C.POINTER(C.POINTER(SvxServeResult))]),
+    "svx_serve_result_free": (None, [C.POINTER(SvxServeResult)]),
+    "svx_serve_stats": (C.c_int, [_VP, C.POINTER(SvxServeStats)]),
+    "svx_serve_now_ms": (C.c_double, [_VP]),
+    "svx_serve_destroy": (C.c_int, [_VP]),
     "svx_solve_flat": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.POINTER(SvxSolveOpts),
                                  C.POINTER(SvxSolution), C.POINTER(SvxError)]),
     "svx_solve_resolved": (C.c_int, [_VP, _VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),

@@ -105,11 +105,13 @@ class Context:
         return out.solution(flat, precision)
 
     def solve_batch(self, flats, tol: float = 1e-10, max_iter: int = 0, want_u: bool = True,
-                    want_stress: bool = True):
+                    want_stress: bool = True, precision: int = abi.SVX_FP64):
         """Solve many independent FlatModels (equal ndof) in one batched launch.
 
         Returns (list of per-model dicts with u / von_mises / iterations /
-        residual / converged / cond_estimate, stats dict).
+        residual / converged / status / cond_estimate / nnz, stats dict).
+        A model rejected on its own (bad element, no constraints, ...) has
+        ``status`` set to that error code and does not affect the others.
         """
         flats = list(flats)
         count = len(flats)
@@ -120,7 +122,8 @@ class Context:
         vm_ptrs = (abi.c_double_p * count)(*[abi.ptr(a, C.c_double) for a in vms])
         results = (abi.SvxBatchResult * count)()
         stats = abi.SvxBatchStats()
-        opts = abi.default_opts(tol=tol, max_iter=max_iter, want_stress=int(want_stress))
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, want_stress=int(want_stress),
+                                precision=precision)
         err = abi.SvxError()
         st = self.lib.svx_batch_solve(self.handle, count, structs, C.byref(opts),
                                       u_ptrs if want_u else None,
@@ -131,10 +134,11 @@ class Context:
         out = [{"u": us[k], "von_mises": vms[k], "iterations": int(results[k].iterations),
                 "residual": float(results[k].residual),
                 "converged": results[k].status == abi.SVX_OK,
+                "status": int(results[k].status), "reason": int(results[k].reason),
+                "elem_index": int(results[k].elem_index),
                 "cond_estimate": float(results[k].cond_estimate),
                 "nnz": int(results[k].nnz)} for k in range(count)]
-        st_d = {name: getattr(stats, name) for name, _ in abi.SvxBatchStats._fields_
-                if name != "pad"}
+        st_d = {name: getattr(stats, name) for name, _ in abi.SvxBatchStats._fields_}
         return out, st_d
 
     def solve_model(self, model: Model, tol: float = 1e-10, precision: int = abi.SVX_FP64,

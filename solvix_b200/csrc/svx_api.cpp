@@ -3,6 +3,7 @@
 // solve_with_thermal (crates/solvix-core/src/lib.rs:614-703).
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -18,39 +19,117 @@ DevicePool::~DevicePool() {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device_);
-    for (auto& kv : sizes_) cudaFree(kv.first);
+    for (auto& kv : sizes_)
+        if (!in_arena(kv.first)) cudaFree(kv.first);
+    if (arena_) cudaFree(arena_);
     cudaSetDevice(prev);
 }
 
 static size_t round_bytes(size_t b) {
-    // 2 MiB granules for large blocks, 512 B below: repeated solves of the
-    // same shape hit the cache exactly.
-    if (b >= (size_t(1) << 21)) return (b + (size_t(1) << 21) - 1) & ~((size_t(1) << 21) - 1);
-    return (b + 511) & ~size_t(511);
+    // 512 B granules below 2 MiB; above, four size classes per octave
+    // (at most 25% slack), so that batches of varying size reuse the cached
+    // blocks instead of calling cudaMalloc for every new size.
+    if (b < (size_t(1) << 21)) return (b + 511) & ~size_t(511);
+    int top = 63 - __builtin_clzll(static_cast<unsigned long long>(b));
+    const size_t step = size_t(1) << (top - 2);
+    return (b + step - 1) & ~(step - 1);
+}
+
+void DevicePool::reserve(size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (arena_ || bytes == 0) return;
+    bytes = (bytes + (size_t(1) << 21) - 1) & ~((size_t(1) << 21) - 1);
+    const auto t0 = std::chrono::steady_clock::now();
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    malloc_ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                      .count();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw ModelFail{SVX_OOM, 0, -1,
+                        "could not reserve a device arena of " + std::to_string(bytes) + " bytes"};
+    }
+    ++mallocs_;
+    arena_ = static_cast<char*>(p);
+    arena_size_ = bytes;
+    ranges_[0] = bytes;
+}
+
+void* DevicePool::carve(size_t bytes) {
+    for (auto it = ranges_.begin(); it != ranges_.end(); ++it) {
+        if (it->second < bytes) continue;
+        const size_t off = it->first, len = it->second;
+        ranges_.erase(it);
+        if (len > bytes) ranges_[off + bytes] = len - bytes;
+        return arena_ + off;
+    }
+    return nullptr;
+}
+
+void DevicePool::give_back(void* p, size_t bytes) {
+    size_t off = size_t(static_cast<char*>(p) - arena_), len = bytes;
+    auto next = ranges_.lower_bound(off);
+    if (next != ranges_.end() && off + len == next->first) {
+        len += next->second;
+        next = ranges_.erase(next);
+    }
+    if (next != ranges_.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            prev->second += len;
+            return;
+        }
+    }
+    ranges_[off] = len;
+}
+
+void DevicePool::flush_arena_cache() {
+    for (auto it = free_.begin(); it != free_.end();) {
+        if (in_arena(it->second)) {
+            cached_ -= it->first;
+            sizes_.erase(it->second);
+            give_back(it->second, it->first);
+            it = free_.erase(it);
+        } else {
+            ++it;
+        }
+    }
 }
 
 void* DevicePool::alloc(size_t bytes) {
-    size_t want = round_bytes(bytes);
-    std::lock_guard<std::mutex> lk(mu_);
-    auto it = free_.lower_bound(want);
-    if (it != free_.end() && it->first <= want + want / 8) {
-        void* p = it->second;
-        free_.erase(it);
-        cached_ -= sizes_[p];
-        in_use_ += sizes_[p];
-        return p;
+    const size_t want = round_bytes(bytes);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.lower_bound(want);
+        if (it != free_.end() && it->first <= want + want / 4) {
+            void* p = it->second;
+            free_.erase(it);
+            cached_ -= sizes_[p];
+            in_use_ += sizes_[p];
+            return p;
+        }
+        if (arena_) {
+            void* p = carve(want);
+            if (!p) {  // cached arena blocks of other sizes go back, coalesced
+                flush_arena_cache();
+                p = carve(want);
+            }
+            if (p) {
+                sizes_[p] = want;
+                in_use_ += want;
+                return p;
+            }
+        }
     }
+    // the driver call runs outside the lock: other streams' allocations
+    // that hit the cache do not wait for it
+    const auto t0 = std::chrono::steady_clock::now();
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         // drop the cache and retry once
         cudaGetLastError();
-        for (auto& kv : free_) {
-            cudaFree(kv.second);
-            sizes_.erase(kv.second);
-        }
-        free_.clear();
-        cached_ = 0;
+        trim();
         e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -58,6 +137,10 @@ void* DevicePool::alloc(size_t bytes) {
                             "device allocation of " + std::to_string(want) + " bytes failed"};
         }
     }
+    std::lock_guard<std::mutex> lk(mu_);
+    malloc_ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                      .count();
+    ++mallocs_;
     sizes_[p] = want;
     in_use_ += want;
     return p;
@@ -73,13 +156,17 @@ void DevicePool::release(void* p) {
 }
 
 void DevicePool::trim() {
+    const auto t0 = std::chrono::steady_clock::now();
     std::lock_guard<std::mutex> lk(mu_);
+    flush_arena_cache();
     for (auto& kv : free_) {
         cudaFree(kv.second);
         sizes_.erase(kv.second);
     }
     free_.clear();
     cached_ = 0;
+    malloc_ms_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                      .count();
 }
 
 }  // namespace svx
@@ -263,32 +350,35 @@ void device_assemble(svx_ctx* ctx, svx_op* op) {
 
 // K1-K4 for a validated flat model; throws ModelFail for element errors.
 svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags,
-                      const double* thick_elem = nullptr) {
+                      const double* thick_elem = nullptr, bool prechecked = false) {
     SVX_CUDA(cudaSetDevice(ctx->device));
-    check_flat(m);
+    if (!prechecked) check_flat(m);
     // ndof_per_node (lib.rs:725-752) runs before assembly
-    bool solid = false, plane = false, beam = false;
-    for (int64_t e = 0; e < m->n_elem; ++e) {
-        int k = m->kind[e];
-        if (k == SVX_C3D8 || k == SVX_C3D4) solid = true;
-        else if (k == SVX_B31) beam = true;
-        else plane = true;
-    }
-    if (beam && (plane || solid))
-        throw ModelFail{SVX_INVALID_MODEL, 0, -1,
-                        "mixed beam and continuum elements (v1: B31-only models)"};
-    if (solid && plane) throw ModelFail{SVX_INVALID_MODEL, 0, -1, "mixed dimensionality"};
-    if (m->ndof != ((solid || beam) ? 3 : 2))
-        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "ndof does not match the element kinds"};
-    // first element failing a material / kind check (host, O(n_elem))
+    // first element failing a material / kind check (host, O(n_elem));
+    // members of a batch were checked one by one already
     int64_t m_fail = -1;
     int m_reason = 0;
-    for (int64_t e = 0; e < m->n_elem; ++e) {
-        int r = material_reason(m, e);
-        if (r) {
-            m_fail = e;
-            m_reason = r;
-            break;
+    if (!prechecked) {
+        bool solid = false, plane = false, beam = false;
+        for (int64_t e = 0; e < m->n_elem; ++e) {
+            int k = m->kind[e];
+            if (k == SVX_C3D8 || k == SVX_C3D4) solid = true;
+            else if (k == SVX_B31) beam = true;
+            else plane = true;
+        }
+        if (beam && (plane || solid))
+            throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                            "mixed beam and continuum elements (v1: B31-only models)"};
+        if (solid && plane) throw ModelFail{SVX_INVALID_MODEL, 0, -1, "mixed dimensionality"};
+        if (m->ndof != ((solid || beam) ? 3 : 2))
+            throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "ndof does not match the element kinds"};
+        for (int64_t e = 0; e < m->n_elem; ++e) {
+            int r = material_reason(m, e);
+            if (r) {
+                m_fail = e;
+                m_reason = r;
+                break;
+            }
         }
     }
 
@@ -330,9 +420,12 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags,
         throw ModelFail{SVX_INVALID_MODEL, m_reason, m_fail, element_message(m, m_fail, m_reason)};
     }
     // loads and constraints
-    std::vector<double> f(size_t(op->n), 0.0);
-    if (m->f) std::memcpy(f.data(), m->f, sizeof(double) * op->n);
-    upload(ctx, op->f_orig, f.data(), size_t(op->n));
+    if (m->f) {
+        upload(ctx, op->f_orig, m->f, size_t(op->n));
+    } else {
+        op->f_orig.alloc(ctx->pool, size_t(op->n) + 1);
+        SVX_CUDA(cudaMemsetAsync(op->f_orig.p, 0, sizeof(double) * size_t(op->n), st));
+    }
     op->n_fixed = m->n_fixed;
     op->h_fixed_row.assign(m->fixed_row, m->fixed_row + m->n_fixed);
     upload(ctx, op->fixed_row, op->h_fixed_row.data(), size_t(m->n_fixed));
@@ -426,6 +519,239 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
 
 }  // namespace
 
+namespace svx {
+
+// Host checks of one batch member, in the reference's order: empty mesh,
+// no constraints (lib.rs:600-606), flat-model consistency, the element
+// kinds against ndof (lib.rs:725-752), then the first element failing a
+// material check (assembly.rs:143-160).
+void check_batch_member(const svx_flat_model_t* m) {
+    check_flat(m);
+    if (m->n_elem == 0) throw ModelFail{SVX_EMPTY_MESH, 0, -1, "empty mesh"};
+    if (m->n_fixed == 0) throw ModelFail{SVX_NO_CONSTRAINTS, 0, -1, "no constraints"};
+    bool solid = false, plane = false, beam = false;
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        const int k = m->kind[e];
+        if (k == SVX_C3D8 || k == SVX_C3D4) solid = true;
+        else if (k == SVX_B31) beam = true;
+        else plane = true;
+    }
+    if (beam && (plane || solid))
+        throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                        "mixed beam and continuum elements (v1: B31-only models)"};
+    if (solid && plane) throw ModelFail{SVX_INVALID_MODEL, 0, -1, "mixed dimensionality"};
+    if (m->ndof != ((solid || beam) ? 3 : 2))
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "ndof does not match the element kinds"};
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        const int r = material_reason(m, e);
+        if (r) throw ModelFail{SVX_INVALID_MODEL, r, e, element_message(m, e, r)};
+    }
+}
+
+
+// One block-diagonal batch.  Every member is checked on its own; a member
+// that fails (host checks, or a non-positive Jacobian found by the element
+// kernel) gets its own status and message and the batch is re-assembled
+// without it, so no member's failure reaches another member.  The members
+// that pass are concatenated (node, element and row offsets), assembled as
+// one operator and solved by one batched PCG launch.
+void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* models,
+               const svx_solve_opts_t& o, double* const* u, double* const* vm,
+               std::vector<BatchModelOut>& out, BatchRun& run) {
+    SVX_CUDA(cudaSetDevice(ctx->device));
+    if (o.precision != SVX_FP64 && o.precision != SVX_MIXED)
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "unknown precision"};
+    out.assign(static_cast<size_t>(count), BatchModelOut{});
+    run = BatchRun{};
+    using clock = std::chrono::steady_clock;
+    auto since = [](clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(clock::now() - t).count();
+    };
+    clock::time_point t_phase = clock::now();
+    int ndof = 0;
+    std::vector<int32_t> live;
+    for (int32_t k = 0; k < count; ++k) {
+        if (!models[k]) throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "null model"};
+        try {
+            check_batch_member(models[k]);
+        } catch (const ModelFail& f) {
+            out[k].status = f.code;
+            out[k].reason = f.reason;
+            out[k].elem_index = f.elem_index;
+            out[k].message = f.message;
+            continue;
+        }
+        if (ndof == 0) ndof = models[k]->ndof;
+        if (models[k]->ndof != ndof)
+            throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "models of one batch share ndof"};
+        live.push_back(k);
+    }
+    while (!live.empty()) {
+        const int32_t L = int32_t(live.size());
+        int64_t nn = 0, ne = 0, nc = 0, nf = 0;
+        for (int32_t k : live) {
+            const svx_flat_model_t& m = *models[k];
+            nn += m.n_nodes;
+            ne += m.n_elem;
+            nc += m.conn_ptr[m.n_elem];
+            nf += m.n_fixed;
+        }
+        // the concatenated model is written straight into the context's
+        // page-locked staging buffer, so assembly uploads it by DMA
+        const size_t une = static_cast<size_t>(ne), unn = static_cast<size_t>(nn);
+        size_t off = 0;
+        auto carve = [&](size_t bytes) {
+            const size_t at = off;
+            off += (bytes + 15) & ~size_t(15);
+            return at;
+        };
+        const size_t o_xyz = carve(24 * unn), o_f = carve(8 * unn * ndof), o_E = carve(8 * une),
+                     o_nu = carve(8 * une), o_th = carve(8 * une), o_cp = carve(8 * (une + 1)),
+                     o_fix = carve(8 * static_cast<size_t>(nf)), o_eid = carve(4 * une),
+                     o_conn = carve(4 * static_cast<size_t>(nc)), o_kind = carve(une);
+        char* base = static_cast<char*>(ctx->staging.get(std::max<size_t>(off, 16)));
+        double* xyz = reinterpret_cast<double*>(base + o_xyz);
+        double* f = reinterpret_cast<double*>(base + o_f);
+        double* E = reinterpret_cast<double*>(base + o_E);
+        double* nu = reinterpret_cast<double*>(base + o_nu);
+        double* th = reinterpret_cast<double*>(base + o_th);
+        int64_t* conn_ptr = reinterpret_cast<int64_t*>(base + o_cp);
+        int64_t* fixed = reinterpret_cast<int64_t*>(base + o_fix);
+        uint32_t* eid = reinterpret_cast<uint32_t*>(base + o_eid);
+        int32_t* conn = reinterpret_cast<int32_t*>(base + o_conn);
+        uint8_t* kind = reinterpret_cast<uint8_t*>(base + o_kind);
+        std::vector<int64_t> node_off(static_cast<size_t>(L) + 1, 0);
+        std::vector<int64_t> elem_off(static_cast<size_t>(L) + 1, 0);
+        conn_ptr[0] = 0;
+        int64_t n_fixed = 0;
+        for (int32_t j = 0; j < L; ++j) {
+            const svx_flat_model_t& m = *models[live[j]];
+            const int64_t n0 = node_off[j], e0 = elem_off[j];
+            std::memcpy(xyz + 3 * n0, m.xyz, sizeof(double) * 3 * m.n_nodes);
+            if (m.f)
+                std::memcpy(f + n0 * ndof, m.f, sizeof(double) * m.n_nodes * ndof);
+            else
+                std::memset(f + n0 * ndof, 0, sizeof(double) * m.n_nodes * ndof);
+            std::memcpy(kind + e0, m.kind, size_t(m.n_elem));
+            std::memcpy(E + e0, m.youngs, sizeof(double) * m.n_elem);
+            std::memcpy(nu + e0, m.poisson, sizeof(double) * m.n_elem);
+            const int64_t c0 = conn_ptr[e0];
+            for (int64_t e = 0; e < m.n_elem; ++e) {
+                th[e0 + e] = m.thickness;
+                eid[e0 + e] = elem_id_of(&m, e);
+                conn_ptr[e0 + e + 1] = c0 + m.conn_ptr[e + 1];
+            }
+            const int32_t shift = int32_t(n0);
+            for (int64_t q = 0; q < m.conn_ptr[m.n_elem]; ++q) conn[c0 + q] = m.conn[q] + shift;
+            for (int64_t q = 0; q < m.n_fixed; ++q) fixed[n_fixed++] = m.fixed_row[q] + n0 * ndof;
+            node_off[j + 1] = n0 + m.n_nodes;
+            elem_off[j + 1] = e0 + m.n_elem;
+        }
+        svx_flat_model_t all{};
+        all.n_nodes = nn;
+        all.xyz = xyz;
+        all.n_elem = ne;
+        all.kind = kind;
+        all.conn_ptr = conn_ptr;
+        all.conn = conn;
+        all.youngs = E;
+        all.poisson = nu;
+        all.elem_id = eid;
+        all.thickness = 1.0;
+        all.ndof = ndof;
+        all.n_fixed = n_fixed;
+        all.fixed_row = fixed;
+        all.f = f;
+        run.wall_prep += since(t_phase);
+        t_phase = clock::now();
+        std::unique_ptr<svx_op> op;
+        try {
+            op.reset(assemble_impl(ctx, &all, 0, th, true));
+        } catch (const ModelFail& fail) {
+            if (fail.code != SVX_INVALID_MODEL || fail.elem_index < 0 || fail.elem_index >= ne)
+                throw;
+            // the element kernel found a bad element: drop its model, retry
+            const int32_t j = int32_t(std::upper_bound(elem_off.begin(), elem_off.end(),
+                                                       fail.elem_index) -
+                                      elem_off.begin()) - 1;
+            BatchModelOut& bad = out[live[j]];
+            bad.status = SVX_INVALID_MODEL;
+            bad.reason = fail.reason;
+            bad.elem_index = fail.elem_index - elem_off[j];
+            bad.message = fail.message;
+            live.erase(live.begin() + j);
+            run.wall_assemble += since(t_phase);
+            t_phase = clock::now();
+            continue;
+        }
+        run.wall_assemble += since(t_phase);
+        t_phase = clock::now();
+        std::vector<double> tol(static_cast<size_t>(L), o.tol);
+        std::vector<int64_t> mi(static_cast<size_t>(L));
+        for (int32_t j = 0; j < L; ++j)
+            mi[j] = o.max_iter > 0 ? o.max_iter
+                                   : default_max_iter((node_off[j + 1] - node_off[j]) * ndof);
+        std::vector<int64_t> it;
+        std::vector<double> res, cond;
+        std::vector<int32_t> status;
+        BatchStats bs;
+        batch_pcg(ctx, op.get(), L, node_off, tol, mi, it, res, status, cond, &bs,
+                  o.precision == SVX_MIXED);
+        run.wall_solve += since(t_phase);
+        t_phase = clock::now();
+        cudaStream_t st = ctx->stream;
+        const bool want_vm = vm && o.want_stress;
+        if (want_vm) {
+            SVX_CUDA(cudaEventRecord(ctx->ev[4], st));
+            if (!op->vm_elem.p) op->vm_elem.alloc(ctx->pool, op->n_elem + 1);
+            recover_stress(ctx, op.get(), op->u.p, op->vm_elem.p, nullptr, nullptr, nullptr);
+            SVX_CUDA(cudaEventRecord(ctx->ev[5], st));
+        }
+        // u and the von Mises field come back in two DMA copies through the
+        // staging buffer (the uploads of this batch are complete), then are
+        // split per member on the host
+        const size_t nu_rows = static_cast<size_t>(nn * ndof);
+        double* host = static_cast<double*>(
+            ctx->staging.get(sizeof(double) * (nu_rows + (want_vm ? une : 0) + 1)));
+        if (u) SVX_CUDA(cudaMemcpyAsync(host, op->u.p, sizeof(double) * nu_rows,
+                                        cudaMemcpyDeviceToHost, st));
+        if (want_vm)
+            SVX_CUDA(cudaMemcpyAsync(host + nu_rows, op->vm_elem.p, sizeof(double) * une,
+                                     cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        if (want_vm) run.ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
+        for (int32_t j = 0; j < L; ++j) {
+            const int32_t k = live[j];
+            if (u && u[k])
+                std::memcpy(u[k], host + node_off[j] * ndof,
+                            sizeof(double) * (node_off[j + 1] - node_off[j]) * ndof);
+            if (want_vm && vm[k])
+                std::memcpy(vm[k], host + nu_rows + elem_off[j],
+                            sizeof(double) * (elem_off[j + 1] - elem_off[j]));
+        }
+        for (int32_t j = 0; j < L; ++j) {
+            BatchModelOut& m = out[live[j]];
+            m.iterations = it[j];
+            m.residual = res[j];
+            m.status = status[j] == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
+            if (m.status != SVX_OK)
+                m.message = "not converged after " + std::to_string(it[j]) + " iterations";
+            m.cond = cond[j];
+            m.nnz = bs.member_nnz[j];
+        }
+        run.wall_output += since(t_phase);
+        run.ms_assemble = op->ms_assemble;
+        run.ms_solve = bs.ms_solve;
+        run.threads_per_cta = bs.threads_per_cta;
+        run.lanes_per_node = bs.lanes_per_node;
+        run.cluster_members = bs.cluster_members;
+        run.fp32_iterations = bs.fp32_iterations;
+        break;
+    }
+}
+
+}  // namespace svx
+
 extern "C" {
 
 const char* svx_version(void) { return "solvix_b200 0.1.0 (sm_100a)"; }
@@ -459,8 +785,18 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         std::unique_ptr<svx_ctx> ctx(new svx_ctx());
         ctx->device = device;
         ctx->sm_count = prop.multiProcessorCount;
-        SVX_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        // the main stream (uploads, assembly, stress, plain solves) has the
+        // highest priority; the long batched PCG kernels run on the lowest,
+        // so a served lane's assembly gets SMs while another lane's batch
+        // is being solved
+        int least = 0, greatest = 0;
+        SVX_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SVX_CUDA(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, greatest));
+        SVX_CUDA(cudaStreamCreateWithPriority(&ctx->pcg_stream, cudaStreamNonBlocking, least));
+        SVX_CUDA(cudaStreamCreateWithPriority(&ctx->aux_stream, cudaStreamNonBlocking, least));
         for (auto& e : ctx->ev) SVX_CUDA(cudaEventCreate(&e));
+        SVX_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+        SVX_CUDA(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
         ctx->pool = new DevicePool(device);
         *out = ctx.release();
         return SVX_OK;
@@ -471,9 +807,16 @@ int svx_ctx_destroy(svx_ctx_t* ctx) {
     if (!ctx) return SVX_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    delete ctx->pool;
+    if (ctx->owns_pool) delete ctx->pool;
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    for (cudaStream_t x : {ctx->pcg_stream, ctx->aux_stream})
+        if (x) {
+            cudaStreamSynchronize(x);
+            cudaStreamDestroy(x);
+        }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SVX_OK;
@@ -649,139 +992,43 @@ int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* model
                     svx_batch_result_t* results, svx_batch_stats_t* stats, svx_error_t* err) {
     if (!ctx || count <= 0 || !models) return SVX_BAD_ARGUMENT;
     return guarded(ctx, err, [&]() -> int {
-        SVX_CUDA(cudaSetDevice(ctx->device));
         svx_solve_opts_t o;
         svx_default_opts(&o);
         if (opts) o = *opts;
-        if (o.precision != SVX_FP64)
-            throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "batched solves run the FP64 form"};
-        const int ndof = models[0].ndof;
-        // concatenate into one block-diagonal model
-        int64_t nn = 0, ne = 0, nc = 0, nf = 0;
-        for (int32_t k = 0; k < count; ++k) {
-            const svx_flat_model_t& m = models[k];
-            try {
-                check_flat(&m);
-            } catch (const ModelFail& f) {
-                throw ModelFail{f.code, f.reason, f.elem_index,
-                                "model " + std::to_string(k) + ": " + f.message};
-            }
-            if (m.ndof != ndof)
-                throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "models of one batch share ndof"};
-            for (int64_t e = 0; e < m.n_elem; ++e) {
-                const int r = material_reason(&m, e);
-                if (r)
-                    throw ModelFail{SVX_INVALID_MODEL, r, e,
-                                    "model " + std::to_string(k) + ": " +
-                                        element_message(&m, e, r)};
-            }
-            nn += m.n_nodes;
-            ne += m.n_elem;
-            nc += m.n_elem ? m.conn_ptr[m.n_elem] : 0;
-            nf += m.n_fixed;
-        }
-        const size_t une = static_cast<size_t>(ne);
-        std::vector<double> xyz(static_cast<size_t>(3 * nn)), E(une), nu(une), th(une);
-        std::vector<double> f(static_cast<size_t>(nn * ndof), 0.0);
-        std::vector<uint8_t> kind(une);
-        std::vector<int64_t> conn_ptr(une + 1, 0), fixed;
-        std::vector<int32_t> conn(static_cast<size_t>(nc));
-        std::vector<int64_t> node_off(static_cast<size_t>(count) + 1, 0);
-        std::vector<int64_t> elem_off(static_cast<size_t>(count) + 1, 0);
-        fixed.reserve(size_t(nf));
-        for (int32_t k = 0; k < count; ++k) {
-            const svx_flat_model_t& m = models[k];
-            const int64_t n0 = node_off[k], e0 = elem_off[k];
-            std::memcpy(xyz.data() + 3 * n0, m.xyz, sizeof(double) * 3 * m.n_nodes);
-            if (m.f) std::memcpy(f.data() + n0 * ndof, m.f, sizeof(double) * m.n_nodes * ndof);
-            const int64_t c0 = conn_ptr[e0];
-            for (int64_t e = 0; e < m.n_elem; ++e) {
-                kind[e0 + e] = m.kind[e];
-                E[e0 + e] = m.youngs[e];
-                nu[e0 + e] = m.poisson[e];
-                th[e0 + e] = m.thickness;
-                conn_ptr[e0 + e + 1] = c0 + m.conn_ptr[e + 1];
-            }
-            for (int64_t q = 0; q < (m.n_elem ? m.conn_ptr[m.n_elem] : 0); ++q)
-                conn[c0 + q] = int32_t(m.conn[q] + n0);
-            for (int64_t j = 0; j < m.n_fixed; ++j) fixed.push_back(m.fixed_row[j] + n0 * ndof);
-            node_off[k + 1] = n0 + m.n_nodes;
-            elem_off[k + 1] = e0 + m.n_elem;
-        }
-        svx_flat_model_t all{};
-        all.n_nodes = nn;
-        all.xyz = xyz.data();
-        all.n_elem = ne;
-        all.kind = kind.data();
-        all.conn_ptr = conn_ptr.data();
-        all.conn = conn.data();
-        all.youngs = E.data();
-        all.poisson = nu.data();
-        all.thickness = 1.0;
-        all.ndof = ndof;
-        all.n_fixed = int64_t(fixed.size());
-        all.fixed_row = fixed.data();
-        all.f = f.data();
-        std::unique_ptr<svx_op> op(assemble_impl(ctx, &all, 0, th.data()));
-        std::vector<double> tol(static_cast<size_t>(count), o.tol);
-        std::vector<int64_t> mi(static_cast<size_t>(count));
-        for (int32_t k = 0; k < count; ++k)
-            mi[k] = o.max_iter > 0 ? o.max_iter
-                                   : default_max_iter((node_off[k + 1] - node_off[k]) * ndof);
-        std::vector<int64_t> it;
-        std::vector<double> res, cond;
-        std::vector<int32_t> status;
-        BatchStats bs;
-        batch_pcg(ctx, op.get(), count, node_off, tol, mi, it, res, status, cond, &bs);
-        cudaStream_t st = ctx->stream;
-        double ms_stress = 0.0;
-        if (von_mises && o.want_stress) {
-            SVX_CUDA(cudaEventRecord(ctx->ev[4], st));
-            if (!op->vm_elem.p) op->vm_elem.alloc(ctx->pool, op->n_elem + 1);
-            recover_stress(ctx, op.get(), op->u.p, op->vm_elem.p, nullptr, nullptr, nullptr);
-            SVX_CUDA(cudaEventRecord(ctx->ev[5], st));
-            ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
-            for (int32_t k = 0; k < count; ++k)
-                if (von_mises[k] && elem_off[k + 1] > elem_off[k])
-                    SVX_CUDA(cudaMemcpyAsync(von_mises[k], op->vm_elem.p + elem_off[k],
-                                             (elem_off[k + 1] - elem_off[k]) * sizeof(double),
-                                             cudaMemcpyDeviceToHost, st));
-        }
-        if (u)
-            for (int32_t k = 0; k < count; ++k)
-                if (u[k])
-                    SVX_CUDA(cudaMemcpyAsync(u[k], op->u.p + node_off[k] * ndof,
-                                             (node_off[k + 1] - node_off[k]) * ndof *
-                                                 sizeof(double),
-                                             cudaMemcpyDeviceToHost, st));
-        SVX_CUDA(cudaStreamSynchronize(st));
-        std::vector<int64_t> nb(static_cast<size_t>(count) + 1);
-        for (int32_t k = 0; k <= count; ++k)
-            SVX_CUDA(cudaMemcpyAsync(&nb[k], op->pat.node_base.p + node_off[k], sizeof(int64_t),
-                                     cudaMemcpyDeviceToHost, st));
-        SVX_CUDA(cudaStreamSynchronize(st));
-        int64_t total_it = 0;
+        std::vector<const svx_flat_model_t*> ptrs(static_cast<size_t>(count));
+        for (int32_t k = 0; k < count; ++k) ptrs[k] = &models[k];
+        std::vector<BatchModelOut> out;
+        BatchRun run;
+        run_batch(ctx, count, ptrs.data(), o, u, von_mises, out, run);
+        int64_t total_it = 0, total_dof = 0;
         int failed = 0;
         for (int32_t k = 0; k < count; ++k) {
+            const BatchModelOut& m = out[k];
             if (results) {
-                results[k].iterations = it[k];
-                results[k].residual = res[k];
-                results[k].status = status[k] == PCG_CONVERGED ? SVX_OK : SVX_NOT_CONVERGED;
-                results[k].cond_estimate = cond[k];
-                results[k].nnz = nb[k + 1] - nb[k];
+                results[k].iterations = m.iterations;
+                results[k].residual = m.residual;
+                results[k].status = m.status;
+                results[k].reason = m.reason;
+                results[k].cond_estimate = m.cond;
+                results[k].nnz = m.nnz;
+                results[k].elem_index = m.elem_index;
             }
-            total_it += it[k];
-            failed += status[k] != PCG_CONVERGED;
+            total_it += m.iterations;
+            if (m.status == SVX_OK || m.status == SVX_NOT_CONVERGED)
+                total_dof += models[k].n_nodes * models[k].ndof;
+            failed += m.status != SVX_OK;
         }
         if (stats) {
-            stats->ms_assemble = op->ms_assemble;
-            stats->ms_solve = bs.ms_solve;
-            stats->ms_stress = ms_stress;
-            stats->threads_per_cta = bs.threads_per_cta;
-            stats->lanes_per_node = bs.lanes_per_node;
+            stats->ms_assemble = run.ms_assemble;
+            stats->ms_solve = run.ms_solve;
+            stats->ms_stress = run.ms_stress;
+            stats->threads_per_cta = run.threads_per_cta;
+            stats->lanes_per_node = run.lanes_per_node;
             stats->total_iterations = total_it;
-            stats->total_dof = nn * ndof;
+            stats->total_dof = total_dof;
             stats->not_converged = failed;
+            stats->cluster_members = run.cluster_members;
+            stats->fp32_iterations = run.fp32_iterations;
         }
         clear_error(err);
         return SVX_OK;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include <cstdint>
@@ -52,22 +53,42 @@ struct ModelFail {
 // Caching device allocator owned by a context: freed blocks are kept and
 // reused by later requests of the same rounded size, so repeated solves on
 // one context do not call cudaMalloc.
+// Caching device allocator.  Freed blocks are kept by size class and handed
+// out again; an optional arena (one cudaMalloc reserved up front, e.g. a
+// server's whole budget) is carved first-fit with coalescing free ranges, so
+// a steady stream of batches of varying size makes no driver calls.
 class DevicePool {
 public:
     explicit DevicePool(int device) : device_(device) {}
     ~DevicePool();
+    void reserve(size_t bytes);  // the arena; throws ModelFail on failure
     void* alloc(size_t bytes);
     void release(void* p);
-    void trim();  // return cached blocks to the driver
+    void trim();  // return cached blocks to the driver (arena blocks to the arena)
     size_t bytes_in_use() const { return in_use_; }
     size_t bytes_cached() const { return cached_; }
+    size_t arena_bytes() const { return arena_size_; }
+    double malloc_ms() const { return malloc_ms_; }  // wall clock in cudaMalloc / cudaFree
+    long long mallocs() const { return mallocs_; }
 
 private:
+    bool in_arena(void* p) const {
+        return arena_ && static_cast<char*>(p) >= arena_ &&
+               static_cast<char*>(p) < arena_ + arena_size_;
+    }
+    void* carve(size_t bytes);        // under mu_
+    void give_back(void* p, size_t bytes);  // under mu_
+    void flush_arena_cache();         // under mu_
     int device_;
     std::mutex mu_;
-    std::multimap<size_t, void*> free_;      // size -> block
+    std::multimap<size_t, void*> free_;      // size -> cached block
     std::map<void*, size_t> sizes_;          // live + cached blocks
+    char* arena_ = nullptr;
+    size_t arena_size_ = 0;
+    std::map<size_t, size_t> ranges_;        // arena offset -> free length
     size_t in_use_ = 0, cached_ = 0;
+    double malloc_ms_ = 0.0;
+    long long mallocs_ = 0;
 };
 
 // Typed device buffer returned to the pool on destruction.
@@ -101,15 +122,54 @@ struct DBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// Growable page-locked host buffer (one per context) that stages batched
+// uploads and downloads, so they run as single DMA copies.  Contents are
+// valid until the next get(); callers synchronise their stream first.
+class PinnedBuffer {
+public:
+    PinnedBuffer() = default;
+    PinnedBuffer(const PinnedBuffer&) = delete;
+    PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+    ~PinnedBuffer() {
+        if (p_) cudaFreeHost(p_);
+    }
+    void* get(size_t bytes) {
+        if (bytes > cap_) {
+            if (p_) cudaFreeHost(p_);
+            p_ = nullptr;
+            cap_ = 0;
+            const size_t want = std::max(bytes, cap_ + cap_ / 2);
+            cudaError_t e = cudaHostAlloc(&p_, want, cudaHostAllocDefault);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                p_ = nullptr;
+                throw ModelFail{SVX_OOM, 0, -1, "page-locked host allocation failed"};
+            }
+            cap_ = want;
+        }
+        return p_;
+    }
+
+private:
+    void* p_ = nullptr;
+    size_t cap_ = 0;
+};
+
 }  // namespace svx
 
 // ------------------------------------------------------------------ context
 struct svx_ctx {
     int device = 0;
     int sm_count = 0;
-    int batch_choice[2] = {-1, -1};  // autotuned batched-PCG config per ndof (2, 3)
+    int batch_choice[4] = {-1, -1, -1, -1};  // autotuned batched-PCG shape: FP64 (2D, 3D),
+                                             // mixed (2D, 3D)
     cudaStream_t stream = nullptr;
+    cudaStream_t pcg_stream = nullptr;  // batched PCG (lowest priority)
+    cudaStream_t aux_stream = nullptr;  // its cluster kernel (lowest priority)
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     svx::DevicePool* pool = nullptr;
+    svx::PinnedBuffer staging;  // batched host<->device staging
+    bool owns_pool = true;  // false for a server lane (pool shared by the lanes)
     std::string last_error;
     cudaEvent_t ev[8] = {};
 };
@@ -258,13 +318,42 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3);
 // (svx_pcg.cu).  node_off[count + 1] delimits each instance's nodes.
 struct BatchStats {
     double ms_solve = 0.0;
+    int64_t fp32_iterations = 0;  // mixed form: iterations on the FP32 operator
+    int cluster_members = 0;      // members solved by the cluster kernel
+    std::vector<int64_t> member_nnz;  // nonzeros of each member's K
     int threads_per_cta = 0;
     int lanes_per_node = 0;
 };
+// FP32 difference-form copy of the operator for the mixed forms (svx_pcg.cu).
+void build_fp32_operator(svx_ctx* ctx, svx_op* op);
 void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& node_off,
                const std::vector<double>& tol, const std::vector<int64_t>& max_iter,
                std::vector<int64_t>& it, std::vector<double>& res, std::vector<int32_t>& status,
-               std::vector<double>& cond, BatchStats* stats);
+               std::vector<double>& cond, BatchStats* stats, bool mixed = false);
+
+// Per-member outcome of one batch (svx_api.cpp).
+struct BatchModelOut {
+    int64_t iterations = 0;
+    double residual = 0.0;
+    int32_t status = 0;      // svx_status
+    int32_t reason = 0;      // svx_elem_reason for InvalidModel
+    int64_t elem_index = -1;  // failing element (index within the member)
+    double cond = 0.0;
+    int64_t nnz = 0;
+    std::string message;
+};
+struct BatchRun {
+    double ms_assemble = 0.0, ms_solve = 0.0, ms_stress = 0.0;
+    // host wall clock of the phases: checks + concatenation, upload +
+    // assembly, batched PCG (incl. launch and result copies), outputs
+    double wall_prep = 0.0, wall_assemble = 0.0, wall_solve = 0.0, wall_output = 0.0;
+    int threads_per_cta = 0, lanes_per_node = 0, cluster_members = 0;
+    int64_t fp32_iterations = 0;
+};
+void check_batch_member(const svx_flat_model_t* m);
+void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* models,
+               const svx_solve_opts_t& o, double* const* u, double* const* vm,
+               std::vector<BatchModelOut>& out, BatchRun& run);
 
 // Generic device helpers (svx_pattern.cu).
 void exclusive_scan_i64(svx_ctx* ctx, const int64_t* in, int64_t* out, int64_t n,

@@ -24,6 +24,8 @@
 
 #include "svx_internal.h"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -38,6 +40,10 @@ constexpr int BLOCK = 256;
 // Resident blocks per SM the node-block SpMV kernels are compiled for; their
 // grids are exactly one wave of that many blocks per SM.
 constexpr int NODE_BLOCKS_PER_SM = 5;
+// Resident threads per SM the batched kernels are compiled for: 1,024 (at
+// most 64 registers a thread) for 3D members, 1,536 for the lighter 2D ones,
+// to keep enough node gathers in flight.
+constexpr int BATCH_MIN_THREADS = 1024;
 
 // ------------------------------------------------------------ reductions
 __device__ __forceinline__ double warp_sum(double v) {
@@ -487,11 +493,51 @@ __global__ void correct_kernel(int64_t n, double* __restrict__ u, const float* _
         u[i] += scale * double(d[i]);
 }
 
-__global__ void to_float_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
-    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * BLOCK)
-        b[i] = float(a[i]);
+// The FP32 operator of the mixed form.  Rounding each entry of K to FP32
+// (relative error ~6e-8) breaks K's translation null space: for a smooth
+// field x the product K x is the small difference of large terms, and the
+// rounded operator's error eps32 * sum_j |K_ij| |x_j| swamps it on a
+// slender, high-contrast model (the true residual of CG on that operator
+// stalls near 1e-8).  The stored operator is therefore written in
+// difference form around each node's own block:
+//   (K x)_i = sum_{j != i} K_ij (x_j - x_i) + R_i x_i,   R_i = sum_j K_ij,
+// an identity for any K.  Off-diagonal node blocks are stored as FP32 and
+// the slot of the node's own block holds R_i (summed in FP64, then
+// rounded), which vanishes in the interior of a free region.  The error of
+// the stored operator becomes sum_{j != i} dK_ij (x_j - x_i) + dR_i x_i:
+// it scales with the differences of x between neighbouring nodes instead of
+// x itself, and a rigid translation is reproduced exactly.  The SpMV of
+// this operator (node_rows_cg / node_rows_mv with M = float) subtracts x_i
+// from every neighbour but the node itself.
+template <int ND>
+__global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                                        const int32_t* __restrict__ adj,
+                                        const int64_t* __restrict__ node_base,
+                                        const double* __restrict__ vals,
+                                        float* __restrict__ out) {
+    const int64_t t = int64_t(blockIdx.x) * BLOCK + threadIdx.x;
+    const int64_t i = t / (ND * ND);
+    if (i >= n_nodes) return;
+    const int da = int(t % (ND * ND)) / ND, db = int(t % ND);
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const int64_t base = node_base[i];
+    if (d == 0) {  // an unreferenced node: its rows hold only the diagonal
+        if (db == 0) out[base + da] = float(vals[base + da]);
+        return;
+    }
+    const int64_t row = base + int64_t(da) * ND * d + db;
+    double sum = 0.0;
+    int self = -1;
+    for (int k = 0; k < d; ++k) {
+        const double v = vals[row + k * ND];
+        sum += v;
+        if (adj[a0 + k] == int32_t(i)) self = k;
+        else out[row + k * ND] = float(v);
+    }
+    if (self >= 0) out[row + self * ND] = float(sum);
 }
+
 
 
 // ------------------------------------------------------------ persistent PCG
@@ -526,12 +572,25 @@ __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr
         return;
     }
     const int rowlen = ND * d;
+    // FP32 operators are stored in difference form (compensated_fp32_kernel)
+    constexpr bool DIFF = std::is_same<M, float>::value;
+    double xi[ND];
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xi[db] = double(__ldcg(x + i * ND + db));
+    }
 #pragma unroll 2
     for (int k = gl; k < d; k += G) {
-        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        const int32_t j = __ldg(adj + a0 + k);
+        const int64_t c = int64_t(j) * ND;
         double xv[ND];
 #pragma unroll
         for (int db = 0; db < ND; ++db) xv[db] = double(__ldcg(x + c + db));
+        if constexpr (DIFF) {
+            if (j != int32_t(i))
+#pragma unroll
+                for (int db = 0; db < ND; ++db) xv[db] -= xi[db];
+        }
 #pragma unroll
         for (int da = 0; da < ND; ++da)
 #pragma unroll
@@ -696,11 +755,14 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
 
 // ------------------------------------------------------------ batched PCG
 // Thousands of independent models concatenated into one block-diagonal
-// operator.  One launch; each CTA takes the next instance from an atomic
-// queue (instances ordered by size, largest first) and runs that instance's
-// whole Jacobi-PCG with CTA-local reductions, so every instance has its own
-// alpha/beta, its own convergence test and its own iteration count, and no
-// CTA ever waits for another.  An instance is always computed by one CTA of
+// operator.  One launch with one CTA per instance (instances ordered by
+// size, largest first, so the block scheduler hands out the longest work
+// first); the CTA runs that instance's whole Jacobi-PCG with CTA-local
+// reductions, so every instance has its own alpha/beta, its own convergence
+// test and its own iteration count, and no CTA ever waits for another.  The
+// grid is not persistent: CTAs of other streams' kernels (the assembly of
+// the next served batch, on a higher-priority stream) are scheduled as soon
+// as any instance finishes.  An instance is always computed by one CTA of
 // the same shape, so its result does not depend on what else is in the
 // batch.
 template <int ND, int G, class M>
@@ -719,11 +781,23 @@ __device__ __forceinline__ void node_rows_mv(const int64_t* __restrict__ adj_ptr
         return;
     }
     const int rowlen = ND * d;
+    constexpr bool DIFF = std::is_same<M, float>::value;  // difference form
+    double xi[ND];
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xi[db] = x[i * ND + db];
+    }
     for (int k = gl; k < d; k += G) {
-        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        const int32_t j = __ldg(adj + a0 + k);
+        const int64_t c = int64_t(j) * ND;
         double xv[ND];
 #pragma unroll
         for (int db = 0; db < ND; ++db) xv[db] = x[c + db];
+        if constexpr (DIFF) {
+            if (j != int32_t(i))
+#pragma unroll
+                for (int db = 0; db < ND; ++db) xv[db] -= xi[db];
+        }
 #pragma unroll
         for (int da = 0; da < ND; ++da)
 #pragma unroll
@@ -733,26 +807,19 @@ __device__ __forceinline__ void node_rows_mv(const int64_t* __restrict__ adj_ptr
 }
 
 template <int ND, int G, int BS, class M>
-__global__ void __launch_bounds__(BS)
+__global__ void __launch_bounds__(BS, (ND == 2 ? 1536 : BATCH_MIN_THREADS) / BS)
 batch_pcg_kernel(int count, const int32_t* __restrict__ order, const int64_t* __restrict__ node_off,
                  const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj,
                  const int64_t* __restrict__ node_base, const M* __restrict__ vals,
                  const double* __restrict__ inv_diag, const double* __restrict__ f, double* u,
                  double* r, double* p, double* q, const double* __restrict__ tol,
                  const int64_t* __restrict__ max_iter, int64_t* __restrict__ out_it,
-                 double* __restrict__ out_res, int32_t* __restrict__ out_status,
-                 unsigned int* queue) {
+                 double* __restrict__ out_res, int32_t* __restrict__ out_status) {
     __shared__ double sh[32];
-    __shared__ int next;
     const int gl = threadIdx.x & (G - 1);
     const int64_t warp_nodes = 32 / G;
     const int64_t step = int64_t(BS / 32) * warp_nodes;
-    for (;;) {
-        if (threadIdx.x == 0) next = int(atomicAdd(queue, 1u));
-        __syncthreads();
-        const int k = next;
-        __syncthreads();
-        if (k >= count) return;
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
         const int inst = order[k];
         const int64_t n0 = node_off[inst], n1 = node_off[inst + 1];
         const int64_t r0 = n0 * ND, r1 = n1 * ND;
@@ -833,6 +900,400 @@ batch_pcg_kernel(int count, const int32_t* __restrict__ order, const int64_t* __
             out_status[inst] = status;
         }
     }
+}
+
+// Mixed form of the batched PCG: per instance, the same CG runs on the FP32
+// difference-form operator (vals32) in segments; a segment ends when its
+// recursive r.r has dropped by delta^2, after SEG_CAP iterations, or when
+// the recursive residual meets the tolerance.  The CTA then replaces r by
+// the true residual f - K u of the FP64 operator (reliable update; the
+// search direction p is kept), tests convergence on it, and switches the
+// instance to the FP64 operator, restarting CG there (p = z), once two
+// segments failed to cut the true residual 3x (continuing the FP32-built
+// search direction under the FP64 operator can stall CG for thousands of
+// iterations).  All of it is CTA-local, so every instance keeps its own
+// scalars and its result does not depend on the rest of the batch.
+template <int ND, int G, int BS>
+__global__ void __launch_bounds__(BS, BATCH_MIN_THREADS / BS)
+batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
+                       const int64_t* __restrict__ node_off, const int64_t* __restrict__ adj_ptr,
+                       const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                       const double* __restrict__ vals, const float* __restrict__ vals32,
+                       const double* __restrict__ inv_diag, const double* __restrict__ f,
+                       double* u, double* r, double* p, double* q, const double* __restrict__ tol,
+                       const int64_t* __restrict__ max_iter, int64_t* __restrict__ out_it,
+                       double* __restrict__ out_res, int32_t* __restrict__ out_status,
+                       int64_t* __restrict__ out_fp32_it) {
+    constexpr int64_t SEG_CAP = 500;
+    constexpr double DELTA2 = 0.01;    // segment ends once r.r dropped 100x (||r|| 10x)
+    constexpr double PROGRESS = 0.3;   // true-residual cut a segment must reach
+    __shared__ double sh[32];
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t warp_nodes = 32 / G;
+    const int64_t step = int64_t(BS / 32) * warp_nodes;
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        const int inst = order[k];
+        const int64_t n0 = node_off[inst], n1 = node_off[inst + 1];
+        const int64_t r0 = n0 * ND, r1 = n1 * ND;
+        const double tl = tol[inst];
+        const int64_t mi = max_iter[inst];
+        double rr = 0.0, rz = 0.0;
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+            const double ri = f[row];
+            u[row] = 0.0;
+            r[row] = ri;
+            const double zi = ri * inv_diag[row];
+            p[row] = zi;
+            rr += ri * ri;
+            rz += ri * zi;
+        }
+        rr = block_sum(rr, sh);
+        rz = block_sum(rz, sh);
+        const double bnorm = sqrt(rr);
+        int64_t it = 0, fp32_it = 0, seg_start = 0;
+        int status = (bnorm == 0.0) ? PCG_CONVERGED : PCG_RUNNING;
+        double res = (bnorm == 0.0) ? 0.0 : 1.0;
+        double seg_stop = DELTA2 * rr, best = 1.0;
+        int stagnant = 0;
+        bool exact = false, restart = false;
+        while (status == PCG_RUNNING) {
+            double dot = 0.0;
+            for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1; nb += step) {
+                const int64_t i = nb + ((threadIdx.x & 31) / G);
+                double acc[ND];
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                if (i < n1) {
+                    if (exact)
+                        node_rows_mv<ND, G, double>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+                    else
+                        node_rows_mv<ND, G, float>(adj_ptr, adj, node_base, vals32, p, i, gl,
+                                                   acc);
+                }
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                if (i < n1 && gl == 0) {
+#pragma unroll
+                    for (int da = 0; da < ND; ++da) {
+                        q[i * ND + da] = acc[da];
+                        dot += p[i * ND + da] * acc[da];
+                    }
+                }
+            }
+            const double pap = block_sum(dot, sh);
+            if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
+                status = PCG_BREAKDOWN;
+                it += 1;
+                res = sqrt(rr) / bnorm;
+                break;
+            }
+            const double alpha = rz / pap;
+            double lrr = 0.0, lrz = 0.0;
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+                u[row] += alpha * p[row];
+                const double ri = r[row] - alpha * q[row];
+                r[row] = ri;
+                const double zi = ri * inv_diag[row];
+                lrr += ri * ri;
+                lrz += ri * zi;
+            }
+            rr = block_sum(lrr, sh);
+            double rz_new = block_sum(lrz, sh);
+            it += 1;
+            if (!exact) ++fp32_it;
+            res = sqrt(rr) / bnorm;
+            if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl)) {
+                // reliable update: r = f - K64 u, then r.r and r.z of it
+                __syncthreads();
+                double trr = 0.0, trz = 0.0;
+                for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1;
+                     nb += step) {
+                    const int64_t i = nb + ((threadIdx.x & 31) / G);
+                    double acc[ND];
+#pragma unroll
+                    for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                    if (i < n1)
+                        node_rows_mv<ND, G, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
+#pragma unroll
+                    for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                    if (i < n1 && gl == 0) {
+#pragma unroll
+                        for (int da = 0; da < ND; ++da) {
+                            const int64_t row = i * ND + da;
+                            const double ri = f[row] - acc[da];
+                            r[row] = ri;
+                            trr += ri * ri;
+                            trz += ri * (ri * inv_diag[row]);
+                        }
+                    }
+                }
+                rr = block_sum(trr, sh);
+                rz_new = block_sum(trz, sh);
+                res = sqrt(rr) / bnorm;
+                // a segment meant to cut the residual 10x that did not cut the
+                // true one 3x is lost to the FP32 operator's error
+                if (res > PROGRESS * best) ++stagnant;
+                best = fmin(best, res);
+                if (stagnant >= 2) {
+                    exact = true;    // FP64 operator from here on, and CG
+                    restart = true;  // restarted: p = z
+                }
+                seg_stop = DELTA2 * rr;
+                seg_start = it;
+            }
+            if (res <= tl) {
+                status = PCG_CONVERGED;
+                break;
+            }
+            if (it >= mi) {
+                status = PCG_MAXITER;
+                break;
+            }
+            const double beta = restart ? 0.0 : rz_new / rz;
+            restart = false;
+            rz = rz_new;
+            __syncthreads();  // r rows written by other lanes of this CTA
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS)
+                p[row] = r[row] * inv_diag[row] + beta * p[row];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            out_it[inst] = it;
+            out_res[inst] = res;
+            out_status[inst] = status;
+            out_fp32_it[inst] = fp32_it;
+        }
+    }
+}
+
+// Large members of a batch: one thread-block cluster of CS CTAs per
+// instance.  A single CTA streams a 100k-DOF member's K at a few tens of
+// GB/s, so the largest members would run alone for seconds at the end of a
+// batch.  The CTAs of a cluster are co-scheduled by the hardware, split the
+// member's nodes into CS contiguous ranges and meet at cluster barriers
+// (barrier.cluster arrive.release / wait.acquire, so the p, u and r rows
+// other CTAs of the cluster wrote are visible, read through L2).  Dots are
+// reduced per CTA, published in shared memory and summed by every CTA over
+// the cluster's ranks through distributed shared memory in rank order, so
+// all CTAs hold bitwise the same scalars and the result does not depend on
+// the rest of the batch.  The partial slots of consecutive phases differ,
+// and every slot is rewritten only after a later cluster barrier, so one
+// barrier per phase suffices.  MIXED runs the reliable-update form of
+// batch_pcg_mixed_kernel with the same rules.
+template <int ND, int G, int BS, int CS, bool MIXED>
+__global__ void __launch_bounds__(BS, (MIXED ? 768 : BATCH_MIN_THREADS) / BS)
+batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
+                         const int64_t* __restrict__ node_off,
+                         const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj,
+                         const int64_t* __restrict__ node_base, const double* __restrict__ vals,
+                         const float* __restrict__ vals32, const double* __restrict__ inv_diag,
+                         const double* __restrict__ f, double* u, double* r, double* p,
+                         double* q, const double* __restrict__ tol,
+                         const int64_t* __restrict__ max_iter, int64_t* __restrict__ out_it,
+                         double* __restrict__ out_res, int32_t* __restrict__ out_status,
+                         int64_t* __restrict__ out_fp32_it) {
+    namespace cgx = cooperative_groups;
+    constexpr int64_t SEG_CAP = 500;
+    constexpr double DELTA2 = 0.01, PROGRESS = 0.3;
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int crank = int(cluster.block_rank());
+    __shared__ double sh[32];
+    __shared__ double part[5];  // A: p.q | B: r.r, r.z | T: true r.r, r.z
+    __shared__ double tot[2];
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t warp_nodes = 32 / G;
+    const int64_t step = int64_t(BS / 32) * warp_nodes;
+    // publish this CTA's block total(s) in part[s0..s0+nv), barrier, sum
+    // over the cluster's ranks in rank order
+    auto reduce = [&](int s0, int nv) {
+        cluster.sync();
+        if (threadIdx.x == 0)
+            for (int s = 0; s < nv; ++s) {
+                double t = 0.0;
+                for (int c = 0; c < CS; ++c) t += *cluster.map_shared_rank(&part[s0 + s], c);
+                tot[s] = t;
+            }
+        __syncthreads();
+    };
+    const int n_clusters = int(gridDim.x) / CS;
+    for (int k = int(blockIdx.x) / CS; k < count; k += n_clusters) {
+        cluster.sync();  // the previous member's partials are read by now
+        const int inst = order[k];
+        const int64_t N0 = node_off[inst], N1 = node_off[inst + 1];
+        const int64_t n0 = N0 + (N1 - N0) * crank / CS, n1 = N0 + (N1 - N0) * (crank + 1) / CS;
+        const int64_t r0 = n0 * ND, r1 = n1 * ND;
+        const double tl = tol[inst];
+        const int64_t mi = max_iter[inst];
+        double lrr = 0.0, lrz = 0.0;
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+            const double ri = f[row];
+            u[row] = 0.0;
+            r[row] = ri;
+            const double zi = ri * inv_diag[row];
+            p[row] = zi;
+            lrr += ri * ri;
+            lrz += ri * zi;
+        }
+        {
+            const double a = block_sum(lrr, sh), b = block_sum(lrz, sh);
+            if (threadIdx.x == 0) {
+                part[1] = a;
+                part[2] = b;
+            }
+        }
+        reduce(1, 2);
+        double rr = tot[0], rz = tot[1];
+        const double bnorm = sqrt(rr);
+        int64_t it = 0, fp32_it = 0, seg_start = 0;
+        int status = (bnorm == 0.0) ? PCG_CONVERGED : PCG_RUNNING;
+        double res = (bnorm == 0.0) ? 0.0 : 1.0;
+        double seg_stop = DELTA2 * rr, best = 1.0;
+        int stagnant = 0;
+        bool exact = !MIXED, restart = false;
+        while (status == PCG_RUNNING) {
+            // A: q = K p on own nodes (neighbours' p from L2), p.q
+            double dot = 0.0;
+            for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1; nb += step) {
+                const int64_t i = nb + ((threadIdx.x & 31) / G);
+                double acc[ND];
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                if (i < n1) {
+                    if (exact)
+                        node_rows_cg<ND, G, double, double>(adj_ptr, adj, node_base, vals, p, i,
+                                                            gl, acc);
+                    else
+                        node_rows_cg<ND, G, float, double>(adj_ptr, adj, node_base, vals32, p, i,
+                                                           gl, acc);
+                }
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                if (i < n1 && gl == 0) {
+#pragma unroll
+                    for (int da = 0; da < ND; ++da) {
+                        q[i * ND + da] = acc[da];
+                        dot += p[i * ND + da] * acc[da];
+                    }
+                }
+            }
+            {
+                const double a = block_sum(dot, sh);
+                if (threadIdx.x == 0) part[0] = a;
+            }
+            reduce(0, 1);
+            const double pap = tot[0];
+            if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
+                status = PCG_BREAKDOWN;
+                it += 1;
+                res = sqrt(rr) / bnorm;
+                break;
+            }
+            const double alpha = rz / pap;
+            // B: u, r on own rows; r.r, r.z
+            lrr = 0.0;
+            lrz = 0.0;
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
+                u[row] += alpha * p[row];
+                const double ri = r[row] - alpha * q[row];
+                r[row] = ri;
+                const double zi = ri * inv_diag[row];
+                lrr += ri * ri;
+                lrz += ri * zi;
+            }
+            {
+                const double a = block_sum(lrr, sh), b = block_sum(lrz, sh);
+                if (threadIdx.x == 0) {
+                    part[1] = a;
+                    part[2] = b;
+                }
+            }
+            reduce(1, 2);
+            rr = tot[0];
+            double rz_new = tot[1];
+            it += 1;
+            if (!exact) ++fp32_it;
+            res = sqrt(rr) / bnorm;
+            if constexpr (MIXED) {
+                if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl)) {
+                    // T: r = f - K64 u on own nodes (neighbours' u from L2)
+                    double trr = 0.0, trz = 0.0;
+                    for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1;
+                         nb += step) {
+                        const int64_t i = nb + ((threadIdx.x & 31) / G);
+                        double acc[ND];
+#pragma unroll
+                        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                        if (i < n1)
+                            node_rows_cg<ND, G, double, double>(adj_ptr, adj, node_base, vals, u,
+                                                                i, gl, acc);
+#pragma unroll
+                        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                        if (i < n1 && gl == 0) {
+#pragma unroll
+                            for (int da = 0; da < ND; ++da) {
+                                const int64_t row = i * ND + da;
+                                const double ri = f[row] - acc[da];
+                                r[row] = ri;
+                                trr += ri * ri;
+                                trz += ri * (ri * inv_diag[row]);
+                            }
+                        }
+                    }
+                    {
+                        const double a = block_sum(trr, sh), b = block_sum(trz, sh);
+                        if (threadIdx.x == 0) {
+                            part[3] = a;
+                            part[4] = b;
+                        }
+                    }
+                    reduce(3, 2);
+                    rr = tot[0];
+                    rz_new = tot[1];
+                    res = sqrt(rr) / bnorm;
+                    if (res > PROGRESS * best) ++stagnant;
+                    best = fmin(best, res);
+                    if (stagnant >= 2) {
+                        exact = true;
+                        restart = true;
+                    }
+                    seg_stop = DELTA2 * rr;
+                    seg_start = it;
+                }
+            }
+            if (res <= tl) {
+                status = PCG_CONVERGED;
+                break;
+            }
+            if (it >= mi) {
+                status = PCG_MAXITER;
+                break;
+            }
+            const double beta = restart ? 0.0 : rz_new / rz;
+            restart = false;
+            rz = rz_new;
+            // C: p = z + beta p on own rows, then the cluster barrier that
+            // makes them visible to the neighbours' SpMV
+            for (int64_t row = r0 + threadIdx.x; row < r1; row += BS)
+                p[row] = r[row] * inv_diag[row] + beta * p[row];
+            cluster.sync();
+        }
+        if (crank == 0 && threadIdx.x == 0) {
+            out_it[inst] = it;
+            out_res[inst] = res;
+            out_status[inst] = status;
+            if (out_fp32_it) out_fp32_it[inst] = fp32_it;
+        }
+    }
+    // no CTA leaves while another may still read its partials
+    cluster.sync();
+}
+
+// Nonzeros of each member: node_base at the members' node offsets.
+__global__ void member_nnz_kernel(int count, const int64_t* __restrict__ node_off,
+                                  const int64_t* __restrict__ node_base,
+                                  int64_t* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) out[k] = node_base[node_off[k + 1]] - node_base[node_off[k]];
 }
 
 // Extreme |K_ii| of each instance (its cond_estimate), one CTA per instance.
@@ -1093,6 +1554,22 @@ int auto_check_every(int64_t n, int64_t nnz) {
 
 }  // namespace
 
+void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
+    if (op->vals32.p) return;
+    op->vals32.alloc(ctx->pool, op->pat.nnz + 1);
+    const int64_t threads = op->n_nodes * op->ndof * op->ndof;
+    const unsigned grid = unsigned(std::max<int64_t>(1, (threads + BLOCK - 1) / BLOCK));
+    const Pattern& P = op->pat;
+    if (op->ndof == 3)
+        compensated_fp32_kernel<3><<<grid, BLOCK, 0, ctx->stream>>>(
+            op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p, op->vals32.p);
+    else
+        compensated_fp32_kernel<2><<<grid, BLOCK, 0, ctx->stream>>>(
+            op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p, op->vals32.p);
+    SVX_LAUNCH_CHECK();
+}
+
+
 std::atomic<long long> g_launches{0};
 
 void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
@@ -1250,23 +1727,19 @@ reliable_resume_kernel(int64_t n, const double* __restrict__ r64, V* __restrict_
 // recursive residual has dropped by `delta` or after `seg_cap` iterations;
 // the host then computes the true residual r = f - K64 u with the FP64
 // operator, replaces the recursive one with it and resumes with the same
-// search direction (the Krylov space is kept).  The FP32 operator differs
-// from K by ~1e-7 per entry, so on an ill-conditioned system the true
-// residual stops improving well above 1e-10; once it fails to halve over two
-// segments the same CG continues with the FP64 operator to the tolerance.
-// The bulk of the iterations stream 4 B instead of 8 B per nonzero.
+// search direction (the Krylov space is kept).  The FP32 operator is the
+// difference form of compensated_fp32_kernel; on an ill-conditioned system
+// its error still slows the true residual, so once two segments failed to
+// cut it by sqrt(delta) the solve continues with the FP64 operator to the
+// tolerance, restarting CG there (p = z).  The FP32 iterations stream
+// 4.44 B instead of 8.44 B per nonzero.
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps) {
     (void)check_every;
     const double delta = (inner_tol > 0.01 && inner_tol < 1.0) ? inner_tol : 0.1;
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
-    if (!op->vals32.p) {
-        op->vals32.alloc(ctx->pool, op->pat.nnz + 1);
-        to_float_kernel<<<grid_vec(ctx, op->pat.nnz), BLOCK, 0, st>>>(op->pat.nnz, op->vals.p,
-                                                                       op->vals32.p);
-        SVX_LAUNCH_CHECK();
-    }
+    build_fp32_operator(ctx, op);
     const int G = pick_node_group(op->pat.max_deg);
     DBuf<double> r, p, q, r64, partials, rr_dev;
     DBuf<PcgScalars> s;
@@ -1370,16 +1843,18 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
             status = PCG_MAXITER;
             break;
         }
-        if (res < 0.5 * best_true) {
-            best_true = res;
-            stagnant = 0;
-        } else {
-            ++stagnant;
-        }
+        // a segment meant to cut the residual by delta that did not cut the
+        // true one by sqrt(delta) is lost to the FP32 operator's error
+        if (res > std::sqrt(delta) * best_true) ++stagnant;
+        best_true = std::min(best_true, res);
         fp64_phase = stagnant >= 2;
         reliable_resume_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, r64.p, r.p, op->inv_diag.p,
                                                                 partials.p, s.p);
         SVX_LAUNCH_CHECK();
+        // entering the FP64 phase restarts CG (p = z): the FP32-built search
+        // direction under the FP64 operator can stall CG for thousands of
+        // iterations
+        if (fp64_phase) set_field(&PcgScalars::beta, 0.0);
         set_field(&PcgScalars::rr, rr_true);
         set_field(&PcgScalars::res, res);
         set_field(&PcgScalars::rr_stop, fp64_phase ? -1.0 : delta * delta * rr_true);
@@ -1582,7 +2057,7 @@ namespace {
 using BatchFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*, const int32_t*,
                          const int64_t*, const double*, const double*, const double*, double*,
                          double*, double*, double*, const double*, const int64_t*, int64_t*,
-                         double*, int32_t*, unsigned int*);
+                         double*, int32_t*);
 
 struct BatchConfig {
     int nd, g, bs;
@@ -1592,6 +2067,89 @@ struct BatchConfig {
 template <int ND, int G, int BS>
 BatchConfig batch_config() {
     return BatchConfig{ND, G, BS, &batch_pcg_kernel<ND, G, BS, double>};
+}
+
+using BatchMixedFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*,
+                              const int32_t*, const int64_t*, const double*, const float*,
+                              const double*, const double*, double*, double*, double*, double*,
+                              const double*, const int64_t*, int64_t*, double*, int32_t*,
+                              int64_t*);
+
+struct BatchMixedConfig {
+    int nd, g, bs;
+    BatchMixedFn fn;
+};
+
+template <int ND, int G, int BS>
+BatchMixedConfig batch_mixed_config() {
+    return BatchMixedConfig{ND, G, BS, &batch_pcg_mixed_kernel<ND, G, BS>};
+}
+
+// Candidate shapes of the batched kernels, in the same order for both forms;
+// the default (used without autotuning) is index 2 for 2D and 1 for 3D.
+std::vector<BatchMixedConfig> batch_mixed_candidates(int ndof) {
+    if (ndof == 3)
+        return {batch_mixed_config<3, 16, 128>(), batch_mixed_config<3, 16, 256>(),
+                batch_mixed_config<3, 16, 512>(), batch_mixed_config<3, 32, 256>(),
+                batch_mixed_config<3, 32, 512>()};
+    return {batch_mixed_config<2, 8, 128>(), batch_mixed_config<2, 8, 256>(),
+            batch_mixed_config<2, 8, 512>(), batch_mixed_config<2, 16, 256>(),
+            batch_mixed_config<2, 16, 512>()};
+}
+
+int batch_default_choice(int ndof) { return ndof == 3 ? 1 : 2; }
+
+// Members with at least this many rows run on a cluster of CLUSTER_CTAS CTAs
+// (build constants).  Measured on the serving mix: 3D members gain from
+// 4k rows up; 2D plates up to 13.5k rows run faster one CTA each (their
+// 18 nonzeros a row leave the cluster barriers too little work to hide).
+#ifndef SVX_CLUSTER_MIN_DOF_3D
+#define SVX_CLUSTER_MIN_DOF_3D 4096
+#endif
+#ifndef SVX_CLUSTER_MIN_DOF_2D
+#define SVX_CLUSTER_MIN_DOF_2D 16384
+#endif
+int64_t cluster_min_dof(int ndof) {
+    return ndof == 3 ? int64_t(SVX_CLUSTER_MIN_DOF_3D) : int64_t(SVX_CLUSTER_MIN_DOF_2D);
+}
+constexpr int CLUSTER_CTAS = 8;  // the portable cluster size
+constexpr int CLUSTER_BS = 256;
+
+using ClusterFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*, const int32_t*,
+                           const int64_t*, const double*, const float*, const double*,
+                           const double*, double*, double*, double*, double*, const double*,
+                           const int64_t*, int64_t*, double*, int32_t*, int64_t*);
+
+void launch_batch_cluster(int ndof, bool mixed, cudaStream_t st, int n_inst,
+                          const int32_t* order, const int64_t* node_off, const int64_t* adj_ptr,
+                          const int32_t* adj, const int64_t* node_base, const double* vals,
+                          const float* vals32, const double* inv_diag, const double* f,
+                          double* u, double* r, double* p, double* q, const double* tol,
+                          const int64_t* max_iter, int64_t* out_it, double* out_res,
+                          int32_t* out_status, int64_t* out_fp32) {
+    ClusterFn fn;
+    if (ndof == 3)
+        fn = mixed ? &batch_pcg_cluster_kernel<3, 16, CLUSTER_BS, CLUSTER_CTAS, true>
+                   : &batch_pcg_cluster_kernel<3, 16, CLUSTER_BS, CLUSTER_CTAS, false>;
+    else
+        fn = mixed ? &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, true>
+                   : &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, false>;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CLUSTER_CTAS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(CLUSTER_BS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(unsigned(n_inst * CLUSTER_CTAS));  // one cluster per member
+    SVX_CUDA(cudaLaunchKernelEx(&cfg, fn, n_inst, order, node_off, adj_ptr, adj, node_base, vals,
+                                vals32, inv_diag, f, u, r, p, q, tol, max_iter, out_it, out_res,
+                                out_status, out_fp32));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 std::vector<BatchConfig> batch_candidates(int ndof) {
@@ -1607,20 +2165,28 @@ std::vector<BatchConfig> batch_candidates(int ndof) {
 void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& node_off,
                const std::vector<double>& tol, const std::vector<int64_t>& max_iter,
                std::vector<int64_t>& it, std::vector<double>& res, std::vector<int32_t>& status,
-               std::vector<double>& cond, BatchStats* stats) {
+               std::vector<double>& cond, BatchStats* stats, bool mixed) {
     cudaStream_t st = ctx->stream;
     const int64_t n = op->n;
     const Pattern& P = op->pat;
-    // largest instances first (longest-processing-time order for the queue)
+    // Members of at least cluster_min_dof rows go to the cluster kernel (CS
+    // CTAs per member), the rest to the CTA-per-member kernel; each class is
+    // queued largest first (longest-processing-time order) and the two
+    // kernels run concurrently on the context's two streams.
     std::vector<int32_t> order(count);
     for (int k = 0; k < count; ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return node_off[a + 1] - node_off[a] > node_off[b + 1] - node_off[b];
-    });
+    auto rows_of = [&](int k) { return (node_off[k + 1] - node_off[k]) * op->ndof; };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return rows_of(a) > rows_of(b); });
+    int n_large = 0;
+    while (n_large < count && rows_of(order[n_large]) >= cluster_min_dof(op->ndof)) ++n_large;
+    const int n_small = count - n_large;
+    // small class first in the order array, then the large class
+    std::vector<int32_t> ordered(order.begin() + n_large, order.end());
+    ordered.insert(ordered.end(), order.begin(), order.begin() + n_large);
     DBuf<int32_t> d_order, d_status;
     DBuf<int64_t> d_off, d_maxit, d_it, d_cap;
     DBuf<double> d_tol, d_res, r, p, q, d_hi, d_lo;
-    DBuf<unsigned int> queue;
     d_order.alloc(ctx->pool, count + 1);
     d_off.alloc(ctx->pool, count + 1);
     d_maxit.alloc(ctx->pool, count + 1);
@@ -1631,12 +2197,11 @@ void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& 
     d_status.alloc(ctx->pool, count + 1);
     d_hi.alloc(ctx->pool, count + 1);
     d_lo.alloc(ctx->pool, count + 1);
-    queue.alloc(ctx->pool, 1);
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
     op->u.alloc(ctx->pool, n + 1);
-    SVX_CUDA(cudaMemcpyAsync(d_order.p, order.data(), count * sizeof(int32_t),
+    SVX_CUDA(cudaMemcpyAsync(d_order.p, ordered.data(), count * sizeof(int32_t),
                              cudaMemcpyHostToDevice, st));
     SVX_CUDA(cudaMemcpyAsync(d_off.p, node_off.data(), (count + 1) * sizeof(int64_t),
                              cudaMemcpyHostToDevice, st));
@@ -1644,32 +2209,53 @@ void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& 
                              cudaMemcpyHostToDevice, st));
     SVX_CUDA(cudaMemcpyAsync(d_tol.p, tol.data(), count * sizeof(double), cudaMemcpyHostToDevice,
                              st));
-    auto launch = [&](const BatchConfig& c, const int64_t* maxit, int n_inst) {
-        int bps = 0;
-        SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)c.fn, c.bs, 0));
-        const int grid = std::max(1, std::min(bps * ctx->sm_count, n_inst));
-        SVX_CUDA(cudaMemsetAsync(queue.p, 0, sizeof(unsigned int), st));
-        c.fn<<<grid, c.bs, 0, st>>>(n_inst, d_order.p, d_off.p, P.adj_ptr.p, P.adj.p,
-                                    P.node_base.p, op->vals.p, op->inv_diag.p, op->f.p, op->u.p,
-                                    r.p, p.p, q.p, d_tol.p, maxit, d_it.p, d_res.p, d_status.p,
-                                    queue.p);
+    DBuf<int64_t> d_fp32;
+    if (mixed) {
+        build_fp32_operator(ctx, op);
+        d_fp32.alloc(ctx->pool, count + 1);
+    }
+    const std::vector<BatchConfig> cands = batch_candidates(op->ndof);
+    const std::vector<BatchMixedConfig> mcands = batch_mixed_candidates(op->ndof);
+    cudaStream_t pst = ctx->pcg_stream;
+    auto launch = [&](int c, const int64_t* maxit, int n_inst) {
+        const int bs = cands[c].bs;
+        const int grid = std::max(1, n_inst);  // one CTA per member
+        if (mixed)
+            mcands[c].fn<<<grid, bs, 0, pst>>>(n_inst, d_order.p, d_off.p, P.adj_ptr.p, P.adj.p,
+                                               P.node_base.p, op->vals.p, op->vals32.p,
+                                               op->inv_diag.p, op->f.p, op->u.p, r.p, p.p, q.p,
+                                               d_tol.p, maxit, d_it.p, d_res.p, d_status.p,
+                                               d_fp32.p);
+        else
+            cands[c].fn<<<grid, bs, 0, pst>>>(n_inst, d_order.p, d_off.p, P.adj_ptr.p, P.adj.p,
+                                              P.node_base.p, op->vals.p, op->inv_diag.p,
+                                              op->f.p, op->u.p, r.p, p.p, q.p, d_tol.p, maxit,
+                                              d_it.p, d_res.p, d_status.p);
         SVX_LAUNCH_CHECK();
     };
-    // autotune (once per context and ndof): threads per CTA and lanes per
-    // node, timed on the largest instances with a short iteration budget
-    int& choice = ctx->batch_choice[op->ndof == 3 ? 1 : 0];
-    const std::vector<BatchConfig> cands = batch_candidates(op->ndof);
+    // the PCG kernels run on the context's low-priority streams, forked
+    // from (and joined back into) its main stream
+    SVX_CUDA(cudaEventRecord(ctx->fork_ev, st));
+    SVX_CUDA(cudaStreamWaitEvent(pst, ctx->fork_ev, 0));
+    // autotune of the CTA-per-member kernel (once per context, form and
+    // ndof): threads per CTA and lanes per node, timed on the largest small
+    // members with a short iteration budget.  A class smaller than the SM
+    // count is too small to time and runs the default shape without fixing
+    // the choice.
+    int& tuned = ctx->batch_choice[(mixed ? 2 : 0) + (op->ndof == 3 ? 1 : 0)];
+    int choice = tuned;
+    if (choice < 0 && n_small < ctx->sm_count) choice = batch_default_choice(op->ndof);
     if (choice < 0) {
-        const int sample = std::min(count, 2 * ctx->sm_count);
+        const int sample = std::min(n_small, 2 * ctx->sm_count);
         std::vector<int64_t> cap(count, 40);
         SVX_CUDA(cudaMemcpyAsync(d_cap.p, cap.data(), count * sizeof(int64_t),
-                                 cudaMemcpyHostToDevice, st));
+                                 cudaMemcpyHostToDevice, pst));
         float best = 0.f;
         for (size_t c = 0; c < cands.size(); ++c) {
-            launch(cands[c], d_cap.p, sample);  // warm
-            SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
-            launch(cands[c], d_cap.p, sample);
-            SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+            launch(int(c), d_cap.p, sample);  // warm
+            SVX_CUDA(cudaEventRecord(ctx->ev[0], pst));
+            launch(int(c), d_cap.p, sample);
+            SVX_CUDA(cudaEventRecord(ctx->ev[1], pst));
             SVX_CUDA(cudaEventSynchronize(ctx->ev[1]));
             float ms = 0.f;
             SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
@@ -1678,19 +2264,41 @@ void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& 
                 choice = int(c);
             }
         }
+        tuned = choice;
     }
     const BatchConfig& cfg = cands[choice];
-    SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
-    launch(cfg, d_maxit.p, count);
-    SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
+    SVX_CUDA(cudaEventRecord(ctx->ev[0], pst));
+    if (n_large > 0) {
+        // the cluster kernel on the second low-priority stream
+        SVX_CUDA(cudaEventRecord(ctx->fork_ev, pst));
+        SVX_CUDA(cudaStreamWaitEvent(ctx->aux_stream, ctx->fork_ev, 0));
+        launch_batch_cluster(op->ndof, mixed, ctx->aux_stream, n_large, d_order.p + n_small,
+                             d_off.p, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p,
+                             mixed ? op->vals32.p : nullptr, op->inv_diag.p, op->f.p, op->u.p,
+                             r.p, p.p, q.p, d_tol.p, d_maxit.p, d_it.p, d_res.p, d_status.p,
+                             mixed ? d_fp32.p : nullptr);
+        SVX_CUDA(cudaEventRecord(ctx->join_ev, ctx->aux_stream));
+    }
+    if (n_small > 0) launch(choice, d_maxit.p, n_small);
+    if (n_large > 0) SVX_CUDA(cudaStreamWaitEvent(pst, ctx->join_ev, 0));
+    SVX_CUDA(cudaEventRecord(ctx->ev[1], pst));
+    SVX_CUDA(cudaEventRecord(ctx->join_ev, pst));
+    SVX_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
     instance_diag_kernel<<<count, 256, 0, st>>>(op->ndof, d_off.p, P.diag_pos.p, op->vals.p,
                                                 d_hi.p, d_lo.p);
     SVX_LAUNCH_CHECK();
+    member_nnz_kernel<<<(count + 255) / 256, 256, 0, st>>>(count, d_off.p, P.node_base.p,
+                                                            d_cap.p);
+    SVX_LAUNCH_CHECK();
+    std::vector<int64_t> nnz(count);
+    SVX_CUDA(cudaMemcpyAsync(nnz.data(), d_cap.p, count * sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, st));
     it.resize(count);
     res.resize(count);
     status.resize(count);
     cond.resize(count);
     std::vector<double> hi(count), lo(count);
+    std::vector<int64_t> f32(mixed ? count : 0);
     SVX_CUDA(cudaMemcpyAsync(it.data(), d_it.p, count * sizeof(int64_t), cudaMemcpyDeviceToHost,
                              st));
     SVX_CUDA(cudaMemcpyAsync(res.data(), d_res.p, count * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1701,15 +2309,22 @@ void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& 
                              st));
     SVX_CUDA(cudaMemcpyAsync(lo.data(), d_lo.p, count * sizeof(double), cudaMemcpyDeviceToHost,
                              st));
+    if (mixed)
+        SVX_CUDA(cudaMemcpyAsync(f32.data(), d_fp32.p, count * sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st));
     SVX_CUDA(cudaStreamSynchronize(st));
     float ms = 0.f;
     SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     for (int k = 0; k < count; ++k) cond[k] = hi[k] / lo[k];
     op->has_solution = true;
     if (stats) {
+        stats->fp32_iterations = 0;
+        for (int64_t v : f32) stats->fp32_iterations += v;
         stats->ms_solve = ms;
         stats->threads_per_cta = cfg.bs;
         stats->lanes_per_node = cfg.g;
+        stats->cluster_members = n_large;
+        stats->member_nnz = std::move(nnz);
     }
 }
 

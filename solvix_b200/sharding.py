@@ -31,3 +31,27 @@ def shard_instances(n_dof, world: int):
         shards[r].append(k)
         heapq.heappush(heap, (load + float(work[k]), r))
     return [sorted(s) for s in shards]
+
+
+def solve_sharded(items, solve_fn, rank: int, world: int, n_dof=None):
+    """Solve ``items`` split over ``world`` ranks and return every result, in
+    item order, on every rank.
+
+    Each rank calls ``solve_fn`` on its own shard only (no data crosses
+    ranks before that); the per-item results are then exchanged once with
+    ``all_gather_object`` over the default process group.  ``n_dof`` gives
+    the per-item sizes used for the split (default: ``item.n_dof``).
+    """
+    sizes = [it.n_dof for it in items] if n_dof is None else list(n_dof)
+    mine = shard_instances(sizes, world)[rank]
+    local = solve_fn([items[k] for k in mine])
+    if world == 1:
+        return list(local)
+    import torch.distributed as dist
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (mine, list(local)))
+    out = [None] * len(items)
+    for idx, res in gathered:
+        for k, r in zip(idx, res):
+            out[k] = r
+    return out

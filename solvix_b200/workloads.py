@@ -172,9 +172,10 @@ def small_cantilever_c3d8(rng: np.random.Generator) -> FlatModel:
 
 
 def request_stream(count: int = 20000, rate_per_s: float = 100.0, seed: int = 5):
-    """[(arrival_s, FlatModel)] with Poisson arrivals."""
+    """[(arrival_s, FlatModel)] with Poisson arrivals.  The models do not
+    depend on the rate (the unit-rate gaps are drawn first and scaled)."""
     rng = _rng(seed)
-    t = np.cumsum(rng.exponential(1.0 / rate_per_s, size=count))
+    t = np.cumsum(rng.exponential(1.0, size=count)) / rate_per_s
     out = []
     for k in range(count):
         m = plate(rng) if rng.random() < 0.7 else small_cantilever_c3d8(rng)

@@ -66,3 +66,35 @@ def test_batch_budget_is_per_model(ctx):
     out, stats = ctx.solve_batch(flats, max_iter=5)
     assert stats["not_converged"] == 8
     assert all(o["iterations"] == 5 and not o["converged"] for o in out)
+
+
+def test_batch_large_members_run_on_clusters(ctx):
+    """Large members (3D >= 4096 rows, 2D >= 16384 rows) are solved by an
+    8-CTA cluster each, beside the CTA-per-member kernel; both classes meet
+    the plain bars and a large member is bitwise the same alone and in the
+    mix."""
+    rng = np.random.Generator(np.random.PCG64(44))
+    big = [workloads.plate(rng, nx=150, ny=60), workloads.plate(rng, nx=130, ny=70)]
+    small = small_plates(10, seed=45)
+    flats = [big[0]] + small[:5] + [big[1]] + small[5:]
+    assert sum(f.n_dof >= 16384 for f in flats) == 2
+    out, stats = ctx.solve_batch(flats)
+    assert stats["cluster_members"] == 2 and stats["not_converged"] == 0
+    for k, f in enumerate(flats):
+        single = ctx.solve_flat(f)
+        assert rel(out[k]["u"], single.u) <= 1e-10
+    alone, st1 = ctx.solve_batch([flats[6]])
+    assert st1["cluster_members"] == 1
+    assert np.array_equal(alone[0]["u"].view(np.int64), out[6]["u"].view(np.int64))
+    hexes = [workloads.cantilever_c3d8(40, 8, 8, lx=1.0, ly=0.2, lz=0.2, seed=46),
+             workloads.cantilever_c3d8(8, 2, 2, lx=0.4, ly=0.1, lz=0.1, seed=47)]
+    out3, st3 = ctx.solve_batch(hexes)
+    assert st3["cluster_members"] == 1
+    for k, f in enumerate(hexes):
+        assert rel(out3[k]["u"], ctx.solve_flat(f).u) <= 1e-10
+    from solvix_b200 import abi
+    mixed, stm = ctx.solve_batch(flats, precision=abi.SVX_MIXED)
+    assert stm["cluster_members"] == 2 and stm["fp32_iterations"] > 0
+    for k in range(len(flats)):
+        assert mixed[k]["converged"]
+        assert rel(mixed[k]["u"], out[k]["u"]) <= 1e-8
