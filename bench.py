@@ -48,7 +48,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default=None,
+                    help="plain and batched forms: fp64 (default); served form: mixed "
+                         "(default, as its workload specifies)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", choices=["plain", "batched", "precision", "served"],
                     default="plain",
@@ -330,7 +332,8 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == 0 else "f32/f64",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
         "config": {"workload": WORKLOAD_NAME, "n_dof": n, "nnz": nnz,
-                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "precision": args.precision or "fp64",
+                   "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (K 125 MB + Ke 189 MB per step vs 126 MB L2); "
                          "L2 flushed before the timed region"},
         "solves_per_s": world * args.steps / (ms_max / 1000.0),
@@ -529,8 +532,8 @@ def run_precision(args, rank, world, local_rank):
 
 SERVED_NAME = ("Poisson stream of solve requests: 70% 2D plates of the batched mix, 30% "
                "C3D8 cantilevers nx~U{20..120}, ny=nz~U{4..16}, E=70e9, nu=0.33, tip load "
-               "U(1e3,1e4) N (seed 5); mixed precision to relative residual 1e-10; 40 GiB "
-               "admission budget; 4 lanes")
+               "U(1e3,1e4) N (seed 5); relative residual 1e-10; 40 GiB admission budget; "
+               "4 lanes")
 
 
 def _serve_run(srv, reqs, rate_scale, base_t):
@@ -567,9 +570,10 @@ def _serve_run(srv, reqs, rate_scale, base_t):
 
 
 def run_served(args, rank, world, local_rank):
-    """C5: the request stream through svx_serve_* (continuous batching), at
-    saturation and at a sweep of Poisson rates; latency from submit to
-    result on the host."""
+    """C5: the request stream through svx_serve_* (continuous batching): all
+    requests at saturation, then a sweep of Poisson rates on a prefix of the
+    stream; latency from submit to result on the host.  The same
+    saturation run in the other precision is reported beside it."""
     import numpy as np
     import torch
 
@@ -577,16 +581,17 @@ def run_served(args, rank, world, local_rank):
     from solvix_b200.serve import Server
 
     torch.cuda.set_device(local_rank)
+    prec_name = args.precision or "mixed"
+    prec = abi.SVX_MIXED if prec_name == "mixed" else abi.SVX_FP64
+    other_name = "fp64" if prec_name == "mixed" else "mixed"
+    other = abi.SVX_FP64 if prec == abi.SVX_MIXED else abi.SVX_MIXED
     count = max(16, args.requests)
     stream = workloads.request_stream(count, 1.0, seed=5)  # unit-rate arrival times
     mine = list(range(rank, count, world))  # round-robin keeps each rank's arrivals Poisson
     reqs = [stream[k][1] for k in mine]
-    base_t = np.array([stream[k][0] for k in mine]) * world  # rank's own unit-rate clock
+    base_t = np.array([stream[k][0] for k in mine])  # arrivals at a total rate of 1/s
     n_dof = {k: f.n_dof for k, f in enumerate(reqs)}
-    srv = Server(local_rank, precision=abi.SVX_MIXED)
-    # warm-up: compile-free, but the first batches size the memory pool
-    warm = [reqs[k] for k in range(min(len(reqs), 256))]
-    _serve_run(srv, warm, 0.0, np.zeros(len(warm)))
+    sweep_n = min(len(reqs), max(200, len(reqs) // 10))
 
     def summarize(results, wall):
         lat = np.array([r["t_done_ms"] - r["t_submit_ms"] for r in results.values()])
@@ -596,46 +601,59 @@ def run_served(args, rank, world, local_rank):
                 "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
                 "p99_ms": float(np.percentile(lat, 99)), "failed": len(results) - len(ok),
                 "mean_batch": float(np.mean([r["batch_size"] for r in results.values()])),
-                "wall_s": wall}
+                "requests": len(results), "wall_s": wall}
+
+    def saturation(p):
+        srv = Server(local_rank, precision=p)
+        warm = reqs[:min(len(reqs), 512)]
+        _serve_run(srv, warm, 0.0, np.zeros(len(warm)))
+        s0 = srv.stats()
+        l0 = srv.lib.svx_launch_count()
+        res, wall = _serve_run(srv, reqs, 0.0, base_t)
+        row = summarize(res, wall)
+        row["rate_per_s"] = "all at t=0"
+        s1 = srv.stats()
+        row["phases_ms"] = {k: round(s1[k] - s0[k], 1) for k in (
+            "prep_ms", "assemble_ms", "solve_ms", "output_ms", "device_solve_ms", "pool_ms")}
+        row["batches"] = int(s1["batches"] - s0["batches"])
+        row["peak_bytes_admitted"] = int(s1["peak_bytes_admitted"])
+        return srv, row, srv.lib.svx_launch_count() - l0
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    launches0 = srv.lib.svx_launch_count()
-    sat_res, sat_wall = _serve_run(srv, reqs, 0.0, base_t)
-    sat = summarize(sat_res, sat_wall)
-    sat["rate_per_s"] = "all at t=0"
+    srv, sat, launches = saturation(prec)
     cap = sat["solves_per_s"] * world
     rates = ([float(x) for x in args.rates.split(",") if x] if args.rates
              else [round(cap * f, 1) for f in (0.25, 0.5, 0.8)])
     sweep = []
+    sub = reqs[:sweep_n]
     for rate in rates:
-        per_rank_rate = rate / world
-        res, wall = _serve_run(srv, reqs, 1.0 / per_rank_rate, base_t / world)
+        res, wall = _serve_run(srv, sub, 1.0 / rate, base_t[:sweep_n])
         row = summarize(res, wall)
         row["rate_per_s"] = rate
         sweep.append(row)
-    clk = clocks.stop()
-    launches = srv.lib.svx_launch_count() - launches0
-    stats = srv.stats()
     srv.close()
+    srv2, sat_other, _ = saturation(other)
+    srv2.close()
+    clk = clocks.stop()
     # error against FP64 and the one-at-a-time plain FP64 GPU path on a sample
     ctx = Context(local_rank)
     rng = np.random.default_rng(1)
     idx = [int(i) for i in rng.choice(len(reqs), min(48, len(reqs)), replace=False)]
-    with Server(local_rank, lanes=1, precision=abi.SVX_MIXED) as one:
+    with Server(local_rank, lanes=1, precision=prec) as one:
         for k in idx:
             one.submit(reqs[k], k)
-        mixed_u = {}
-        while len(mixed_u) < len(idx):
+        served_u = {}
+        while len(served_u) < len(idx):
             r = one.poll(200)
             if r is not None:
-                mixed_u[r["tag"]] = r["u"]
+                served_u[r["tag"]] = r["u"]
     ctx.solve_flat(reqs[idx[0]])
     t0 = time.perf_counter()
     errs = []
     for k in idx:
         ref = ctx.solve_flat(reqs[k])
-        errs.append(float(np.linalg.norm(mixed_u[k] - ref.u) / np.linalg.norm(ref.u)))
+        errs.append(float(np.linalg.norm(served_u[k] - ref.u) / np.linalg.norm(ref.u)))
     one_per = (time.perf_counter() - t0) / len(idx)
     ctx.close()
     rows = [sat] + sweep
@@ -648,6 +666,7 @@ def run_served(args, rank, world, local_rank):
                  "p95_ms": max(g[i]["p95_ms"] for g in gathered),
                  "p99_ms": max(g[i]["p99_ms"] for g in gathered),
                  "failed": sum(g[i]["failed"] for g in gathered),
+                 "requests": sum(g[i]["requests"] for g in gathered),
                  "mean_batch": float(np.mean([g[i]["mean_batch"] for g in gathered])),
                  "wall_s": max(g[i]["wall_s"] for g in gathered),
                  "rate_per_s": rows[i]["rate_per_s"]} for i in range(len(rows))]
@@ -656,22 +675,24 @@ def run_served(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "form": "served", "value": sat["dof_iter_per_s"], "unit": UNIT,
         "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1000 * sat["wall_s"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == abi.SVX_FP64 else "f64+f32",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
-        "config": {"workload": SERVED_NAME, "requests_per_point": count,
+        "config": {"workload": SERVED_NAME, "precision": prec_name, "requests": count,
+                   "sweep_requests_per_rate": sweep_n,
                    "parallelism": f"requests round-robin over {world} GPU(s), no collective"},
         "solves_per_s": sat["solves_per_s"],
         "latency_ms": {"p50": head["p50_ms"], "p95": head["p95_ms"], "p99": head["p99_ms"],
                        "at_rate_per_s": head["rate_per_s"]},
         "sweep": rows,
+        f"saturation_{other_name}": sat_other,
         "rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
                             "sample": len(errs)},
         "one_at_a_time": {"solves_per_s": 1.0 / one_per,
                           "sample": f"{len(idx)} requests through svx_solve_flat (FP64) one "
                                     "after another, wall clock",
-                          "speedup_served": sat["solves_per_s"] * one_per},
-        "server": {k: stats[k] for k in ("batches", "peak_bytes_admitted",
-                                         "peak_device_bytes")},
+                          "speedup_served": sat["solves_per_s"] * one_per,
+                          f"speedup_served_{other_name}": sat_other["solves_per_s"] * one_per},
         "e2e": {"value": sat["dof_iter_per_s"], "unit": UNIT,
                 "note": "submit of host models to results on the host, wall clock",
                 "h2d_bytes_per_step": int(sum(f.nbytes() for f in reqs)),

@@ -326,9 +326,11 @@ int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* model
  * per-model convergence) and publishes each result as its batch completes.
  * Batches of different lanes run concurrently on the device.  A request is
  * admitted only while the estimated device bytes of all admitted, unfinished
- * requests stay within hbm_budget_bytes.  The lanes share one device memory
- * pool whose arena, the whole budget, is reserved at creation, so batches
- * of any size make no cudaMalloc / cudaFree calls in steady state. */
+ * requests stay within hbm_budget_bytes.  Each lane has its own device
+ * memory pool (blocks are reused only on the stream that freed them) whose
+ * arena, budget / lanes, is reserved at creation, so batches of any size
+ * make no cudaMalloc / cudaFree calls in steady state; a lane's batch stays
+ * within its arena. */
 typedef struct svx_server svx_server_t;
 
 typedef struct svx_serve_opts {
@@ -366,9 +368,9 @@ typedef struct svx_serve_stats {
     int64_t in_flight;         /* admitted, not yet published */
     int64_t bytes_admitted;    /* estimated device bytes of in-flight work */
     int64_t peak_bytes_admitted;
-    int64_t device_bytes;      /* device memory the lanes' pool holds: its
-                                  arena (the budget, reserved at creation) or,
-                                  if more, the blocks in use + cached */
+    int64_t device_bytes;      /* device memory the lanes' pools hold: their
+                                  arenas (budget / lanes each) or, if more,
+                                  the blocks in use + cached */
     int64_t peak_device_bytes;
     /* summed over batches, ms of host wall clock per phase: member checks
      * and concatenation, upload + assembly, batched PCG, result copies;

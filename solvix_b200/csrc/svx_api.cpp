@@ -807,7 +807,7 @@ int svx_ctx_destroy(svx_ctx_t* ctx) {
     if (!ctx) return SVX_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->owns_pool) delete ctx->pool;
+    delete ctx->pool;
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);

@@ -169,7 +169,6 @@ struct svx_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     svx::DevicePool* pool = nullptr;
     svx::PinnedBuffer staging;  // batched host<->device staging
-    bool owns_pool = true;  // false for a server lane (pool shared by the lanes)
     std::string last_error;
     cudaEvent_t ev[8] = {};
 };

@@ -8,11 +8,15 @@
 // requests are queued as they arrive and solved in batches while later ones
 // keep arriving (continuous batching).
 //
-// Design.  `lanes` dispatcher threads each own a CUDA stream (a context
-// whose memory pool is shared by all lanes).  A free lane takes every
-// waiting request, in arrival order, that has the ndof of the oldest one,
-// until max_batch or until the next one's estimated device bytes do not fit
-// what is left of the admission budget; it then solves them as one
+// Design.  `lanes` dispatcher threads each own a context (CUDA streams and
+// a device memory pool of their own: a block a lane frees may still be read
+// by that lane's queued kernels, so it is reused only on that lane's
+// streams).  Each lane's pool reserves budget / lanes as its arena.  A free
+// lane takes every waiting request, in arrival order, that has the ndof of
+// the oldest one, until max_batch, until its batch would exceed half its
+// arena,
+// or until the next one's estimated device bytes do not fit what is left of
+// the admission budget; it then solves them as one
 // block-diagonal batch (run_batch: per-model checks, per-model convergence,
 // a failed member isolated from the others) and publishes one result per
 // request.  While one lane's batch runs, other lanes start the requests
@@ -96,7 +100,6 @@ int element_nodes(int kind) {
 struct svx_server {
     svx_serve_opts_t opts{};
     int device = 0;
-    DevicePool* pool = nullptr;
     std::vector<svx_ctx*> lane_ctx;
     std::vector<std::thread> lanes;
     std::mutex mu;
@@ -156,6 +159,11 @@ void fill_result_error(svx_serve_result_t& r, int code, int reason, int64_t elem
 
 void svx_server::lane_loop(int lane) {
     svx_ctx* ctx = lane_ctx[lane];
+    DevicePool* pool = ctx->pool;
+    // a batch takes at most half of the lane's arena: the rest absorbs the
+    // fragmentation of blocks with different lifetimes, so batches are
+    // carved from the arena instead of falling back to cudaMalloc
+    const int64_t lane_cap = std::max<int64_t>(1, opts.hbm_budget_bytes / opts.lanes / 2);
     cudaSetDevice(device);
     for (;;) {
         std::vector<Request> batch;
@@ -178,6 +186,7 @@ void svx_server::lane_loop(int lane) {
                 // the oldest request always fits here (see the wait above)
                 if (bytes_admitted + it->bytes > opts.hbm_budget_bytes && bytes_admitted > 0)
                     break;
+                if (!batch.empty() && batch_bytes + it->bytes > lane_cap) break;
                 bytes_admitted += it->bytes;
                 batch_bytes += it->bytes;
                 batch.push_back(std::move(*it));
@@ -254,11 +263,14 @@ void svx_server::lane_loop(int lane) {
         }
         batch.clear();  // the model copies go before the budget is returned
         // blocks beyond the arena (admission estimates are upper bounds, so
-        // rarely) go back to the driver once the footprint exceeds the budget
-        const int64_t dev = int64_t(std::max(pool->arena_bytes(),
-                                             pool->bytes_in_use() + pool->bytes_cached()));
-        if (int64_t(pool->bytes_in_use() + pool->bytes_cached()) > opts.hbm_budget_bytes)
+        // rarely) go back to the driver once the lane exceeds its share
+        if (int64_t(pool->bytes_in_use() + pool->bytes_cached()) >
+            opts.hbm_budget_bytes / opts.lanes)
             pool->trim();
+        int64_t dev = 0;
+        for (svx_ctx* c : lane_ctx)
+            dev += int64_t(std::max(c->pool->arena_bytes(),
+                                    c->pool->bytes_in_use() + c->pool->bytes_cached()));
         {
             std::lock_guard<std::mutex> lk(mu);
             peak_device_bytes = std::max(peak_device_bytes, dev);
@@ -308,7 +320,6 @@ int svx_serve_create(int device, const svx_serve_opts_t* opts, svx_server_t** ou
     }
     if (srv->opts.lanes > 64) srv->opts.lanes = 64;
     srv->device = device;
-    srv->pool = new DevicePool(device);
     for (int l = 0; l < srv->opts.lanes; ++l) {
         svx_ctx_t* c = nullptr;
         const int st = svx_ctx_create(device, &c);
@@ -320,19 +331,16 @@ int svx_serve_create(int device, const svx_serve_opts_t* opts, svx_server_t** ou
                 svx_last_error(nullptr, err->message, sizeof(err->message));
             }
             for (svx_ctx* x : srv->lane_ctx) svx_ctx_destroy(x);
-            delete srv->pool;
             return st;
         }
-        delete c->pool;  // lanes share the server's pool
-        c->pool = srv->pool;
-        c->owns_pool = false;
         srv->lane_ctx.push_back(c);
     }
-    // the whole admission budget is reserved up front as the lanes' arena:
+    // the admission budget is reserved up front as the lanes' arenas:
     // steady-state batches make no cudaMalloc / cudaFree calls
     try {
         cudaSetDevice(device);
-        srv->pool->reserve(size_t(srv->opts.hbm_budget_bytes));
+        for (svx_ctx* c : srv->lane_ctx)
+            c->pool->reserve(size_t(srv->opts.hbm_budget_bytes / srv->opts.lanes));
     } catch (const ModelFail& f) {
         if (err) {
             err->code = f.code;
@@ -341,7 +349,6 @@ int svx_serve_create(int device, const svx_serve_opts_t* opts, svx_server_t** ou
             std::snprintf(err->message, sizeof(err->message), "%s", f.message.c_str());
         }
         for (svx_ctx* x : srv->lane_ctx) svx_ctx_destroy(x);
-        delete srv->pool;
         return f.code;
     }
     svx_server* s = srv.get();
@@ -437,16 +444,21 @@ int svx_serve_stats(svx_server_t* srv, svx_serve_stats_t* st) {
     st->in_flight = srv->in_flight;
     st->bytes_admitted = srv->bytes_admitted;
     st->peak_bytes_admitted = srv->peak_bytes_admitted;
-    st->device_bytes = int64_t(std::max(srv->pool->arena_bytes(),
-                                        srv->pool->bytes_in_use() + srv->pool->bytes_cached()));
+    st->device_bytes = 0;
+    st->pool_ms = 0.0;
+    st->pool_mallocs = 0;
+    for (svx_ctx* c : srv->lane_ctx) {
+        st->device_bytes += int64_t(std::max(c->pool->arena_bytes(),
+                                             c->pool->bytes_in_use() + c->pool->bytes_cached()));
+        st->pool_ms += c->pool->malloc_ms();
+        st->pool_mallocs += c->pool->mallocs();
+    }
     st->peak_device_bytes = std::max(srv->peak_device_bytes, st->device_bytes);
     st->prep_ms = srv->prep_ms;
     st->assemble_ms = srv->assemble_ms;
     st->solve_ms = srv->solve_ms;
     st->output_ms = srv->output_ms;
     st->device_solve_ms = srv->device_solve_ms;
-    st->pool_ms = srv->pool->malloc_ms();
-    st->pool_mallocs = srv->pool->mallocs();
     return SVX_OK;
 }
 
@@ -462,7 +474,6 @@ int svx_serve_destroy(svx_server_t* srv) {
     for (auto& t : srv->lanes) t.join();
     for (svx_serve_result_t* b : srv->done) svx_serve_result_free(b);
     for (svx_ctx* c : srv->lane_ctx) svx_ctx_destroy(c);
-    delete srv->pool;
     delete srv;
     return SVX_OK;
 }
