@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "PCG DOF-iters/s & solves/s: mixed/batched vs FP64 at 1e-8 err; p50/p99 ms"
 UNIT = "DOF*iter/s"
 HBM_FALLBACK_GBS = 6650.0
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_dot_fp64_c3d8_160x16x16.txt")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "pcg_persistent_fp64_c3d8_160x16x16.txt")
 
 
 def parse_args():
@@ -86,12 +86,12 @@ def measured_peaks():
 
 
 def ncu_traffic():
-    """DRAM bytes per spmv_dot launch from the committed ncu summary."""
+    """DRAM bytes per iteration of the persistent PCG kernel (ncu summary)."""
     try:
         with open(TRAFFIC_FILE) as fh:
             for line in fh:
-                if line.startswith("dram_bytes_per_launch:"):
-                    return int(float(line.split(":", 1)[1].strip()))
+                if line.startswith("dram_bytes_per_iteration:"):
+                    return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None
@@ -264,12 +264,24 @@ def run_ours(args, rank, world, local_rank):
     dof_iters = float(np.sum(iters)) * n
     value = world * dof_iters / (ms_max / 1000.0)
 
-    # roofline of the SpMV: algorithmic bytes / live CUDA-event duration
-    kms = op.time_kernels(reps=50)
-    spmv_bytes = nnz * (8 + 4) + 4 * (n + 1) + 2 * 8 * n
-    achieved = spmv_bytes / (kms[0] / 1000.0) / 1e9
+    # roofline of the dominant kernel, the persistent PCG kernel: its
+    # algorithmic bytes per launch (CHUNK iterations) over its average
+    # launch duration, from the PCG device time of the timed steps
+    from solvix_b200.kernel_timer import pcg_iteration_bytes, spmv_node_bytes
+    # iterations per persistent launch (persistent_chunk in svx_pcg.cu)
+    chunk = 64 if nnz > 100_000_000 else (256 if nnz > 10_000_000 else 1024)
+    it_total = float(np.sum(iters))
+    launches_pcg = float(sum(-(-i // chunk) for i in iters))
+    iter_bytes = pcg_iteration_bytes(n, nnz, flat.ndof, flat.n_nodes)
+    launch_ms = ms_parts[1] / launches_pcg
+    launch_bytes = iter_bytes * it_total / launches_pcg
+    achieved = launch_bytes / (launch_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic()
+    traffic_it = ncu_traffic()
+    traffic = traffic_it * it_total / launches_pcg if traffic_it else None
+    # the node-block SpMV alone (spmv_node_dot), back-to-back launches
+    kms = op.time_kernels(reps=50)
+    spmv_bytes = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
 
     # e2e: the public C ABI call from pinned host memory
     keep = []
@@ -344,12 +356,21 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                 "solves_per_s": world * e2e_steps / (float(e_ms.item()) / 1000.0)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "spmv_dot (FP64 CSR SpMV + p.Kp)",
+        "roofline": {"bound": "hbm", "kernel": "pcg_persistent_kernel<3,16,double> "
+                                                 f"(FP64, {chunk} PCG iterations a launch)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": int(spmv_bytes),
-                     "launch_ms": float(kms[0]),
+                     "algorithmic_bytes_per_launch": int(launch_bytes),
+                     "algorithmic_bytes_per_iteration": int(iter_bytes),
+                     "launch_ms": float(launch_ms),
                      "traffic": traffic,
+                     "note": "K (87.7 MB in FP64 node blocks) fits the 126 MB L2; traffic "
+                             "(ncu DRAM bytes) below the algorithmic bytes is K served from "
+                             "L2 across iterations",
+                     "spmv_node_dot_alone": {
+                         "launch_ms": float(kms[0]), "bytes": int(spmv_bytes),
+                         "gbs": spmv_bytes / (kms[0] / 1000.0) / 1e9,
+                         "frac": spmv_bytes / (kms[0] / 1000.0) / 1e9 / peak},
                      "other_kernels_ms": {"update": float(kms[1]), "p_update": float(kms[2])}},
         "clocks": clk,
     }
@@ -364,7 +385,7 @@ def run_ours(args, rank, world, local_rank):
 
 BATCH_NAME = ("4,096 independent 2D plates (nx~U{10..160}, ny~U{4..40}, h=1, CPS4 or CPS3 "
               "p=0.5, E=10^U(9,log10 3e11), nu~U(0.15,0.45), t~U(0.001,0.05), left edge "
-              "clamped, one CLOAD U(100,1e4) N at a random right-edge node; seed 4), FP64 "
+              "clamped, one CLOAD U(100,1e4) N at a random right-edge node; seed 4), "
               "Jacobi-PCG to 1e-10 per model, centroid von Mises")
 
 
@@ -374,7 +395,8 @@ def run_batched(args, rank, world, local_rank):
     import numpy as np
     import torch
 
-    from solvix_b200 import Context, workloads
+    from solvix_b200 import Context, abi, workloads
+    from solvix_b200.kernel_timer import pcg_iteration_bytes
     from solvix_b200.sharding import shard_instances
 
     torch.cuda.set_device(local_rank)
@@ -383,8 +405,9 @@ def run_batched(args, rank, world, local_rank):
     sub = [flats[k] for k in mine]
     ctx = Context(local_rank)
     lib = ctx.lib
+    prec = abi.SVX_MIXED if args.precision == "mixed" else abi.SVX_FP64
     for _ in range(max(args.warmup, 0)):
-        ctx.solve_batch(sub)
+        ctx.solve_batch(sub, precision=prec)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -394,15 +417,15 @@ def run_batched(args, rank, world, local_rank):
     dev_ms, wall_s, dof_it, bytes_alg = [], [], 0.0, 0.0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        out, st = ctx.solve_batch(sub)
+        out, st = ctx.solve_batch(sub, precision=prec)
         wall_s.append(time.perf_counter() - t0)
         dev_ms.append(st["ms_assemble"] + st["ms_solve"] + st["ms_stress"])
         solve_ms = st["ms_solve"]
         dof_it = float(sum(f.n_dof * o["iterations"] for f, o in zip(sub, out)))
-        # node-block SpMV (8 B value + 4 B per 2x2 / 3x3 block index) and the
-        # 13 FP64 vector streams, per iteration of each model
-        nd = sub[0].ndof
-        bytes_alg = float(sum(o["iterations"] * (o["nnz"] * (8 + 4 / (nd * nd)) + 104 * f.n_dof)
+        # per iteration of each model: the node-block SpMV and the vector
+        # streams of the update (pcg_iteration_bytes)
+        bytes_alg = float(sum(o["iterations"] * pcg_iteration_bytes(f.n_dof, o["nnz"], f.ndof,
+                                                                    f.n_nodes)
                               for f, o in zip(sub, out)))
     launches = lib.svx_launch_count() - launches0
     clk = clocks.stop()
@@ -423,9 +446,11 @@ def run_batched(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "form": "batched", "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if prec == abi.SVX_FP64 else "f64+f32",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
         "config": {"workload": BATCH_NAME, "models": len(flats),
+                   "precision": args.precision or "fp64",
                    "total_dof": int(sum(f.n_dof for f in flats)),
                    "parallelism": f"instances sharded over {world} GPU(s), no collective",
                    "autotuned": {"threads_per_cta": st["threads_per_cta"],
@@ -435,13 +460,16 @@ def run_batched(args, rank, world, local_rank):
                        "max": int(iters.max())},
         "ms_breakdown": {"assemble": st["ms_assemble"], "pcg": st["ms_solve"],
                          "stress": st["ms_stress"]},
+        "cluster_members": st["cluster_members"], "fp32_iterations": st["fp32_iterations"],
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "solves_per_s": len(flats) * args.steps / wall_max,
                 "h2d_bytes_per_step": int(sum(f.nbytes() for f in sub)),
                 "d2h_bytes_per_step": int(sum(8 * (f.n_dof + f.n_elem) for f in sub)),
                 "note": "svx_batch_solve from pageable host arrays, wall clock per call"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel (one launch per step)",
+        "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel (one CTA per member) beside "
+                                                 "batch_pcg_cluster_kernel (one 8-CTA cluster "
+                                                 "per large member), one launch each per step",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": int(bytes_alg),
@@ -496,13 +524,15 @@ def run_precision(args, rank, world, local_rank):
             times.append(time.perf_counter() - t0)
             its.append(it)
         res[name] = {"u": u, "iterations": its[-1], "s_per_solve": float(np.mean(times)),
-                     "residual": r}
+                     "residual": r, "fp32_iterations": op.last_fp32_iterations}
     kms = op.time_kernels(reps=10)
     err = float(np.linalg.norm(res["mixed"]["u"] - res["fp64"]["u"]) /
                 np.linalg.norm(res["fp64"]["u"]))
     peak, peak_kind = measured_peaks()
     nnz = op.nnz
-    spmv_bytes = nnz * (8 + 4 / 9) + 16 * (flat.n_nodes + 1) + 16 * n
+    from solvix_b200.kernel_timer import spmv_node_bytes
+    spmv_bytes = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
+    fp32_bytes = spmv_bytes - 4 * nnz
     f64 = res["fp64"]
     line = {
         "metric": METRIC, "form": "precision", "value": n * f64["iterations"] / f64["s_per_solve"],
@@ -514,6 +544,9 @@ def run_precision(args, rank, world, local_rank):
         "fp64": {"iterations": f64["iterations"], "s_per_solve": f64["s_per_solve"],
                  "solves_per_s": 1 / f64["s_per_solve"], "residual": f64["residual"]},
         "mixed": {"iterations": res["mixed"]["iterations"],
+                  "fp32_iterations": res["mixed"]["fp32_iterations"],
+                  "fp32_spmv_ms": float(kms[3]),
+                  "fp32_spmv_gbs": fp32_bytes / (kms[3] / 1000) / 1e9,
                   "s_per_solve": res["mixed"]["s_per_solve"],
                   "solves_per_s": 1 / res["mixed"]["s_per_solve"],
                   "residual_fp64_true": res["mixed"]["residual"],

@@ -191,6 +191,7 @@ typedef struct svx_solution {
     double ms_assemble;        /* device time of element integration + assembly */
     double ms_solve;           /* device time of the PCG */
     double ms_stress;          /* device time of stress + reaction recovery */
+    int64_t fp32_iterations;   /* mixed: iterations on the FP32 operator */
 } svx_solution_t;
 
 typedef struct svx_ctx svx_ctx_t;
@@ -407,10 +408,11 @@ int svx_serve_destroy(svx_server_t* srv);
 /* Kernels this process has launched through the library (graph nodes count
  * when their graph is launched). */
 int64_t svx_launch_count(void);
-/* Average device time in ms of the three FP64 PCG iteration kernels of an
- * operator (ms3[0] = SpMV + p.Kp, ms3[1] = u/r update + dots, ms3[2] = p
- * update), each over `reps` back-to-back launches on the context stream. */
-int svx_op_time_kernels(svx_op_t* op, int reps, double* ms3);
+/* Average device time in ms of the PCG iteration kernels of an operator,
+ * each over `reps` back-to-back launches on the context stream: ms4[0] =
+ * FP64 node-block SpMV + p.Kp, ms4[1] = u/r update + dots, ms4[2] = p
+ * update, ms4[3] = the difference-form FP32 SpMV of the mixed form. */
+int svx_op_time_kernels(svx_op_t* op, int reps, double* ms4);
 
 /* ---- PCG without device allocation ---------------------------------- */
 /* Largest system (rows) svx_pcg_solve_noalloc accepts. */

@@ -137,6 +137,7 @@ class SvxSolution(C.Structure):
         ("ms_assemble", C.c_double),
         ("ms_solve", C.c_double),
         ("ms_stress", C.c_double),
+        ("fp32_iterations", C.c_int64),
     ]
 
 

@@ -266,8 +266,9 @@ class Operator:
             _raise(st, None, "svx_op_set_solution failed")
 
     def time_kernels(self, reps: int = 50):
-        """(spmv_dot, update, p_update) average device ms per launch."""
-        ms = np.zeros(3)
+        """(FP64 spmv_node_dot, update, p_update, FP32 difference-form
+        spmv_node_dot) average device ms per launch."""
+        ms = np.zeros(4)
         st = self.lib.svx_op_time_kernels(self.handle, int(reps), abi.ptr(ms, C.c_double))
         if st != abi.SVX_OK:
             _raise(st, None, "svx_op_time_kernels failed")
@@ -293,6 +294,7 @@ class Operator:
         st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
         if st != abi.SVX_OK:
             _raise(st, err)
+        self.last_fp32_iterations = int(sol.fp32_iterations)
         return int(sol.iterations), float(sol.final_residual), float(sol.ms_solve), \
             float(sol.ms_stress), float(sol.ms_assemble)
 
@@ -307,6 +309,7 @@ class Operator:
         st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
         if st != abi.SVX_OK:
             _raise(st, err)
+        self.last_fp32_iterations = int(sol.fp32_iterations)
         return u, int(sol.iterations), float(sol.final_residual), float(sol.cond_estimate)
 
     def stress(self):

@@ -484,6 +484,7 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
     if (sol) {
         sol->iterations = r.iterations;
         sol->outer_iterations = outer;
+        sol->fp32_iterations = opts.precision == SVX_MIXED ? op->mixed_sloppy_iters : 0;
         sol->final_residual = r.residual;
         sol->cond_estimate = op->cond_estimate;
         sol->ms_assemble = op->ms_assemble;
@@ -844,12 +845,12 @@ void* svx_ctx_stream(svx_ctx_t* ctx) { return ctx ? (void*)ctx->stream : nullptr
 
 int64_t svx_launch_count(void) { return int64_t(g_launches.load()); }
 
-int svx_op_time_kernels(svx_op_t* op, int reps, double* ms3) {
-    if (!op || !ms3 || reps <= 0) return SVX_BAD_ARGUMENT;
+int svx_op_time_kernels(svx_op_t* op, int reps, double* ms4) {
+    if (!op || !ms4 || reps <= 0) return SVX_BAD_ARGUMENT;
     svx_ctx* ctx = op->ctx;
     return guarded(ctx, nullptr, [&]() -> int {
         SVX_CUDA(cudaSetDevice(ctx->device));
-        time_iteration_kernels(ctx, op, reps, ms3);
+        time_iteration_kernels(ctx, op, reps, ms4);
         return SVX_OK;
     });
 }

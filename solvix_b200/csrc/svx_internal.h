@@ -311,7 +311,7 @@ void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double*
 int choose_spmv_group(const svx_op* op);
 // Average device time (ms) of the three FP64 PCG iteration kernels
 // (spmv_dot, update, p_update) over `reps` back-to-back launches each.
-void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3);
+void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms4);
 
 // Batched PCG over a block-diagonal concatenation of independent models
 // (svx_pcg.cu).  node_off[count + 1] delimits each instance's nodes.

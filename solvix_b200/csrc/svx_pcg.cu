@@ -168,15 +168,17 @@ spmv_dot_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
 //                                * x[adj[k]*ND + db]
 // G lanes own one node and split its d blocks; lane k loads one index, ND
 // x values and ND*ND matrix values, all independent of each other.
-template <int ND, int G, class V>
+// M = float is the difference-form FP32 operator (compensated_fp32_kernel):
+// every neighbour but the node itself multiplies x_j - x_i.
+template <int ND, int G, class M, class V>
 __device__ __forceinline__ void node_rows(const int64_t* __restrict__ adj_ptr,
                                           const int32_t* __restrict__ adj,
                                           const int64_t* __restrict__ node_base,
-                                          const V* __restrict__ vals, const V* __restrict__ x,
+                                          const M* __restrict__ vals, const V* __restrict__ x,
                                           int64_t i, int gl, double* acc) {
     const int64_t a0 = adj_ptr[i];
     const int d = int(adj_ptr[i + 1] - a0);
-    const V* __restrict__ v = vals + node_base[i];
+    const M* __restrict__ v = vals + node_base[i];
     if (d == 0) {  // an unreferenced node: rows of length 1 (the diagonal)
         if (gl == 0)
 #pragma unroll
@@ -184,11 +186,23 @@ __device__ __forceinline__ void node_rows(const int64_t* __restrict__ adj_ptr,
         return;
     }
     const int rowlen = ND * d;
+    constexpr bool DIFF = std::is_same<M, float>::value;
+    double xi[ND];
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xi[db] = double(x[i * ND + db]);
+    }
     for (int k = gl; k < d; k += G) {
-        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        const int32_t j = __ldg(adj + a0 + k);
+        const int64_t c = int64_t(j) * ND;
         double xv[ND];
 #pragma unroll
         for (int db = 0; db < ND; ++db) xv[db] = double(x[c + db]);
+        if constexpr (DIFF) {
+            if (j != int32_t(i))
+#pragma unroll
+                for (int db = 0; db < ND; ++db) xv[db] -= xi[db];
+        }
 #pragma unroll
         for (int da = 0; da < ND; ++da)
 #pragma unroll
@@ -206,11 +220,11 @@ __device__ __forceinline__ double group_sum(double v) {
 
 // q = K p (node blocks) and the per-block partial of p.q; the last block
 // forms pap and alpha exactly like spmv_dot_kernel.
-template <int ND, int G, class V>
+template <int ND, int G, class M, class V>
 __global__ void __launch_bounds__(BLOCK, NODE_BLOCKS_PER_SM)
 spmv_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                      const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
-                     const V* __restrict__ vals, const V* __restrict__ p, V* __restrict__ q,
+                     const M* __restrict__ vals, const V* __restrict__ p, V* __restrict__ q,
                      double* __restrict__ partials, PcgScalars* __restrict__ s) {
     __shared__ double sh[32];
     if (s->status != PCG_RUNNING) return;
@@ -223,7 +237,7 @@ spmv_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         double acc[ND];
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = 0.0;
-        if (i < n_nodes) node_rows<ND, G, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
+        if (i < n_nodes) node_rows<ND, G, M, V>(adj_ptr, adj, node_base, vals, p, i, gl, acc);
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
         if (i < n_nodes && gl == 0) {
@@ -268,7 +282,8 @@ spmv_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         double acc[ND];
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = 0.0;
-        if (i < n_nodes) node_rows<ND, G, double>(adj_ptr, adj, node_base, vals, x, i, gl, acc);
+        if (i < n_nodes)
+            node_rows<ND, G, double, double>(adj_ptr, adj, node_base, vals, x, i, gl, acc);
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
         if (i < n_nodes && gl == 0)
@@ -296,7 +311,8 @@ residual_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         double acc[ND];
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = 0.0;
-        if (i < n_nodes) node_rows<ND, G, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
+        if (i < n_nodes)
+            node_rows<ND, G, double, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
         if (i < n_nodes && gl == 0)
@@ -363,6 +379,8 @@ update_kernel(int64_t n, U* __restrict__ u, V* __restrict__ r, const V* __restri
                 s->status = PCG_CONVERGED;
             } else if (s->it >= s->max_iter) {
                 s->status = PCG_MAXITER;
+            } else if (trr <= s->rr_stop) {
+                s->status = PCG_RELIABLE;  // s->rz stays r.z of the previous iterate
             } else {
                 s->beta = trz / s->rz;
                 s->rz = trz;
@@ -1390,12 +1408,12 @@ unsigned grid_nodes(const svx_ctx* ctx, int64_t n_nodes, int G) {
         }                                                               \
     } while (0)
 
-template <class V>
+template <class M, class V>
 void launch_spmv_node_dot(const svx_op* op, int G, unsigned grid, cudaStream_t st,
-                          const V* vals, const V* p, V* q, double* partials, PcgScalars* s) {
+                          const M* vals, const V* p, V* q, double* partials, PcgScalars* s) {
     const Pattern& P = op->pat;
     SVX_NODE_DISPATCH(op->ndof, G,
-                      (spmv_node_dot_kernel<ND, GG, V><<<grid, BLOCK, 0, st>>>(
+                      (spmv_node_dot_kernel<ND, GG, M, V><<<grid, BLOCK, 0, st>>>(
                           op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, vals, p, q,
                           partials, s)));
 }
@@ -1417,14 +1435,9 @@ struct PcgRun {
     PcgScalars* h_s;  // pinned
 
     void enqueue_iteration(cudaStream_t st) {
-        if constexpr (std::is_same<M, V>::value) {
-            launch_spmv_node_dot<V>(op, G, grid_r, st, vals, p, q, partials, s);
-            update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
-            p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
-        } else {
-            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
-                            "mixed precision needs cooperative launch (persistent PCG)"};
-        }
+        launch_spmv_node_dot<M, V>(op, G, grid_r, st, vals, p, q, partials, s);
+        update_kernel<V, U><<<grid_v, BLOCK, 0, st>>>(n, u, r, p, q, inv_diag, partials, s);
+        p_update_kernel<V><<<grid_v, BLOCK, 0, st>>>(n, p, r, inv_diag, s);
     }
 
     // Persistent form: cooperative launches of up to `chunk` iterations each
@@ -1537,6 +1550,15 @@ struct PinnedScalars {
 
 // Iterations per persistent launch: a few to tens of milliseconds of work,
 // so the host sees progress and a long solve is not one unbounded launch.
+// Systems above GRAPH_MIN_NNZ iterate with the three standalone kernels in a
+// CUDA graph instead of the persistent kernel: there an iteration streams
+// more than 400 MB, so launch gaps are noise, and the standalone node SpMV
+// (5 blocks of 256 threads per SM, more loads in flight) runs at ~80% of
+// the HBM copy peak where the persistent kernel's SpMV phase (2 blocks of
+// 512) reaches ~55%.  Below it, K stays in L2 and the persistent kernel's
+// absence of launch gaps wins.
+constexpr int64_t GRAPH_MIN_NNZ = 50000000;
+
 int persistent_chunk(int64_t nnz) {
     if (nnz > 100000000) return 64;
     if (nnz > 10000000) return 256;
@@ -1572,7 +1594,7 @@ void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
 
 std::atomic<long long> g_launches{0};
 
-void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
+void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms4) {
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
     DBuf<double> u, r, p, q, partials;
@@ -1606,15 +1628,21 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms3) {
         g_launches.fetch_add(reps + 1, std::memory_order_relaxed);
         return double(ms) / reps;
     };
-    ms3[0] = timed([&] {
-        launch_spmv_node_dot<double>(op, G, grid_r, st, op->vals.p, p.p, q.p, partials.p, s.p);
+    ms4[0] = timed([&] {
+        launch_spmv_node_dot<double, double>(op, G, grid_r, st, op->vals.p, p.p, q.p, partials.p,
+                                             s.p);
     });
-    ms3[1] = timed([&] {
+    ms4[1] = timed([&] {
         update_kernel<double, double><<<grid_v, BLOCK, 0, st>>>(n, u.p, r.p, p.p, q.p,
                                                                 op->inv_diag.p, partials.p, s.p);
     });
-    ms3[2] = timed([&] {
+    ms4[2] = timed([&] {
         p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p.p, r.p, op->inv_diag.p, s.p);
+    });
+    build_fp32_operator(ctx, op);
+    ms4[3] = timed([&] {
+        launch_spmv_node_dot<float, double>(op, G, grid_r, st, op->vals32.p, p.p, q.p,
+                                            partials.p, s.p);
     });
     SVX_CUDA(cudaGetLastError());
 }
@@ -1680,7 +1708,8 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     SVX_CUDA(cudaStreamSynchronize(st));
     int status = hs.h->status;
     if (status == PCG_RUNNING) {
-        status = run.iterate_persistent(persistent_chunk(op->pat.nnz));
+        status = (op->pat.nnz > GRAPH_MIN_NNZ) ? -1
+                                               : run.iterate_persistent(persistent_chunk(op->pat.nnz));
         if (status < 0) status = run.iterate(check_every);
     }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
@@ -1735,7 +1764,8 @@ reliable_resume_kernel(int64_t n, const double* __restrict__ r64, V* __restrict_
 // 4.44 B instead of 8.44 B per nonzero.
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps) {
-    (void)check_every;
+    if (check_every <= 0) check_every = auto_check_every(op->n, op->pat.nnz);
+    const bool graph = op->pat.nnz > GRAPH_MIN_NNZ;
     const double delta = (inner_tol > 0.01 && inner_tol < 1.0) ? inner_tol : 0.1;
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
@@ -1820,14 +1850,13 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     const int chunk = persistent_chunk(op->pat.nnz);
     while (status == PCG_RUNNING) {
         if (fp64_phase) {
-            status = exact.iterate_persistent(chunk);
+            status = graph ? -1 : exact.iterate_persistent(chunk);
+            if (status < 0) status = exact.iterate(check_every);
             res = hs.h->res;
             break;
         }
-        status = sloppy.iterate_persistent(chunk);
-        if (status < 0)
-            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
-                            "mixed precision needs cooperative launch (persistent PCG)"};
+        status = graph ? -1 : sloppy.iterate_persistent(chunk);
+        if (status < 0) status = sloppy.iterate(check_every);
         sloppy_iters = hs.h->it;
         if (status == PCG_BREAKDOWN) break;
         // segment ended (reduced by delta, capped, or sloppy-converged):

@@ -14,9 +14,8 @@
 // streams).  Each lane's pool reserves budget / lanes as its arena.  A free
 // lane takes every waiting request, in arrival order, that has the ndof of
 // the oldest one, until max_batch, until its batch would exceed half its
-// arena,
-// or until the next one's estimated device bytes do not fit what is left of
-// the admission budget; it then solves them as one
+// arena, or until the next one's estimated device bytes do not fit what is
+// left of the admission budget; it then solves them as one
 // block-diagonal batch (run_batch: per-model checks, per-model convergence,
 // a failed member isolated from the others) and publishes one result per
 // request.  While one lane's batch runs, other lanes start the requests

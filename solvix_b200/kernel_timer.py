@@ -1,13 +1,16 @@
 """Device timing of the PCG iteration kernels on a synthetic workload.
 
     python -m solvix_b200.kernel_timer [--workload c3d8_160|c3d8_480|cps4_200] [--reps N]
+                                       [--solve]
 
 Assembles the workload on cuda:0, then times the three FP64 iteration
-kernels (SpMV + p.Kp, u/r update + dots, p update) with CUDA events over
-``--reps`` back-to-back launches each and prints their average duration
-and the SpMV's HBM throughput from its algorithmic bytes.  Small and
-self-contained, so it is also the command to profile a single kernel with
-ncu.
+kernels (node-block SpMV + p.Kp, u/r update + dots, p update) with CUDA
+events over ``--reps`` back-to-back launches each and prints their average
+duration and the SpMV's HBM throughput from its algorithmic bytes.  With
+``--solve`` it runs one full FP64 solve instead (the persistent cooperative
+PCG kernel, one launch per chunk of iterations) and prints its device time
+and per-iteration algorithmic bytes.  Small and self-contained, so it is
+also the command to profile a single kernel with ncu.
 """
 from __future__ import annotations
 
@@ -29,18 +32,42 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="time the PCG iteration kernels")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3d8_160")
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--solve", action="store_true", help="one full persistent FP64 solve")
     args = ap.parse_args(argv)
     flat = WORKLOADS[args.workload]()
     with Context(0) as ctx:
         op = ctx.assemble(flat)
-        ms = op.time_kernels(reps=args.reps)
         n, nnz = op.n, op.nnz
-        spmv_bytes = nnz * 12 + 4 * (n + 1) + 16 * n
-        out = {"workload": args.workload, "n": n, "nnz": nnz, "reps": args.reps,
-               "spmv_ms": ms[0], "update_ms": ms[1], "p_update_ms": ms[2],
-               "spmv_bytes": spmv_bytes, "spmv_gbs": spmv_bytes / (ms[0] * 1e-3) / 1e9}
+        if args.solve:
+            it, res, ms_solve, _, _ = op.solve_device(want_stress=False)
+            b = pcg_iteration_bytes(n, nnz, flat.ndof, flat.n_nodes)
+            out = {"workload": args.workload, "n": n, "nnz": nnz, "iterations": it,
+                   "residual": res, "pcg_ms": ms_solve, "bytes_per_iteration": b,
+                   "gbs": b * it / (ms_solve * 1e-3) / 1e9}
+        else:
+            ms = op.time_kernels(reps=args.reps)
+            spmv_bytes = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
+            out = {"workload": args.workload, "n": n, "nnz": nnz, "reps": args.reps,
+                   "spmv_ms": ms[0], "update_ms": ms[1], "p_update_ms": ms[2],
+                   "spmv_bytes": spmv_bytes, "spmv_gbs": spmv_bytes / (ms[0] * 1e-3) / 1e9,
+                   "spmv_fp32_ms": ms[3],
+                   "spmv_fp32_gbs": (spmv_bytes - 4 * nnz) / (ms[3] * 1e-3) / 1e9}
         op.free()
     print(json.dumps(out))
+
+
+def spmv_node_bytes(n: int, nnz: int, ndof: int, n_nodes: int) -> int:
+    """Algorithmic bytes of one node-block SpMV + p.Kp (spmv_node_dot): K
+    values, one 4-byte column index per ndof x ndof block, adj_ptr and
+    node_base, p gathered once, q written, p read for the dot."""
+    return int(8 * nnz + 4 * nnz // (ndof * ndof) + 16 * (n_nodes + 1) + 24 * n)
+
+
+def pcg_iteration_bytes(n: int, nnz: int, ndof: int, n_nodes: int) -> int:
+    """Algorithmic bytes of one persistent PCG iteration: the node-block
+    SpMV with p.Kp, then u/r update (u r/w, p, r r/w, q, inv_diag) and the
+    p update (p r/w, r, inv_diag)."""
+    return spmv_node_bytes(n, nnz, ndof, n_nodes) + 8 * n * 11
 
 
 if __name__ == "__main__":
