@@ -571,7 +571,22 @@ __global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restri
 // launch (p, q, partials) is read with ld.global.cg (L2), never through L1.
 // The barrier spins are bounded: on timeout the kernel raises an error flag
 // and returns, and the host reports a device error.
-constexpr int PBLOCK = 512;
+// Persistent kernel shape (build constants): CTA size, CTAs per SM and lanes
+// per node for 3D models (2D models use 16).  Measured on the 160x16x16
+// C3D8 case (us per iteration): 512 x 2 with 32 lanes 34.9, with 16 lanes
+// 39.2, with 8 lanes 36.6; 1024 x 1 35.6-37.5; 256 x 4 41.9; 256 x 6 47.7;
+// 128 x 8 54.7 (more CTAs make every grid barrier dearer).
+#ifndef SVX_PBLOCK
+#define SVX_PBLOCK 512
+#endif
+#ifndef SVX_PBLOCKS_PER_SM
+#define SVX_PBLOCKS_PER_SM 2
+#endif
+#ifndef SVX_PG3D
+#define SVX_PG3D 32
+#endif
+constexpr int PBLOCK = SVX_PBLOCK;
+constexpr int PBLOCKS_PER_SM = SVX_PBLOCKS_PER_SM;
 constexpr long long BARRIER_SPIN_LIMIT = 1LL << 25;
 
 template <int ND, int G, class M, class V>
@@ -658,7 +673,7 @@ __device__ __forceinline__ double sum_partials_cg(const double* partials, int n,
 }
 
 template <int ND, int G, class M, class V, class U>
-__global__ void __launch_bounds__(PBLOCK, 2)
+__global__ void __launch_bounds__(PBLOCK, PBLOCKS_PER_SM)
 pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                       const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
                       const M* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
@@ -1447,17 +1462,17 @@ struct PcgRun {
     int iterate_persistent(int chunk) {
         cudaStream_t st = ctx->stream;
         const int ND = op->ndof;
-        const int PG = (op->pat.max_deg <= 8) ? 8 : 16;
+        const bool narrow = op->pat.max_deg <= 8;
         void* fn = nullptr;
-        if (ND == 3) fn = PG == 8 ? (void*)pcg_persistent_kernel<3, 8, M, V, U>
-                                  : (void*)pcg_persistent_kernel<3, 16, M, V, U>;
-        else fn = PG == 8 ? (void*)pcg_persistent_kernel<2, 8, M, V, U>
-                          : (void*)pcg_persistent_kernel<2, 16, M, V, U>;
+        if (ND == 3) fn = narrow ? (void*)pcg_persistent_kernel<3, 8, M, V, U>
+                                 : (void*)pcg_persistent_kernel<3, SVX_PG3D, M, V, U>;
+        else fn = narrow ? (void*)pcg_persistent_kernel<2, 8, M, V, U>
+                         : (void*)pcg_persistent_kernel<2, 16, M, V, U>;
         int coop = 0, bps = 0;
         SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
         SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, PBLOCK, 0));
         if (!coop || bps <= 0) return -1;
-        const unsigned int B = unsigned(std::min(bps, 2) * ctx->sm_count);
+        const unsigned int B = unsigned(std::min(bps, PBLOCKS_PER_SM) * ctx->sm_count);
         DBuf<double> part_a, part_b;
         DBuf<GridBarrier> gb;
         part_a.alloc(ctx->pool, B + 1);
