@@ -503,14 +503,6 @@ residual_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
     }
 }
 
-// u64 += scale * d32
-__global__ void correct_kernel(int64_t n, double* __restrict__ u, const float* __restrict__ d,
-                               double scale) {
-    for (int64_t i = int64_t(blockIdx.x) * BLOCK + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * BLOCK)
-        u[i] += scale * double(d[i]);
-}
-
 // The FP32 operator of the mixed form.  Rounding each entry of K to FP32
 // (relative error ~6e-8) breaks K's translation null space: for a smooth
 // field x the product K x is the small difference of large terms, and the
@@ -1366,13 +1358,6 @@ int pick_group(double mean_row) {
     if (mean_row < 40) return 8;
     if (mean_row < 96) return 16;
     return 32;
-}
-
-unsigned grid_rows(const svx_ctx* ctx, int64_t n, int G) {
-    int64_t per_block = BLOCK / G;
-    int64_t need = (n + per_block - 1) / per_block;
-    int64_t cap = int64_t(ctx->sm_count) * 8;
-    return unsigned(std::max<int64_t>(1, std::min(need, cap)));
 }
 
 unsigned grid_vec(const svx_ctx* ctx, int64_t n) {
