@@ -557,6 +557,8 @@ __global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restri
 //   A: q = K p on own nodes, partial p.q          -> grid barrier
 //   B: alpha; u, r update on own rows, partials    -> grid barrier
 //   C: beta; p = z + beta p on own rows            -> grid barrier
+// (3D models; 2D models run pcg_persistent2_kernel, which forms p inside A
+// and needs only the first two barriers).
 // Every block sums the same partials in the same order, so all blocks hold
 // bitwise identical scalars and take the same exit (converged, breakdown,
 // budget) without a broadcast.  Data written by other blocks during the
@@ -664,13 +666,14 @@ __device__ __forceinline__ double sum_partials_cg(const double* partials, int n,
     return block_sum(v, sh);
 }
 
+// The three-barrier kernel (3D models).
 template <int ND, int G, class M, class V, class U>
 __global__ void __launch_bounds__(PBLOCK, PBLOCKS_PER_SM)
 pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                       const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
                       const M* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
-                      V* p, V* q, double* part_a, double* part_b, PcgScalars* s,
-                      GridBarrier* gb, int chunk) {
+                      V* p, V* /*p2*/, V* q, double* part_a, double* part_b,
+                      PcgScalars* s, GridBarrier* gb, int chunk) {
     __shared__ double sh[32];
     const unsigned int B = gridDim.x;
     const int64_t nb0 = n_nodes * int64_t(blockIdx.x) / B;
@@ -774,6 +777,189 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         s->res = res;
         s->rr = rr;
         s->rz = rz;
+    }
+}
+
+// Node rows of the persistent kernel with the search direction formed on
+// the fly: x_j = r_j * inv_diag_j + beta * pprev_j (p of this iteration,
+// from the previous p, this iteration's r and beta), so no pass and no grid
+// barrier is spent writing p before the SpMV reads it.
+template <int ND, int G, class M, class V>
+__device__ __forceinline__ void node_rows_pp(const int64_t* __restrict__ adj_ptr,
+                                             const int32_t* __restrict__ adj,
+                                             const int64_t* __restrict__ node_base,
+                                             const M* __restrict__ vals, const V* r,
+                                             const V* __restrict__ inv_diag, const V* pprev,
+                                             V bprev, int64_t i, int gl, double* acc) {
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const M* __restrict__ v = vals + node_base[i];
+    auto pdir = [&](int64_t row) -> double {
+        return double(__ldcg(r + row) * __ldg(inv_diag + row) + bprev * __ldcg(pprev + row));
+    };
+    if (d == 0) {
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = double(v[da]) * pdir(i * ND + da);
+        return;
+    }
+    const int rowlen = ND * d;
+    // FP32 operators are stored in difference form (compensated_fp32_kernel)
+    constexpr bool DIFF = std::is_same<M, float>::value;
+    double xi[ND];
+    if constexpr (DIFF) {
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xi[db] = pdir(i * ND + db);
+    }
+#pragma unroll 2
+    for (int k = gl; k < d; k += G) {
+        const int32_t j = __ldg(adj + a0 + k);
+        const int64_t c = int64_t(j) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xv[db] = pdir(c + db);
+        if constexpr (DIFF) {
+            if (j != int32_t(i))
+#pragma unroll
+                for (int db = 0; db < ND; ++db) xv[db] -= xi[db];
+        }
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                acc[da] += double(__ldg(v + da * rowlen + k * ND + db)) * xv[db];
+    }
+}
+
+// Two grid barriers per iteration (2D models).  Iteration k keeps p_k in buf[k & 1]
+// (buf[0] = p, buf[1] = p2) and forms it on the fly from p_{k-1} in the
+// other buffer: at the start of iteration k, r_k, beta_{k-1} (PcgScalars.beta)
+// and p_{k-1} are final; p_{-1} is zero and beta_{-1} = 0, so p_0 = z_0.
+//   A: q = K p_k on own nodes (neighbours' p_k formed from their r and
+//      p_{k-1}), p_k of own rows stored, p_k.q     -> grid barrier
+//   B: alpha; u += alpha p_k, r -= alpha q on own rows; r.r, r.z
+//                                                   -> grid barrier
+// then beta_k = r.z / r.z_prev and the next iteration.  A block writes one
+// buffer while every block reads the other, and r is written only in B, so
+// the two barriers order every access.  Forming p on the fly triples the
+// gathered vector loads of the SpMV: on the 200x20 CPS4 case (9 neighbour
+// blocks a node) an iteration takes 11.7 us against 14.2 us with three
+// barriers, on the 160x16x16 C3D8 case (27 blocks) 48.9 us against 34.9 us,
+// so 3D models keep the three-barrier kernel.
+template <int ND, int G, class M, class V, class U>
+__global__ void __launch_bounds__(PBLOCK, PBLOCKS_PER_SM)
+pcg_persistent2_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                       const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                       const M* __restrict__ vals, const V* __restrict__ inv_diag, U* u, V* r,
+                       V* p, V* p2, V* q, double* part_a, double* part_b, PcgScalars* s,
+                       GridBarrier* gb, int chunk) {
+    __shared__ double sh[32];
+    const unsigned int B = gridDim.x;
+    const int64_t nb0 = n_nodes * int64_t(blockIdx.x) / B;
+    const int64_t nb1 = n_nodes * int64_t(blockIdx.x + 1) / B;
+    const int64_t r0 = nb0 * ND, r1 = nb1 * ND;
+    volatile PcgScalars* vs = s;
+    if (vs->status != PCG_RUNNING) return;
+    double rz = vs->rz, rr = vs->rr, res = vs->res, beta = vs->beta;
+    const double bnorm = vs->bnorm, tol = vs->tol, rr_stop = vs->rr_stop;
+    long long it = vs->it;
+    const long long max_iter = vs->max_iter;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t warp_nodes = 32 / G;
+    const int64_t step = int64_t(PBLOCK / 32) * warp_nodes;
+    const bool writer = (blockIdx.x == 0 && threadIdx.x == 0);
+    for (int c = 0; c < chunk; ++c) {
+        V* pcur = (it & 1) ? p2 : p;
+        const V* pprev = (it & 1) ? p : p2;
+        const V bprev = V(beta);
+        // A: q = K p_k on own nodes, p_k of own rows, p_k.q
+        double dot = 0.0;
+        for (int64_t nb = nb0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < nb1; nb += step) {
+            const int64_t i = nb + ((threadIdx.x & 31) / G);
+            double acc[ND];
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+            if (i < nb1)
+                node_rows_pp<ND, G, M, V>(adj_ptr, adj, node_base, vals, r, inv_diag, pprev,
+                                          bprev, i, gl, acc);
+#pragma unroll
+            for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+            if (i < nb1 && gl == 0) {
+#pragma unroll
+                for (int da = 0; da < ND; ++da) {
+                    const int64_t row = i * ND + da;
+                    const V pk = __ldcg(r + row) * inv_diag[row] + bprev * __ldcg(pprev + row);
+                    pcur[row] = pk;
+                    const V qv = V(acc[da]);
+                    q[row] = qv;
+                    dot += double(pk) * double(qv);
+                }
+            }
+        }
+        double bs = block_sum(dot, sh);
+        if (threadIdx.x == 0) part_a[blockIdx.x] = bs;
+        if (!grid_sync(gb, B)) return;
+        const double pap = sum_partials_cg(part_a, int(B), 1, 0, sh);
+        if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
+            if (writer) {
+                s->pap = pap;
+                s->it = it + 1;
+                s->res = sqrt(rr) / bnorm;
+                s->rr = rr;
+                s->rz = rz;
+                __threadfence();
+                s->status = PCG_BREAKDOWN;
+            }
+            return;
+        }
+        const double alpha = rz / pap;
+        // B: u += alpha p_k, r -= alpha q on own rows; r.r, r.z
+        const V a = V(alpha);
+        double lrr = 0.0, lrz = 0.0;
+        for (int64_t row = r0 + threadIdx.x; row < r1; row += PBLOCK) {
+            const V pi = __ldcg(pcur + row);
+            u[row] = U(u[row] + U(a) * U(pi));
+            const V ri = __ldcg(r + row) - a * __ldcg(q + row);
+            r[row] = ri;
+            const V zi = ri * inv_diag[row];
+            lrr += double(ri) * double(ri);
+            lrz += double(ri) * double(zi);
+        }
+        const double brr = block_sum(lrr, sh);
+        const double brz = block_sum(lrz, sh);
+        if (threadIdx.x == 0) {
+            part_b[2 * blockIdx.x] = brr;
+            part_b[2 * blockIdx.x + 1] = brz;
+        }
+        if (!grid_sync(gb, B)) return;
+        const double rr_new = sum_partials_cg(part_b, int(B), 2, 0, sh);
+        const double rz_new = sum_partials_cg(part_b, int(B), 2, 1, sh);
+        it += 1;
+        rr = rr_new;
+        res = sqrt(rr) / bnorm;
+        if (res <= tol || it >= max_iter || rr <= rr_stop) {
+            if (writer) {
+                s->it = it;
+                s->res = res;
+                s->rr = rr;
+                s->rz = rz;         // r.z of the previous iterate (beta's denominator)
+                s->pap = rz_new;    // r.z of this iterate
+                s->alpha = alpha;
+                __threadfence();
+                s->status = (res <= tol) ? PCG_CONVERGED
+                                         : (it >= max_iter ? PCG_MAXITER : PCG_RELIABLE);
+            }
+            return;
+        }
+        beta = rz_new / rz;
+        rz = rz_new;
+    }
+    if (writer) {
+        s->it = it;
+        s->res = res;
+        s->rr = rr;
+        s->rz = rz;
+        s->beta = beta;
     }
 }
 
@@ -1430,6 +1616,7 @@ struct PcgRun {
     const V* inv_diag;
     U* u;
     V *r, *p, *q;
+    V* p2 = nullptr;  // the persistent kernel's second search-direction buffer (zeroed)
     double* partials;
     PcgScalars* s;
     PcgScalars* h_s;  // pinned
@@ -1451,8 +1638,8 @@ struct PcgRun {
         void* fn = nullptr;
         if (ND == 3) fn = narrow ? (void*)pcg_persistent_kernel<3, 8, M, V, U>
                                  : (void*)pcg_persistent_kernel<3, SVX_PG3D, M, V, U>;
-        else fn = narrow ? (void*)pcg_persistent_kernel<2, 8, M, V, U>
-                         : (void*)pcg_persistent_kernel<2, 16, M, V, U>;
+        else fn = narrow ? (void*)pcg_persistent2_kernel<2, 8, M, V, U>
+                         : (void*)pcg_persistent2_kernel<2, 16, M, V, U>;
         int coop = 0, bps = 0;
         SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
         SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, PBLOCK, 0));
@@ -1471,9 +1658,11 @@ struct PcgRun {
         GridBarrier* gbp = gb.p;
         double* pa = part_a.p;
         double* pb = part_b.p;
+        if (!p2) return -1;
         void* args[] = {&n_nodes, (void*)&a_ptr, (void*)&a_idx, (void*)&nbase, (void*)&vals,
-                        (void*)&inv_diag, (void*)&u, (void*)&r, (void*)&p, (void*)&q,
-                        (void*)&pa, (void*)&pb, (void*)&s, (void*)&gbp, (void*)&chunk};
+                        (void*)&inv_diag, (void*)&u, (void*)&r, (void*)&p, (void*)&p2,
+                        (void*)&q, (void*)&pa, (void*)&pb, (void*)&s, (void*)&gbp,
+                        (void*)&chunk};
         SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
         SVX_CUDA(cudaStreamSynchronize(st));
         const long long launches_max = h_s->max_iter / chunk + 2;
@@ -1669,11 +1858,16 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     cudaStream_t st = ctx->stream;
     PcgResult out{PCG_CONVERGED, 0, 0.0, 0.0};
     if (check_every <= 0) check_every = auto_check_every(n, op->pat.nnz);
-    DBuf<double> r, p, q, partials;
+    DBuf<double> r, p, p2, q, partials;
     DBuf<PcgScalars> s;
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
+    const bool graph = op->pat.nnz > GRAPH_MIN_NNZ;
+    if (!graph) {
+        p2.alloc(ctx->pool, n + 1);
+        SVX_CUDA(cudaMemsetAsync(p2.p, 0, (n + 1) * sizeof(double), st));
+    }
     const int G = pick_node_group(op->pat.max_deg);
     PcgRun<double, double, double> run;
     run.ctx = ctx;
@@ -1701,6 +1895,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     run.r = r.p;
     run.p = p.p;
     run.q = q.p;
+    run.p2 = p2.p;
     run.partials = partials.p;
     run.s = s.p;
     run.h_s = hs.h;
@@ -1708,8 +1903,9 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     SVX_CUDA(cudaStreamSynchronize(st));
     int status = hs.h->status;
     if (status == PCG_RUNNING) {
-        status = (op->pat.nnz > GRAPH_MIN_NNZ) ? -1
-                                               : run.iterate_persistent(persistent_chunk(op->pat.nnz));
+        // the graph form starts from the init kernel's p = z0 too: a
+        // persistent launch that cannot start leaves p untouched
+        status = graph ? -1 : run.iterate_persistent(persistent_chunk(op->pat.nnz));
         if (status < 0) status = run.iterate(check_every);
     }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
@@ -1771,12 +1967,16 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     cudaStream_t st = ctx->stream;
     build_fp32_operator(ctx, op);
     const int G = pick_node_group(op->pat.max_deg);
-    DBuf<double> r, p, q, r64, partials, rr_dev;
+    DBuf<double> r, p, p2, q, r64, partials, rr_dev;
     DBuf<PcgScalars> s;
     DBuf<unsigned int> counter;
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
+    if (!graph) {
+        p2.alloc(ctx->pool, n + 1);
+        SVX_CUDA(cudaMemsetAsync(p2.p, 0, (n + 1) * sizeof(double), st));
+    }
     r64.alloc(ctx->pool, n + 1);
     rr_dev.alloc(ctx->pool, 1);
     counter.alloc(ctx->pool, 1);
@@ -1799,6 +1999,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         run.r = r.p;
         run.p = p.p;
         run.q = q.p;
+        run.p2 = p2.p;
         run.partials = partials.p;
         run.s = s.p;
         run.h_s = hs.h;
@@ -1850,13 +2051,17 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     const int chunk = persistent_chunk(op->pat.nnz);
     while (status == PCG_RUNNING) {
         if (fp64_phase) {
-            status = graph ? -1 : exact.iterate_persistent(chunk);
-            if (status < 0) status = exact.iterate(check_every);
+            status = graph ? exact.iterate(check_every) : exact.iterate_persistent(chunk);
+            if (status < 0)
+                throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                "mixed precision below 50M nonzeros needs a cooperative launch"};
             res = hs.h->res;
             break;
         }
-        status = graph ? -1 : sloppy.iterate_persistent(chunk);
-        if (status < 0) status = sloppy.iterate(check_every);
+        status = graph ? sloppy.iterate(check_every) : sloppy.iterate_persistent(chunk);
+        if (status < 0)
+            throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                            "mixed precision below 50M nonzeros needs a cooperative launch"};
         sloppy_iters = hs.h->it;
         if (status == PCG_BREAKDOWN) break;
         // segment ended (reduced by delta, capped, or sloppy-converged):
@@ -1890,8 +2095,13 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         set_field(&PcgScalars::max_iter,
                   fp64_phase ? max_iter : std::min(max_iter, hs.h->it + seg_cap));
         set_field(&PcgScalars::status, int(PCG_RUNNING));
-        p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p.p, r.p, op->inv_diag.p, s.p);
-        SVX_LAUNCH_CHECK();
+        // the graph form and the three-barrier (3D) persistent kernel
+        // update p here; the two-barrier (2D) one forms the next p itself
+        // from r, the previous p and beta
+        if (graph || op->ndof == 3) {
+            p_update_kernel<double><<<grid_v, BLOCK, 0, st>>>(n, p.p, r.p, op->inv_diag.p, s.p);
+            SVX_LAUNCH_CHECK();
+        }
         status = PCG_RUNNING;
     }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));
