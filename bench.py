@@ -228,6 +228,10 @@ def run_ours(args, rank, world, local_rank):
         op.reassemble()
         return op.solve_device(precision=precision, want_stress=True)
 
+    # nvidia-smi starts before the warm-up, so that its start-up (driver and
+    # NVML initialisation) does not fall into the timed steps
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for _ in range(max(args.warmup, 0)):
         step()
     # flush L2 before the timed region (the per-step working set, K + Ke
@@ -239,8 +243,6 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     launches0 = lib.svx_launch_count()

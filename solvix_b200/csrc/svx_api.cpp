@@ -797,6 +797,7 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         SVX_CUDA(cudaStreamCreateWithPriority(&ctx->aux_stream, cudaStreamNonBlocking, least));
         for (auto& e : ctx->ev) SVX_CUDA(cudaEventCreate(&e));
         SVX_CUDA(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+        SVX_CUDA(cudaMallocHost(&ctx->h_scalars, 256));
         SVX_CUDA(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
         ctx->pool = new DevicePool(device);
         *out = ctx.release();
@@ -811,6 +812,7 @@ int svx_ctx_destroy(svx_ctx_t* ctx) {
     delete ctx->pool;
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     for (cudaStream_t x : {ctx->pcg_stream, ctx->aux_stream})

@@ -171,6 +171,7 @@ struct svx_ctx {
     svx::PinnedBuffer staging;  // batched host<->device staging
     std::string last_error;
     cudaEvent_t ev[8] = {};
+    void* h_scalars = nullptr;  // page-locked PcgScalars of the context's solves
 };
 
 namespace svx {

@@ -1729,12 +1729,14 @@ struct PcgRun {
     }
 };
 
+static_assert(sizeof(PcgScalars) <= 256, "the context's pinned scalar slot holds 256 bytes");
+
 struct PinnedScalars {
     PcgScalars* h = nullptr;
-    PinnedScalars() { SVX_CUDA(cudaMallocHost(&h, sizeof(PcgScalars))); }
-    ~PinnedScalars() {
-        if (h) cudaFreeHost(h);
-    }
+    // the context's page-locked slot: no cudaMallocHost / cudaFreeHost per
+    // solve (each can stall for milliseconds while other processes hold
+    // the driver)
+    explicit PinnedScalars(svx_ctx* ctx) : h(static_cast<PcgScalars*>(ctx->h_scalars)) {}
 };
 
 // Iterations per persistent launch: a few to tens of milliseconds of work,
@@ -1878,7 +1880,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     run.grid_v = grid_vec(ctx, n);
     partials.alloc(ctx->pool, 2 * size_t(std::max(run.grid_r, run.grid_v)) + 2);
     s.alloc(ctx->pool, 1);
-    PinnedScalars hs;
+    PinnedScalars hs(ctx);
     PcgScalars init{};
     init.tol = tol;
     init.max_iter = max_iter;
@@ -1984,7 +1986,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     const unsigned grid_r = grid_nodes(ctx, op->n_nodes, G), grid_v = grid_vec(ctx, n);
     partials.alloc(ctx->pool, 2 * size_t(std::max(grid_r, grid_v)) + 2);
     s.alloc(ctx->pool, 1);
-    PinnedScalars hs;
+    PinnedScalars hs(ctx);
     PcgRun<float, double, double> sloppy;
     PcgRun<double, double, double> exact;
     auto wire = [&](auto& run) {
