@@ -1,7 +1,7 @@
 """Device timing of the PCG iteration kernels on a synthetic workload.
 
     python -m solvix_b200.kernel_timer [--workload c3d8_160|c3d8_480|cps4_200] [--reps N]
-                                       [--solve]
+                                       [--solve] [--batch N]
 
 Assembles the workload on cuda:0, then times the three FP64 iteration
 kernels (node-block SpMV + p.Kp, u/r update + dots, p update) with CUDA
@@ -9,8 +9,10 @@ events over ``--reps`` back-to-back launches each and prints their average
 duration and the SpMV's HBM throughput from its algorithmic bytes.  With
 ``--solve`` it runs one full FP64 solve instead (the persistent cooperative
 PCG kernel, one launch per chunk of iterations) and prints its device time
-and per-iteration algorithmic bytes.  Small and self-contained, so it is
-also the command to profile a single kernel with ncu.
+and per-iteration algorithmic bytes.  With ``--batch N`` it runs one
+batched FP64 solve of the first N plates of the 4,096-plate mix.  Small and
+self-contained, so it is also the command to profile a single kernel with
+ncu.
 """
 from __future__ import annotations
 
@@ -33,7 +35,22 @@ def main(argv=None):
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3d8_160")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--solve", action="store_true", help="one full persistent FP64 solve")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead: one batched solve of this many plates of the 4,096-plate mix")
     args = ap.parse_args(argv)
+    if args.batch > 0:
+        flats = workloads.plate_batch(4096, seed=4)[:args.batch]
+        with Context(0) as ctx:
+            out, st = ctx.solve_batch(flats)
+            its = sum(o["iterations"] for o in out)
+            b = sum(o["iterations"] * pcg_iteration_bytes(f.n_dof, o["nnz"], f.ndof, f.n_nodes)
+                    for f, o in zip(flats, out))
+            print(json.dumps({"batch": len(flats), "total_dof": st["total_dof"],
+                              "iterations": its, "pcg_ms": st["ms_solve"],
+                              "threads_per_cta": st["threads_per_cta"],
+                              "lanes_per_node": st["lanes_per_node"], "algorithmic_bytes": b,
+                              "gbs": b / (st["ms_solve"] * 1e-3) / 1e9}))
+        return
     flat = WORKLOADS[args.workload]()
     with Context(0) as ctx:
         op = ctx.assemble(flat)
