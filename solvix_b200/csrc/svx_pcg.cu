@@ -1,26 +1,35 @@
-// svx_pcg.cu - K5 CSR SpMV, K6 fused PCG vector kernels and K7 mixed
-// precision defect correction.
+// svx_pcg.cu - K5 SpMV, K6 fused PCG vector kernels, the persistent PCG
+// kernels, K7 mixed precision and K8 batched PCG.
 //
 // The plain form restates solver::pcg_with_threads
 // (crates/solvix-core/src/solver.rs:82-149) on the device:
-//   per iteration  q = K p ; pap = p.q            (spmv_dot, one pass)
+//   per iteration  q = K p ; pap = p.q
 //                  alpha = rz / pap ; u += alpha p ; r -= alpha q ;
-//                  rr = r.r ; z = r * inv_diag ; rz' = r.z   (update, one pass)
-//                  beta = rz' / rz ; p = z + beta p          (p_update, one pass)
+//                  rr = r.r ; z = r * inv_diag ; rz' = r.z
+//                  beta = rz' / rz ; p = z + beta p
 // with the same stopping rule (||r|| / ||f|| <= tol, checked after the r
 // update; pap <= 0 or NaN is a breakdown) and the same iteration count
 // semantics.  Every reduction is deterministic: fixed launch geometry,
-// warp-shuffle then shared-memory trees inside a block, and the last block
-// to finish (atomic ticket) sums the per-block partials in index order.
-// The three kernels of an iteration run as a CUDA graph of `check_every`
-// iterations; kernels return immediately once the device status says the
-// solve stopped, and the host reads the status once per graph launch.
+// warp-shuffle then shared-memory trees inside a block, and either the last
+// block to finish (atomic ticket) or every block after a grid barrier sums
+// the per-block partials in index order.
 //
-// SpMV layout: G consecutive lanes own one row (G picked from the mean row
-// length: 81 nnz/row C3D8 rows use G = 16); lanes stream col_idx / vals
-// with unit stride (coalesced), gather x through L1/L2 (the x window of a
-// row block of a structured mesh is three node planes, far larger than
-// shared memory, so x is not staged there), and combine with shuffles.
+// Three ways to run an iteration:
+//  * the persistent cooperative kernels (systems up to 50M nonzeros): one
+//    launch runs up to `persistent_chunk` whole iterations, its blocks
+//    meeting at bounded grid barriers;
+//  * the CUDA-graph form (larger systems): the standalone node-block SpMV
+//    (spmv_node_dot), update and p_update kernels, `check_every` iterations
+//    per graph launch; kernels return at once after the device status
+//    leaves RUNNING, and the host reads the status once per graph launch;
+//  * the batched kernels: one CTA, or one 8-CTA cluster, per model.
+//
+// SpMV layout: K is stored in node blocks (a node's ndof rows over its
+// sorted neighbours, contiguous); G lanes own one node and split its
+// neighbour blocks, each lane loading one column index, ndof x values and
+// ndof^2 K values, all independent of each other; the x gathers go through
+// L1/L2 and the lanes combine with shuffles.  The CSR kernels further down
+// serve the allocation-free entry point, which takes a caller's CSR.
 
 #include "svx_internal.h"
 
