@@ -568,7 +568,7 @@ def run_precision(args, rank, world, local_rank):
 SERVED_NAME = ("Poisson stream of solve requests: 70% 2D plates of the batched mix, 30% "
                "C3D8 cantilevers nx~U{20..120}, ny=nz~U{4..16}, E=70e9, nu=0.33, tip load "
                "U(1e3,1e4) N (seed 5); relative residual 1e-10; 40 GiB admission budget; "
-               "4 lanes")
+               "2 lanes")
 
 
 def _serve_run(srv, reqs, rate_scale, base_t):

@@ -331,14 +331,17 @@ int svx_batch_solve(svx_ctx_t* ctx, int32_t count, const svx_flat_model_t* model
  * memory pool (blocks are reused only on the stream that freed them) whose
  * arena, budget / lanes, is reserved at creation, so batches of any size
  * make no cudaMalloc / cudaFree calls in steady state; a lane's batch stays
- * within its arena. */
+ * within its arena (blocks that fragmentation leaves no room for fall back
+ * to cudaMalloc). */
 typedef struct svx_server svx_server_t;
 
 typedef struct svx_serve_opts {
     int64_t hbm_budget_bytes;  /* admission budget; 0 = 40 GiB */
-    int32_t lanes;             /* concurrent batches (streams); 0 = 4 */
+    int32_t lanes;             /* concurrent batches (streams); 0 = 2 */
     int32_t max_batch;         /* requests per batch at most; 0 = 4096 */
     svx_solve_opts_t solve;    /* tolerance, precision, max_iter, want_stress */
+    int64_t max_batch_bytes;   /* estimated device bytes per batch at most;
+                                  0 = a lane's arena (budget / lanes) */
 } svx_serve_opts_t;
 
 typedef struct svx_serve_result {

@@ -174,6 +174,7 @@ class SvxServeOpts(C.Structure):
         ("lanes", C.c_int32),
         ("max_batch", C.c_int32),
         ("solve", SvxSolveOpts),
+        ("max_batch_bytes", C.c_int64),
     ]
 
 

@@ -43,15 +43,16 @@ from .model import DeviceError
 class Server:
     """A served-solve loop on one device (svx_serve_create)."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 40 << 30, lanes: int = 4,
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 40 << 30, lanes: int = 2,
                  max_batch: int = 4096, tol: float = 1e-10, precision: int = abi.SVX_MIXED,
-                 max_iter: int = 0, want_stress: bool = True):
+                 max_iter: int = 0, want_stress: bool = True, max_batch_bytes: int = 0):
         self.lib = abi.load()
         opts = abi.SvxServeOpts()
         self.lib.svx_serve_default_opts(C.byref(opts))
         opts.hbm_budget_bytes = int(hbm_budget_bytes)
         opts.lanes = int(lanes)
         opts.max_batch = int(max_batch)
+        opts.max_batch_bytes = int(max_batch_bytes)
         opts.solve = abi.default_opts(tol=tol, precision=precision, max_iter=max_iter,
                                       want_stress=int(want_stress))
         self.opts = opts
@@ -267,7 +268,7 @@ def main(argv=None) -> int:
                     help="JSON-lines requests on stdin, results on stdout")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
-    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--tol", type=float, default=1e-10)
     args = ap.parse_args(argv)
