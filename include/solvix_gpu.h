@@ -417,6 +417,16 @@ int64_t svx_launch_count(void);
  * update, ms4[3] = the difference-form FP32 SpMV of the mixed form. */
 int svx_op_time_kernels(svx_op_t* op, int reps, double* ms4);
 
+/* ---- diagnostics ---------------------------------------------------- */
+/* No counterpart in the reference.  Runs the persistent PCG kernels' grid
+ * barrier with one block where it expects two, so that nothing ever
+ * releases it, and a spin limit of `spins` polls (1..2^24).  Every wait in
+ * the library's kernels is bounded this way; on a healthy device the wait
+ * runs out, the kernel raises the barrier's error flag and returns, and the
+ * context stays usable.  Fills *returned_ok (0 = the barrier reported the
+ * time-out to its caller) and *error_flag (1 = the flag was raised). */
+int svx_diag_barrier_timeout(int device, long long spins, int* returned_ok, int* error_flag);
+
 /* ---- PCG without device allocation ---------------------------------- */
 /* Largest system (rows) svx_pcg_solve_noalloc accepts. */
 #define SVX_NOALLOC_MAX_DOF 262144

@@ -226,6 +226,8 @@ SIGNATURES = {
     "svx_ctx_stream": (C.c_void_p, [_VP]),
     "svx_op_reassemble": (C.c_int, [_VP, C.POINTER(SvxError)]),
     "svx_launch_count": (C.c_int64, []),
+    "svx_diag_barrier_timeout": (C.c_int, [C.c_int, C.c_longlong, C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int)]),
     "svx_op_time_kernels": (C.c_int, [_VP, C.c_int, c_double_p]),
     "svx_pcg_solve_noalloc": (C.c_int, [C.c_int64, _VP, _VP, _VP, _VP, C.c_double, C.c_int64,
                                         _VP, c_int64_p, c_double_p, _VP]),

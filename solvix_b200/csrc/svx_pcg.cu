@@ -636,7 +636,8 @@ __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr
 }
 
 // Bounded grid-wide barrier (all blocks co-resident: cooperative launch).
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks,
+                                          long long spin_limit = BARRIER_SPIN_LIMIT) {
     __shared__ int ok;
     __threadfence();
     __syncthreads();
@@ -652,7 +653,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks)
         } else {
             long long spins = 0;
             while (*vgen == g) {
-                if (++spins > BARRIER_SPIN_LIMIT) {
+                if (++spins > spin_limit) {
                     atomicExch(&gb->error, 1);
                     good = 0;
                     break;
@@ -2579,3 +2580,51 @@ void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& 
 }
 
 }  // namespace svx
+
+// ------------------------------------------------------------ diagnostics
+namespace svx {
+namespace {
+
+// One block meets a barrier that expects two: nothing ever releases it, so
+// the wait must run out, raise the error flag and return.
+__global__ void barrier_timeout_kernel(GridBarrier* gb, long long spin_limit, int* out) {
+    const bool ok = grid_sync(gb, 2u, spin_limit);
+    if (threadIdx.x == 0) out[0] = ok ? 1 : 0;
+}
+
+}  // namespace
+}  // namespace svx
+
+extern "C" int svx_diag_barrier_timeout(int device, long long spins, int* returned_ok,
+                                        int* error_flag) {
+    using namespace svx;
+    if (spins <= 0 || spins > (1LL << 24) || !returned_ok || !error_flag)
+        return SVX_BAD_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return SVX_CUDA_ERROR;
+    }
+    GridBarrier* gb = nullptr;
+    int* out = nullptr;
+    cudaError_t e = cudaMalloc(&gb, sizeof(GridBarrier));
+    if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(gb, 0, sizeof(GridBarrier));
+    if (e == cudaSuccess) e = cudaMemset(out, 0xff, sizeof(int));
+    if (e == cudaSuccess) {
+        barrier_timeout_kernel<<<1, 32>>>(gb, spins, out);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        e = cudaGetLastError();
+    }
+    GridBarrier h{};
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&h, gb, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(returned_ok, out, sizeof(int), cudaMemcpyDeviceToHost);
+    if (gb) cudaFree(gb);
+    if (out) cudaFree(out);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return SVX_CUDA_ERROR;
+    }
+    *error_flag = int(h.error);
+    return SVX_OK;
+}
