@@ -3,7 +3,11 @@
 // solve_with_thermal (crates/solvix-core/src/lib.rs:614-703).
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -302,6 +306,35 @@ void check_flat(const svx_flat_model_t* m) {
             bad("fixed row " + std::to_string(m->fixed_row[k]) + " out of range");
 }
 
+// fn(0..count-1) on up to 16 host threads (members of a batch are
+// independent); the first exception is rethrown on the calling thread.
+template <class F>
+void parallel_for(int32_t count, F&& fn) {
+    const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
+    const int threads = std::min({hw, 16, int(count / 8) + 1});
+    if (threads <= 1) {
+        for (int32_t k = 0; k < count; ++k) fn(k);
+        return;
+    }
+    std::atomic<int32_t> next{0};
+    std::exception_ptr first;
+    std::mutex mu;
+    auto work = [&] {
+        try {
+            for (int32_t k = next.fetch_add(1); k < count; k = next.fetch_add(1)) fn(k);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!first) first = std::current_exception();
+            next.store(count);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    if (first) std::rethrow_exception(first);
+}
+
 template <class T>
 void upload(svx_ctx* ctx, DBuf<T>& dst, const T* src, size_t count) {
     dst.alloc(ctx->pool, count + 1);
@@ -571,8 +604,10 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
     clock::time_point t_phase = clock::now();
     int ndof = 0;
     std::vector<int32_t> live;
-    for (int32_t k = 0; k < count; ++k) {
+    for (int32_t k = 0; k < count; ++k)
         if (!models[k]) throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "null model"};
+    // the members' host checks are independent: run them on the host cores
+    parallel_for(count, [&](int32_t k) {
         try {
             check_batch_member(models[k]);
         } catch (const ModelFail& f) {
@@ -580,8 +615,10 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
             out[k].reason = f.reason;
             out[k].elem_index = f.elem_index;
             out[k].message = f.message;
-            continue;
         }
+    });
+    for (int32_t k = 0; k < count; ++k) {
+        if (out[k].status != SVX_OK) continue;
         if (ndof == 0) ndof = models[k]->ndof;
         if (models[k]->ndof != ndof)
             throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "models of one batch share ndof"};
@@ -623,11 +660,21 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
         uint8_t* kind = reinterpret_cast<uint8_t*>(base + o_kind);
         std::vector<int64_t> node_off(static_cast<size_t>(L) + 1, 0);
         std::vector<int64_t> elem_off(static_cast<size_t>(L) + 1, 0);
-        conn_ptr[0] = 0;
-        int64_t n_fixed = 0;
+        std::vector<int64_t> conn_off(static_cast<size_t>(L) + 1, 0);
+        std::vector<int64_t> fix_off(static_cast<size_t>(L) + 1, 0);
         for (int32_t j = 0; j < L; ++j) {
             const svx_flat_model_t& m = *models[live[j]];
-            const int64_t n0 = node_off[j], e0 = elem_off[j];
+            node_off[j + 1] = node_off[j] + m.n_nodes;
+            elem_off[j + 1] = elem_off[j] + m.n_elem;
+            conn_off[j + 1] = conn_off[j] + m.conn_ptr[m.n_elem];
+            fix_off[j + 1] = fix_off[j] + m.n_fixed;
+        }
+        const int64_t n_fixed = fix_off[L];
+        conn_ptr[0] = 0;
+        // every member fills its own ranges: copy them on the host cores
+        parallel_for(L, [&](int32_t j) {
+            const svx_flat_model_t& m = *models[live[j]];
+            const int64_t n0 = node_off[j], e0 = elem_off[j], c0 = conn_off[j];
             std::memcpy(xyz + 3 * n0, m.xyz, sizeof(double) * 3 * m.n_nodes);
             if (m.f)
                 std::memcpy(f + n0 * ndof, m.f, sizeof(double) * m.n_nodes * ndof);
@@ -636,7 +683,6 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
             std::memcpy(kind + e0, m.kind, size_t(m.n_elem));
             std::memcpy(E + e0, m.youngs, sizeof(double) * m.n_elem);
             std::memcpy(nu + e0, m.poisson, sizeof(double) * m.n_elem);
-            const int64_t c0 = conn_ptr[e0];
             for (int64_t e = 0; e < m.n_elem; ++e) {
                 th[e0 + e] = m.thickness;
                 eid[e0 + e] = elem_id_of(&m, e);
@@ -644,10 +690,9 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
             }
             const int32_t shift = int32_t(n0);
             for (int64_t q = 0; q < m.conn_ptr[m.n_elem]; ++q) conn[c0 + q] = m.conn[q] + shift;
-            for (int64_t q = 0; q < m.n_fixed; ++q) fixed[n_fixed++] = m.fixed_row[q] + n0 * ndof;
-            node_off[j + 1] = n0 + m.n_nodes;
-            elem_off[j + 1] = e0 + m.n_elem;
-        }
+            for (int64_t q = 0; q < m.n_fixed; ++q)
+                fixed[fix_off[j] + q] = m.fixed_row[q] + n0 * ndof;
+        });
         svx_flat_model_t all{};
         all.n_nodes = nn;
         all.xyz = xyz;
@@ -721,7 +766,7 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
                                      cudaMemcpyDeviceToHost, st));
         SVX_CUDA(cudaStreamSynchronize(st));
         if (want_vm) run.ms_stress = elapsed_ms(ctx->ev[4], ctx->ev[5]);
-        for (int32_t j = 0; j < L; ++j) {
+        parallel_for(L, [&](int32_t j) {
             const int32_t k = live[j];
             if (u && u[k])
                 std::memcpy(u[k], host + node_off[j] * ndof,
@@ -729,7 +774,7 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
             if (want_vm && vm[k])
                 std::memcpy(vm[k], host + nu_rows + elem_off[j],
                             sizeof(double) * (elem_off[j + 1] - elem_off[j]));
-        }
+        });
         for (int32_t j = 0; j < L; ++j) {
             BatchModelOut& m = out[live[j]];
             m.iterations = it[j];
