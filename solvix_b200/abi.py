@@ -112,6 +112,13 @@ class SvxFlatModel(C.Structure):
     ]
 
 
+class SvxFlatModelRaw(C.Structure):
+    """svx_flat_model_t with untyped pointers: the same layout, filled from
+    integer addresses (cheap for thousands of batch members)."""
+    _fields_ = [(name, C.c_void_p if issubclass(t, C._Pointer) else t)
+                for name, t in SvxFlatModel._fields_]
+
+
 class SvxSolveOpts(C.Structure):
     _fields_ = [
         ("tol", C.c_double),

@@ -115,7 +115,8 @@ class Context:
         """
         flats = list(flats)
         count = len(flats)
-        structs = (abi.SvxFlatModel * count)(*[f.as_struct() for f in flats])
+        raw = (abi.SvxFlatModelRaw * count)(*[f.raw_fields() for f in flats])
+        structs = C.cast(raw, C.POINTER(abi.SvxFlatModel))
         us = [np.zeros(f.n_dof) if want_u else None for f in flats]
         vms = [np.zeros(f.n_elem) if want_stress else None for f in flats]
         u_ptrs = (abi.c_double_p * count)(*[abi.ptr(a, C.c_double) for a in us])

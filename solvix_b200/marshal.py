@@ -93,6 +93,17 @@ class FlatModel:
         s.f = abi.ptr(self.f, C.c_double)
         return s
 
+    def raw_fields(self) -> tuple:
+        """The svx_flat_model_t fields with integer addresses, in field order
+        (for abi.SvxFlatModelRaw)."""
+        def addr(a):
+            return None if a is None else a.__array_interface__["data"][0]
+        return (self.n_nodes, addr(self.xyz), addr(self.node_id), self.n_elem, addr(self.kind),
+                addr(self.conn_ptr), addr(self.conn), addr(self.youngs), addr(self.poisson),
+                addr(self.no_material), addr(self.elem_id), float(self.thickness),
+                int(self.ndof), int(self.fixed_row.shape[0]), addr(self.fixed_row),
+                addr(self.f))
+
     @classmethod
     def from_struct(cls, s: abi.SvxFlatModel) -> "FlatModel":
         """Copy a library-owned svx_flat_model_t into numpy arrays."""

@@ -232,3 +232,20 @@ def test_resolve_errors_match_oracle(case):
 def test_patch_deck_resolves():
     fp, st, _ = product_resolve(patch_deck())
     assert st == abi.SVX_OK and list(fp.fixed_row) == [0, 14, 6, 1]
+
+
+def test_raw_flat_struct_is_byte_identical_to_the_typed_one():
+    """Batches marshal svx_flat_model_t from integer addresses; the bytes
+    must be the typed struct's."""
+    import ctypes as C
+    import numpy as np
+    from solvix_b200 import abi, workloads
+    rng = np.random.Generator(np.random.PCG64(8))
+    flats = [workloads.plate(rng, nx=5, ny=3),
+             workloads.cantilever_c3d8(3, 2, 2, lx=0.3, ly=0.2, lz=0.2, seed=1)]
+    size = C.sizeof(abi.SvxFlatModel)
+    assert C.sizeof(abi.SvxFlatModelRaw) == size
+    for f in flats:
+        typed = f.as_struct()
+        raw = abi.SvxFlatModelRaw(*f.raw_fields())
+        assert C.string_at(C.addressof(typed), size) == C.string_at(C.addressof(raw), size)
