@@ -391,6 +391,25 @@ BATCH_NAME = ("4,096 independent 2D plates (nx~U{10..160}, ny~U{4..40}, h=1, CPS
               "Jacobi-PCG to 1e-10 per model, centroid von Mises")
 
 
+def one_at_a_time(ctx, flats):
+    """The one-at-a-time plain FP64 GPU path on a sample: every model through
+    svx_solve_flat, one after another, wall clock.  Two passes over the
+    sample (the first also warms the context's pool); the faster is kept.
+    Returns (seconds per solve, device ms per solve of assembly + PCG +
+    stress recovery in that pass)."""
+    best = None
+    for _ in range(2):
+        dev = 0.0
+        t0 = time.perf_counter()
+        for f in flats:
+            sol = ctx.solve_flat(f)
+            dev += sol.ms_assemble + sol.ms_solve + sol.ms_stress
+        per = (time.perf_counter() - t0) / len(flats)
+        if best is None or per < best[0]:
+            best = (per, dev / len(flats))
+    return best
+
+
 def run_batched(args, rank, world, local_rank):
     """C4: the whole plate mix per step through svx_batch_solve; models are
     sharded over ranks (greedy on estimated work, no collective)."""
@@ -482,15 +501,12 @@ def run_batched(args, rank, world, local_rank):
         # the one-at-a-time plain GPU path on a sample of the same models
         rng = np.random.default_rng(0)
         idx = rng.choice(len(flats), 64, replace=False)
-        ctx.solve_flat(flats[int(idx[0])])
-        t0 = time.perf_counter()
-        for k in idx:
-            ctx.solve_flat(flats[int(k)])
-        per = (time.perf_counter() - t0) / len(idx)
+        per, dev_ms = one_at_a_time(ctx, [flats[int(k)] for k in idx])
         line["one_at_a_time"] = {
             "solves_per_s": 1.0 / per,
+            "device_ms_per_solve": dev_ms,
             "sample": "64 models of the mix through svx_solve_flat one after another "
-                      "(wall clock), projected to the set",
+                      "(wall clock, faster of two passes), projected to the set",
             "speedup_device": line["solves_per_s"] * per,
             "speedup_e2e": line["e2e"]["solves_per_s"] * per}
     ctx.close()
@@ -616,7 +632,7 @@ def run_served(args, rank, world, local_rank):
     from solvix_b200.serve import Server
 
     torch.cuda.set_device(local_rank)
-    prec_name = args.precision or "mixed"
+    prec_name = args.precision or "fp64"
     prec = abi.SVX_MIXED if prec_name == "mixed" else abi.SVX_FP64
     other_name = "fp64" if prec_name == "mixed" else "mixed"
     other = abi.SVX_FP64 if prec == abi.SVX_MIXED else abi.SVX_MIXED
@@ -683,13 +699,11 @@ def run_served(args, rank, world, local_rank):
             r = one.poll(200)
             if r is not None:
                 served_u[r["tag"]] = r["u"]
-    ctx.solve_flat(reqs[idx[0]])
-    t0 = time.perf_counter()
     errs = []
     for k in idx:
         ref = ctx.solve_flat(reqs[k])
         errs.append(float(np.linalg.norm(served_u[k] - ref.u) / np.linalg.norm(ref.u)))
-    one_per = (time.perf_counter() - t0) / len(idx)
+    one_per, one_dev_ms = one_at_a_time(ctx, [reqs[k] for k in idx])
     ctx.close()
     rows = [sat] + sweep
     if world > 1:
@@ -724,8 +738,9 @@ def run_served(args, rank, world, local_rank):
         "rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
                             "sample": len(errs)},
         "one_at_a_time": {"solves_per_s": 1.0 / one_per,
+                          "device_ms_per_solve": one_dev_ms,
                           "sample": f"{len(idx)} requests through svx_solve_flat (FP64) one "
-                                    "after another, wall clock",
+                                    "after another, wall clock, faster of two passes",
                           "speedup_served": sat["solves_per_s"] * one_per,
                           f"speedup_served_{other_name}": sat_other["solves_per_s"] * one_per},
         "e2e": {"value": sat["dof_iter_per_s"], "unit": UNIT,

@@ -53,6 +53,14 @@ constexpr int NODE_BLOCKS_PER_SM = 5;
 // most 64 registers a thread) for 3D members, 1,536 for the lighter 2D ones,
 // to keep enough node gathers in flight.
 constexpr int BATCH_MIN_THREADS = 1024;
+// The mixed form stops an FP32 segment as converged only once the true FP64
+// residual is below MIXED_FP32_TOL x tol (the FP64 phase stops at tol).  The
+// FP32 operator's error leaves the iterate's error in the stiffness's low
+// modes, where the residual hardly shows it: on a seeded mix of 120 plates
+// and cantilevers stopping at tol left up to 1.0e-8 relative displacement
+// error against the FP64 solve, stopping at tol / 2 up to 3.0e-9, for 5%
+// more iterations.
+constexpr double MIXED_FP32_TOL = 0.5;
 
 // ------------------------------------------------------------ reductions
 __device__ __forceinline__ double warp_sum(double v) {
@@ -1126,13 +1134,13 @@ batch_pcg_kernel(int count, const int32_t* __restrict__ order, const int64_t* __
 // Mixed form of the batched PCG: per instance, the same CG runs on the FP32
 // difference-form operator (vals32) in segments; a segment ends when its
 // recursive r.r has dropped by delta^2, after SEG_CAP iterations, or when
-// the recursive residual meets the tolerance.  The CTA then replaces r by
-// the true residual f - K u of the FP64 operator (reliable update; the
-// search direction p is kept), tests convergence on it, and switches the
-// instance to the FP64 operator, restarting CG there (p = z), once two
-// segments failed to cut the true residual 3x (continuing the FP32-built
-// search direction under the FP64 operator can stall CG for thousands of
-// iterations).  All of it is CTA-local, so every instance keeps its own
+// the recursive residual meets MIXED_FP32_TOL x the tolerance.  The CTA then
+// replaces r by the true residual f - K u of the FP64 operator (reliable
+// update; the search direction p is kept), tests convergence on it, and
+// switches the instance to the FP64 operator, restarting CG there (p = z),
+// once two segments failed to cut the true residual 3x (continuing the
+// FP32-built search direction under the FP64 operator can stall CG for
+// thousands of iterations).  All of it is CTA-local, so every instance keeps its own
 // scalars and its result does not depend on the rest of the batch.
 template <int ND, int G, int BS>
 __global__ void __launch_bounds__(BS, BATCH_MIN_THREADS / BS)
@@ -1156,7 +1164,7 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
         const int inst = order[k];
         const int64_t n0 = node_off[inst], n1 = node_off[inst + 1];
         const int64_t r0 = n0 * ND, r1 = n1 * ND;
-        const double tl = tol[inst];
+        const double tl = tol[inst], tl32 = MIXED_FP32_TOL * tl;
         const int64_t mi = max_iter[inst];
         double rr = 0.0, rz = 0.0;
         for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
@@ -1223,7 +1231,7 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
             it += 1;
             if (!exact) ++fp32_it;
             res = sqrt(rr) / bnorm;
-            if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl)) {
+            if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl32)) {
                 // reliable update: r = f - K64 u, then r.r and r.z of it
                 __syncthreads();
                 double trr = 0.0, trz = 0.0;
@@ -1262,7 +1270,7 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
                 seg_stop = DELTA2 * rr;
                 seg_start = it;
             }
-            if (res <= tl) {
+            if (res <= (exact ? tl : tl32)) {
                 status = PCG_CONVERGED;
                 break;
             }
@@ -1343,7 +1351,7 @@ batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
         const int64_t N0 = node_off[inst], N1 = node_off[inst + 1];
         const int64_t n0 = N0 + (N1 - N0) * crank / CS, n1 = N0 + (N1 - N0) * (crank + 1) / CS;
         const int64_t r0 = n0 * ND, r1 = n1 * ND;
-        const double tl = tol[inst];
+        const double tl = tol[inst], tl32 = MIXED_FP32_TOL * tl;
         const int64_t mi = max_iter[inst];
         double lrr = 0.0, lrz = 0.0;
         for (int64_t row = r0 + threadIdx.x; row < r1; row += BS) {
@@ -1435,7 +1443,7 @@ batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
             if (!exact) ++fp32_it;
             res = sqrt(rr) / bnorm;
             if constexpr (MIXED) {
-                if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl)) {
+                if (!exact && (rr <= seg_stop || it - seg_start >= SEG_CAP || res <= tl32)) {
                     // T: r = f - K64 u on own nodes (neighbours' u from L2)
                     double trr = 0.0, trz = 0.0;
                     for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1;
@@ -1481,7 +1489,7 @@ batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
                     seg_start = it;
                 }
             }
-            if (res <= tl) {
+            if (res <= (exact ? tl : tl32)) {
                 status = PCG_CONVERGED;
                 break;
             }
@@ -1968,7 +1976,8 @@ reliable_resume_kernel(int64_t n, const double* __restrict__ r64, V* __restrict_
 // difference form of compensated_fp32_kernel; on an ill-conditioned system
 // its error still slows the true residual, so once two segments failed to
 // cut it by sqrt(delta) the solve continues with the FP64 operator to the
-// tolerance, restarting CG there (p = z).  The FP32 iterations stream
+// tolerance, restarting CG there (p = z).  FP32 segments count as converged
+// at MIXED_FP32_TOL x tol of the true residual.  The FP32 iterations stream
 // 4.44 B instead of 8.44 B per nonzero.
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps) {
@@ -2040,8 +2049,10 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     };
 
     SVX_CUDA(cudaEventRecord(ctx->ev[0], st));
+    // FP32 segments converge at tol32, the FP64 phase at tol
+    const double tol32 = MIXED_FP32_TOL * tol;
     PcgScalars init{};
-    init.tol = tol;
+    init.tol = tol32;
     init.max_iter = max_iter;
     init.status = PCG_RUNNING;
     SVX_CUDA(cudaMemcpyAsync(s.p, &init, sizeof(init), cudaMemcpyHostToDevice, st));
@@ -2081,7 +2092,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         ++outer;
         const double rr_true = true_residual();
         res = std::sqrt(rr_true) / bnorm;
-        if (res <= tol) {
+        if (res <= tol32) {
             status = PCG_CONVERGED;
             break;
         }
@@ -2100,7 +2111,10 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         // entering the FP64 phase restarts CG (p = z): the FP32-built search
         // direction under the FP64 operator can stall CG for thousands of
         // iterations
-        if (fp64_phase) set_field(&PcgScalars::beta, 0.0);
+        if (fp64_phase) {
+            set_field(&PcgScalars::beta, 0.0);
+            set_field(&PcgScalars::tol, tol);
+        }
         set_field(&PcgScalars::rr, rr_true);
         set_field(&PcgScalars::res, res);
         set_field(&PcgScalars::rr_stop, fp64_phase ? -1.0 : delta * delta * rr_true);

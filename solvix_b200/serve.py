@@ -44,7 +44,7 @@ class Server:
     """A served-solve loop on one device (svx_serve_create)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 40 << 30, lanes: int = 2,
-                 max_batch: int = 4096, tol: float = 1e-10, precision: int = abi.SVX_MIXED,
+                 max_batch: int = 4096, tol: float = 1e-10, precision: int = abi.SVX_FP64,
                  max_iter: int = 0, want_stress: bool = True, max_batch_bytes: int = 0):
         self.lib = abi.load()
         opts = abi.SvxServeOpts()
@@ -203,7 +203,7 @@ def result_json(ident, r: dict) -> dict:
     }
 
 
-SOLVER_PRECISION = [abi.SVX_MIXED]
+SOLVER_PRECISION = [abi.SVX_FP64]
 
 
 def serve_json(inp, out, server: Server) -> int:
@@ -269,7 +269,7 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--lanes", type=int, default=2)
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--tol", type=float, default=1e-10)
     args = ap.parse_args(argv)
     prec = abi.SVX_MIXED if args.precision == "mixed" else abi.SVX_FP64

@@ -1,7 +1,8 @@
 """The served form (continuous batching) and the mixed batched form (GPU).
 
 Each served result must be the same alone and in a mix of concurrently
-arriving requests (within the mixed form's 1e-8 bar against FP64), a bad
+arriving requests (within 1e-10 in FP64, the default, and within the mixed
+form's 1e-8 bar against FP64 in the mixed form), a bad
 request must come back as its own failure without touching the others, and
 admission must keep the admitted device bytes under the budget.
 """
@@ -72,9 +73,10 @@ def test_mixed_single_solve_meets_fp64_bar(ctx):
     assert rel(u, ref.u) <= 1e-8
 
 
-def test_served_results_are_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("precision,bar", [(abi.SVX_FP64, 1e-10), (abi.SVX_MIXED, 1e-8)])
+def test_served_results_are_the_same_alone_and_in_the_mix(precision, bar):
     flats = mix(40, seed=71)
-    with Server(lanes=3, precision=abi.SVX_MIXED) as srv:
+    with Server(lanes=3, precision=precision) as srv:
         for k, f in enumerate(flats):
             st, msg = srv.submit(f, k)
             assert st == abi.SVX_OK, msg
@@ -84,13 +86,13 @@ def test_served_results_are_the_same_alone_and_in_the_mix():
         stats = srv.stats()
     assert stats["completed"] == len(flats) and stats["batches"] >= 2
     assert max(r["batch_size"] for r in in_mix.values()) > 1
-    with Server(lanes=1, precision=abi.SVX_MIXED) as srv:
+    with Server(lanes=1, precision=precision) as srv:
         for k in (0, 3, 17, 39):
             srv.submit(flats[k], 1000 + k)
             alone = drain(srv, 1)[1000 + k]
             assert alone["batch_size"] == 1
             assert alone["status"] == abi.SVX_OK and in_mix[k]["status"] == abi.SVX_OK
-            assert rel(in_mix[k]["u"], alone["u"]) <= 1e-8
+            assert rel(in_mix[k]["u"], alone["u"]) <= bar
     for k in (1, 2):
         ref = oracle.solve_flat(flats[k])
         assert rel(in_mix[k]["u"], ref.u) <= 1e-8
