@@ -629,6 +629,7 @@ def run_served(args, rank, world, local_rank):
     import torch
 
     from solvix_b200 import Context, abi, workloads
+    from solvix_b200.kernel_timer import pcg_iteration_bytes
     from solvix_b200.serve import Server
 
     torch.cuda.set_device(local_rank)
@@ -648,7 +649,13 @@ def run_served(args, rank, world, local_rank):
         lat = np.array([r["t_done_ms"] - r["t_submit_ms"] for r in results.values()])
         ok = [r for r in results.values() if r["status"] == 0]
         dof_it = float(sum(n_dof[r["tag"]] * r["iterations"] for r in results.values()))
+        # algorithmic bytes of every member iteration (node-block SpMV and
+        # vector streams), as in the batched form
+        alg = float(sum(r["iterations"] * pcg_iteration_bytes(
+            n_dof[r["tag"]], r["nnz"], reqs[r["tag"]].ndof, reqs[r["tag"]].n_nodes)
+            for r in ok))
         return {"solves_per_s": len(ok) / wall, "dof_iter_per_s": dof_it / wall,
+                "algorithmic_bytes": alg,
                 "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
                 "p99_ms": float(np.percentile(lat, 99)), "failed": len(results) - len(ok),
                 "mean_batch": float(np.mean([r["batch_size"] for r in results.values()])),
@@ -711,6 +718,7 @@ def run_served(args, rank, world, local_rank):
         torch.distributed.all_gather_object(gathered, rows)
         rows = [{"solves_per_s": sum(g[i]["solves_per_s"] for g in gathered),
                  "dof_iter_per_s": sum(g[i]["dof_iter_per_s"] for g in gathered),
+                 "algorithmic_bytes": sum(g[i]["algorithmic_bytes"] for g in gathered),
                  "p50_ms": max(g[i]["p50_ms"] for g in gathered),
                  "p95_ms": max(g[i]["p95_ms"] for g in gathered),
                  "p99_ms": max(g[i]["p99_ms"] for g in gathered),
@@ -721,6 +729,7 @@ def run_served(args, rank, world, local_rank):
                  "rate_per_s": rows[i]["rate_per_s"]} for i in range(len(rows))]
     sat = rows[0]
     head = rows[-1] if len(rows) > 1 else sat
+    peak, peak_kind = measured_peaks()
     line = {
         "metric": METRIC, "form": "served", "value": sat["dof_iter_per_s"], "unit": UNIT,
         "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1000 * sat["wall_s"],
@@ -748,6 +757,15 @@ def run_served(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(sum(f.nbytes() for f in reqs)),
                 "d2h_bytes_per_step": int(sum(8 * (f.n_dof + f.n_elem) for f in reqs))},
         "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel / batch_pcg_cluster_kernel "
+                     "of every lane's batches",
+                     "achieved": sat["algorithmic_bytes"] / sat["wall_s"] / 1e9,
+                     "peak": peak, "unit": "GB/s",
+                     "frac": sat["algorithmic_bytes"] / sat["wall_s"] / 1e9 / peak,
+                     "peak_source": peak_kind,
+                     "algorithmic_bytes": sat["algorithmic_bytes"],
+                     "note": "over the saturation run's wall clock, host phases included",
+                     "traffic": None},
         "clocks": clk,
     }
     return line

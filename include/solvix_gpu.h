@@ -361,6 +361,7 @@ typedef struct svx_serve_result {
     const double* u;           /* [n_nodes * ndof], owned by the result */
     const double* von_mises;   /* [n_elem] centroid von Mises (NULL if off) */
     svx_error_t error;         /* why a request failed (status != SVX_OK) */
+    int64_t nnz;               /* stored nonzeros of its K (0 if it failed before assembly) */
 } svx_serve_result_t;
 
 typedef struct svx_serve_stats {

@@ -203,6 +203,7 @@ class SvxServeResult(C.Structure):
         ("u", C.POINTER(C.c_double)),
         ("von_mises", C.POINTER(C.c_double)),
         ("error", SvxError),
+        ("nnz", C.c_int64),
     ]
 
 

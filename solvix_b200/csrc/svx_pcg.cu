@@ -1310,7 +1310,9 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
 // barrier per phase suffices.  MIXED runs the reliable-update form of
 // batch_pcg_mixed_kernel with the same rules.
 template <int ND, int G, int BS, int CS, bool MIXED>
-__global__ void __launch_bounds__(BS, (MIXED ? 768 : BATCH_MIN_THREADS) / BS)
+__global__ void __launch_bounds__(BS, (MIXED ? 768 : BATCH_MIN_THREADS) / BS > 0
+                                          ? (MIXED ? 768 : BATCH_MIN_THREADS) / BS
+                                          : 1)
 batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
                          const int64_t* __restrict__ node_off,
                          const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj,
@@ -2377,8 +2379,26 @@ int batch_default_choice(int ndof) { return ndof == 3 ? 1 : 2; }
 int64_t cluster_min_dof(int ndof) {
     return ndof == 3 ? int64_t(SVX_CLUSTER_MIN_DOF_3D) : int64_t(SVX_CLUSTER_MIN_DOF_2D);
 }
-constexpr int CLUSTER_CTAS = 8;  // the portable cluster size
-constexpr int CLUSTER_BS = 256;
+// CTAs per member cluster, threads per CTA and lanes per 3D node (build
+// constants); clusters above the portable 8 CTAs are allowed explicitly at
+// launch.  Measured on the first 200 C3D8 cantilevers of the served request
+// stream (5.48M DOF, 191 cluster members), device PCG time of one batched
+// solve: 8 x 256 626-631 ms, 8 x 512 437-441 ms, 8 x 768 499 ms, 8 x 1024
+// 469 ms, 16 x 256 460 ms, 16 x 512 502 ms, 4 x 1024 476 ms, 8 x 512 with
+// 32 lanes per node 488 ms.
+#ifndef SVX_CLUSTER_CTAS
+#define SVX_CLUSTER_CTAS 8
+#endif
+#ifndef SVX_CLUSTER_BS
+#define SVX_CLUSTER_BS 512
+#endif
+#ifndef SVX_CLUSTER_G3D
+#define SVX_CLUSTER_G3D 16
+#endif
+constexpr int CLUSTER_CTAS = SVX_CLUSTER_CTAS;
+constexpr int CLUSTER_G3D = SVX_CLUSTER_G3D;  // lanes per node of 3D members
+constexpr int CLUSTER_BS = SVX_CLUSTER_BS;
+static_assert(CLUSTER_CTAS >= 1 && CLUSTER_CTAS <= 16, "cluster size 1..16");
 
 using ClusterFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*, const int32_t*,
                            const int64_t*, const double*, const float*, const double*,
@@ -2394,11 +2414,14 @@ void launch_batch_cluster(int ndof, bool mixed, cudaStream_t st, int n_inst,
                           int32_t* out_status, int64_t* out_fp32) {
     ClusterFn fn;
     if (ndof == 3)
-        fn = mixed ? &batch_pcg_cluster_kernel<3, 16, CLUSTER_BS, CLUSTER_CTAS, true>
-                   : &batch_pcg_cluster_kernel<3, 16, CLUSTER_BS, CLUSTER_CTAS, false>;
+        fn = mixed ? &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS, CLUSTER_CTAS, true>
+                   : &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS, CLUSTER_CTAS, false>;
     else
         fn = mixed ? &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, true>
                    : &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, false>;
+    if (CLUSTER_CTAS > 8)
+        SVX_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

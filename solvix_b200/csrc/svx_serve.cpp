@@ -258,6 +258,7 @@ void svx_server::lane_loop(int lane) {
             r.iterations = o.iterations;
             r.residual = o.residual;
             r.cond_estimate = o.cond;
+            r.nnz = o.nnz;
             if (o.status != SVX_OK) {
                 fill_result_error(r, o.status, o.reason, o.elem_index, o.message);
                 r.error.iterations = o.iterations;

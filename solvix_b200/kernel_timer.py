@@ -1,7 +1,7 @@
 """Device timing of the PCG iteration kernels on a synthetic workload.
 
     python -m solvix_b200.kernel_timer [--workload c3d8_160|c3d8_480|cps4_200] [--reps N]
-                                       [--solve] [--batch N]
+                                       [--solve] [--batch N | --batch-3d N]
 
 Assembles the workload on cuda:0, then times the three FP64 iteration
 kernels (node-block SpMV + p.Kp, u/r update + dots, p update) with CUDA
@@ -10,7 +10,9 @@ duration and the SpMV's HBM throughput from its algorithmic bytes.  With
 ``--solve`` it runs one full FP64 solve instead (the persistent cooperative
 PCG kernel, one launch per chunk of iterations) and prints its device time
 and per-iteration algorithmic bytes.  With ``--batch N`` it runs one
-batched FP64 solve of the first N plates of the 4,096-plate mix.  Small and
+batched FP64 solve of the first N plates of the 4,096-plate mix, with
+``--batch-3d N`` of the first N C3D8 cantilevers of the served request
+stream (the cluster kernel's members).  Small and
 self-contained, so it is also the command to profile a single kernel with
 ncu.
 """
@@ -37,19 +39,41 @@ def main(argv=None):
     ap.add_argument("--solve", action="store_true", help="one full persistent FP64 solve")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: one batched solve of this many plates of the 4,096-plate mix")
+    ap.add_argument("--batch-3d", type=int, default=0,
+                    help="instead: one batched solve of the first this many C3D8 cantilevers "
+                         "of the served request stream")
+    ap.add_argument("--repeat", type=int, default=1, help="batched solves (the last is printed)")
+    ap.add_argument("--solo", action="store_true",
+                    help="with --batch/--batch-3d: also solve each model alone (svx_solve_flat) "
+                         "and print the summed device PCG time")
     args = ap.parse_args(argv)
-    if args.batch > 0:
-        flats = workloads.plate_batch(4096, seed=4)[:args.batch]
+    if args.batch > 0 or args.batch_3d > 0:
+        if args.batch > 0:
+            flats = workloads.plate_batch(4096, seed=4)[:args.batch]
+        else:
+            stream = workloads.request_stream(max(64, 4 * args.batch_3d), 1.0, seed=5)
+            flats = [m for _, m in stream if m.ndof == 3][:args.batch_3d]
         with Context(0) as ctx:
-            out, st = ctx.solve_batch(flats)
+            for _ in range(max(1, args.repeat)):
+                out, st = ctx.solve_batch(flats)
             its = sum(o["iterations"] for o in out)
             b = sum(o["iterations"] * pcg_iteration_bytes(f.n_dof, o["nnz"], f.ndof, f.n_nodes)
                     for f, o in zip(flats, out))
             print(json.dumps({"batch": len(flats), "total_dof": st["total_dof"],
                               "iterations": its, "pcg_ms": st["ms_solve"],
                               "threads_per_cta": st["threads_per_cta"],
-                              "lanes_per_node": st["lanes_per_node"], "algorithmic_bytes": b,
+                              "lanes_per_node": st["lanes_per_node"],
+                              "cluster_members": st["cluster_members"],
+                              "algorithmic_bytes": b,
                               "gbs": b / (st["ms_solve"] * 1e-3) / 1e9}))
+            if args.solo:
+                ms = its_solo = 0
+                for f in flats:
+                    sol = ctx.solve_flat(f, want_stress=False)
+                    ms += sol.ms_solve
+                    its_solo += sol.iterations
+                print(json.dumps({"solo_pcg_ms": ms, "solo_iterations": its_solo,
+                                  "batched_speedup": ms / st["ms_solve"]}))
         return
     flat = WORKLOADS[args.workload]()
     with Context(0) as ctx:

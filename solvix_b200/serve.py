@@ -99,6 +99,7 @@ class Server:
                               if r.von_mises and r.n_elem else None),
                 "message": r.error.message.decode() if r.status != abi.SVX_OK else "",
                 "reason": int(r.error.reason), "elem_index": int(r.error.elem_index),
+                "nnz": int(r.nnz),
             }
         finally:
             self.lib.svx_serve_result_free(out)

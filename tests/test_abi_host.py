@@ -249,3 +249,37 @@ def test_raw_flat_struct_is_byte_identical_to_the_typed_one():
         typed = f.as_struct()
         raw = abi.SvxFlatModelRaw(*f.raw_fields())
         assert C.string_at(C.addressof(typed), size) == C.string_at(C.addressof(raw), size)
+
+
+# every ctypes mirror against the C compiler's own layout of the public header
+STRUCTS = [("svx_error_t", abi.SvxError), ("svx_model_desc_t", abi.SvxModelDesc),
+           ("svx_flat_model_t", abi.SvxFlatModel), ("svx_solve_opts_t", abi.SvxSolveOpts),
+           ("svx_solution_t", abi.SvxSolution), ("svx_batch_result_t", abi.SvxBatchResult),
+           ("svx_batch_stats_t", abi.SvxBatchStats), ("svx_serve_opts_t", abi.SvxServeOpts),
+           ("svx_serve_result_t", abi.SvxServeResult), ("svx_serve_stats_t", abi.SvxServeStats)]
+
+
+def test_ctypes_mirrors_match_the_c_header_layout(tmp_path):
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "solvix_gpu.h"',
+             "int main(void) {"]
+    for cname, cls in STRUCTS:
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out.splitlines()}
+    for cname, cls in STRUCTS:
+        assert got[(cname, "sizeof")] == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
