@@ -673,6 +673,7 @@ def run_served(args, rank, world, local_rank):
         s1 = srv.stats()
         row["phases_ms"] = {k: round(s1[k] - s0[k], 1) for k in (
             "prep_ms", "assemble_ms", "solve_ms", "output_ms", "device_solve_ms", "pool_ms")}
+        row["pool_mallocs"] = int(s1["pool_mallocs"] - s0["pool_mallocs"])
         row["batches"] = int(s1["batches"] - s0["batches"])
         row["peak_bytes_admitted"] = int(s1["peak_bytes_admitted"])
         return srv, row, srv.lib.svx_launch_count() - l0

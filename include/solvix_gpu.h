@@ -341,7 +341,7 @@ typedef struct svx_serve_opts {
     int32_t max_batch;         /* requests per batch at most; 0 = 4096 */
     svx_solve_opts_t solve;    /* tolerance, precision, max_iter, want_stress */
     int64_t max_batch_bytes;   /* estimated device bytes per batch at most;
-                                  0 = a lane's arena (budget / lanes) */
+                                  0 = 4/5 of a lane's arena (budget / lanes) */
 } svx_serve_opts_t;
 
 typedef struct svx_serve_result {

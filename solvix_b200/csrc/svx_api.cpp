@@ -101,11 +101,16 @@ void DevicePool::flush_arena_cache() {
 }
 
 void* DevicePool::alloc(size_t bytes) {
+    // cached blocks up to 25% larger are reused; the arena is carved at the
+    // 512 B-aligned size (a size class's slack there would make a batch that
+    // the admission estimate fits overflow the arena); a driver allocation
+    // takes the size class, so that later sizes of the class reuse it
+    const size_t exact = (std::max<size_t>(bytes, 1) + 511) & ~size_t(511);
     const size_t want = round_bytes(bytes);
     {
         std::lock_guard<std::mutex> lk(mu_);
-        auto it = free_.lower_bound(want);
-        if (it != free_.end() && it->first <= want + want / 4) {
+        auto it = free_.lower_bound(exact);
+        if (it != free_.end() && it->first <= exact + exact / 4) {
             void* p = it->second;
             free_.erase(it);
             cached_ -= sizes_[p];
@@ -113,14 +118,14 @@ void* DevicePool::alloc(size_t bytes) {
             return p;
         }
         if (arena_) {
-            void* p = carve(want);
+            void* p = carve(exact);
             if (!p) {  // cached arena blocks of other sizes go back, coalesced
                 flush_arena_cache();
-                p = carve(want);
+                p = carve(exact);
             }
             if (p) {
-                sizes_[p] = want;
-                in_use_ += want;
+                sizes_[p] = exact;
+                in_use_ += exact;
                 return p;
             }
         }

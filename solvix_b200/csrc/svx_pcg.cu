@@ -1309,10 +1309,15 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
 // and every slot is rewritten only after a later cluster barrier, so one
 // barrier per phase suffices.  MIXED runs the reliable-update form of
 // batch_pcg_mixed_kernel with the same rules.
+#ifndef SVX_CLUSTER_MIXED_MIN_THREADS
+#define SVX_CLUSTER_MIXED_MIN_THREADS 768
+#endif
+constexpr int CLUSTER_MIXED_MIN_THREADS = SVX_CLUSTER_MIXED_MIN_THREADS;
 template <int ND, int G, int BS, int CS, bool MIXED>
-__global__ void __launch_bounds__(BS, (MIXED ? 768 : BATCH_MIN_THREADS) / BS > 0
-                                          ? (MIXED ? 768 : BATCH_MIN_THREADS) / BS
-                                          : 1)
+__global__ void __launch_bounds__(
+    BS, (MIXED ? CLUSTER_MIXED_MIN_THREADS : BATCH_MIN_THREADS) / BS > 0
+            ? (MIXED ? CLUSTER_MIXED_MIN_THREADS : BATCH_MIN_THREADS) / BS
+            : 1)
 batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
                          const int64_t* __restrict__ node_off,
                          const int64_t* __restrict__ adj_ptr, const int32_t* __restrict__ adj,
@@ -2358,7 +2363,8 @@ std::vector<BatchMixedConfig> batch_mixed_candidates(int ndof) {
     if (ndof == 3)
         return {batch_mixed_config<3, 16, 128>(), batch_mixed_config<3, 16, 256>(),
                 batch_mixed_config<3, 16, 512>(), batch_mixed_config<3, 32, 256>(),
-                batch_mixed_config<3, 32, 512>()};
+                batch_mixed_config<3, 32, 512>(), batch_mixed_config<3, 8, 256>(),
+                batch_mixed_config<3, 8, 512>()};
     return {batch_mixed_config<2, 8, 128>(), batch_mixed_config<2, 8, 256>(),
             batch_mixed_config<2, 8, 512>(), batch_mixed_config<2, 16, 256>(),
             batch_mixed_config<2, 16, 512>()};
@@ -2383,9 +2389,11 @@ int64_t cluster_min_dof(int ndof) {
 // constants); clusters above the portable 8 CTAs are allowed explicitly at
 // launch.  Measured on the first 200 C3D8 cantilevers of the served request
 // stream (5.48M DOF, 191 cluster members), device PCG time of one batched
-// solve: 8 x 256 626-631 ms, 8 x 512 437-441 ms, 8 x 768 499 ms, 8 x 1024
-// 469 ms, 16 x 256 460 ms, 16 x 512 502 ms, 4 x 1024 476 ms, 8 x 512 with
-// 32 lanes per node 488 ms.
+// solve with 16 lanes per node: 8 x 256 626-631 ms, 8 x 512 437-441 ms,
+// 8 x 768 499 ms, 8 x 1024 469 ms, 16 x 256 460 ms, 16 x 512 502 ms,
+// 4 x 1024 476 ms (32 lanes at 8 x 512: 488 ms); with 8 lanes per node
+// 8 x 512 394 ms (4.36 TB/s algorithmic), 8 x 256 534 ms, 8 x 1024 429 ms,
+// 16 x 512 459 ms, and 4 lanes at 8 x 512 396 ms.
 #ifndef SVX_CLUSTER_CTAS
 #define SVX_CLUSTER_CTAS 8
 #endif
@@ -2393,11 +2401,17 @@ int64_t cluster_min_dof(int ndof) {
 #define SVX_CLUSTER_BS 512
 #endif
 #ifndef SVX_CLUSTER_G3D
-#define SVX_CLUSTER_G3D 16
+#define SVX_CLUSTER_G3D 8
 #endif
 constexpr int CLUSTER_CTAS = SVX_CLUSTER_CTAS;
 constexpr int CLUSTER_G3D = SVX_CLUSTER_G3D;  // lanes per node of 3D members
 constexpr int CLUSTER_BS = SVX_CLUSTER_BS;
+// the mixed form's cluster kernel carries the reliable-update state in
+// more registers; it keeps 256-thread CTAs
+#ifndef SVX_CLUSTER_BS_MIXED
+#define SVX_CLUSTER_BS_MIXED 256
+#endif
+constexpr int CLUSTER_BS_MIXED = SVX_CLUSTER_BS_MIXED;
 static_assert(CLUSTER_CTAS >= 1 && CLUSTER_CTAS <= 16, "cluster size 1..16");
 
 using ClusterFn = void (*)(int, const int32_t*, const int64_t*, const int64_t*, const int32_t*,
@@ -2414,10 +2428,11 @@ void launch_batch_cluster(int ndof, bool mixed, cudaStream_t st, int n_inst,
                           int32_t* out_status, int64_t* out_fp32) {
     ClusterFn fn;
     if (ndof == 3)
-        fn = mixed ? &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS, CLUSTER_CTAS, true>
-                   : &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS, CLUSTER_CTAS, false>;
+        fn = mixed
+                 ? &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS_MIXED, CLUSTER_CTAS, true>
+                 : &batch_pcg_cluster_kernel<3, CLUSTER_G3D, CLUSTER_BS, CLUSTER_CTAS, false>;
     else
-        fn = mixed ? &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, true>
+        fn = mixed ? &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS_MIXED, CLUSTER_CTAS, true>
                    : &batch_pcg_cluster_kernel<2, 8, CLUSTER_BS, CLUSTER_CTAS, false>;
     if (CLUSTER_CTAS > 8)
         SVX_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
@@ -2428,7 +2443,7 @@ void launch_batch_cluster(int ndof, bool mixed, cudaStream_t st, int n_inst,
     attr[0].val.clusterDim.x = CLUSTER_CTAS;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(CLUSTER_BS);
+    cfg.blockDim = dim3(mixed ? CLUSTER_BS_MIXED : CLUSTER_BS);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cfg.attrs = attr;
@@ -2443,7 +2458,8 @@ void launch_batch_cluster(int ndof, bool mixed, cudaStream_t st, int n_inst,
 std::vector<BatchConfig> batch_candidates(int ndof) {
     if (ndof == 3)
         return {batch_config<3, 16, 128>(), batch_config<3, 16, 256>(), batch_config<3, 16, 512>(),
-                batch_config<3, 32, 256>(), batch_config<3, 32, 512>()};
+                batch_config<3, 32, 256>(), batch_config<3, 32, 512>(), batch_config<3, 8, 256>(),
+                batch_config<3, 8, 512>()};
     return {batch_config<2, 8, 128>(), batch_config<2, 8, 256>(), batch_config<2, 8, 512>(),
             batch_config<2, 16, 256>(), batch_config<2, 16, 512>()};
 }

@@ -159,14 +159,18 @@ void fill_result_error(svx_serve_result_t& r, int code, int reason, int64_t elem
 void svx_server::lane_loop(int lane) {
     svx_ctx* ctx = lane_ctx[lane];
     DevicePool* pool = ctx->pool;
-    // a batch takes at most the lane's arena (estimated bytes; blocks that
-    // fragmentation leaves no room for fall back to cudaMalloc).  Measured
-    // on 6,000 requests of the serving mix (FP64, solves/s): 2 lanes with
-    // whole-arena batches 960, with half-arena batches 650; 4 lanes 725 /
-    // 537: larger batches fill the device better than more lanes do.
+    // a batch takes at most 4/5 of the lane's arena in estimated bytes: the
+    // rest absorbs fragmentation, so that no block falls back to cudaMalloc
+    // and the device-synchronising cudaFree of the trim below.  Measured on
+    // 6,000 requests of the serving mix (FP64, solves/s): 2 lanes with 4/5
+    // arena batches 1,078 (no pool time), whole-arena 969 (0.8 s in the
+    // driver's allocator), half-arena 650; 3 lanes whole-arena 939, 4 lanes
+    // 725 / 537 (whole / half): large batches on two lanes fill the device
+    // best.
     const int64_t lane_cap =
-        opts.max_batch_bytes > 0 ? opts.max_batch_bytes
-                                 : std::max<int64_t>(1, opts.hbm_budget_bytes / opts.lanes);
+        opts.max_batch_bytes > 0
+            ? opts.max_batch_bytes
+            : std::max<int64_t>(1, opts.hbm_budget_bytes / opts.lanes / 5 * 4);
     cudaSetDevice(device);
     for (;;) {
         std::vector<Request> batch;

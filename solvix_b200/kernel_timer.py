@@ -21,7 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 
-from . import workloads
+from . import abi, workloads
 from .core import Context
 
 WORKLOADS = {
@@ -43,6 +43,8 @@ def main(argv=None):
                     help="instead: one batched solve of the first this many C3D8 cantilevers "
                          "of the served request stream")
     ap.add_argument("--repeat", type=int, default=1, help="batched solves (the last is printed)")
+    ap.add_argument("--mixed", action="store_true",
+                    help="with --batch/--batch-3d: the mixed form instead of FP64")
     ap.add_argument("--solo", action="store_true",
                     help="with --batch/--batch-3d: also solve each model alone (svx_solve_flat) "
                          "and print the summed device PCG time")
@@ -55,7 +57,8 @@ def main(argv=None):
             flats = [m for _, m in stream if m.ndof == 3][:args.batch_3d]
         with Context(0) as ctx:
             for _ in range(max(1, args.repeat)):
-                out, st = ctx.solve_batch(flats)
+                out, st = ctx.solve_batch(
+                    flats, precision=abi.SVX_MIXED if args.mixed else abi.SVX_FP64)
             its = sum(o["iterations"] for o in out)
             b = sum(o["iterations"] * pcg_iteration_bytes(f.n_dof, o["nnz"], f.ndof, f.n_nodes)
                     for f, o in zip(flats, out))
