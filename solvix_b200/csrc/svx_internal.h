@@ -200,8 +200,8 @@ enum { PCG_RUNNING = 0, PCG_CONVERGED = 1, PCG_BREAKDOWN = 2, PCG_MAXITER = 3,
 
 // State of the bounded grid-wide barrier of the persistent PCG kernel.
 struct GridBarrier {
-    unsigned int count;  // blocks arrived at the current barrier
-    unsigned int gen;    // barrier generation
+    unsigned int count;  // arrivals in this launch (zeroed by the host before each launch)
+    unsigned int gen;    // unused
     int error;           // 1 after a bounded spin gave up
     int pad;
 };

@@ -644,33 +644,45 @@ __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr
 }
 
 // Bounded grid-wide barrier (all blocks co-resident: cooperative launch).
+// gb->count only grows during a launch (the host zeroes it before each
+// launch); every block keeps its own running target, nblocks more per
+// barrier.  After bar.sync, thread 0 arrives with a gpu-scope release add
+// (cumulative over the block's writes ordered before it by the bar.sync)
+// and polls with acquire loads until the count reaches the target; the
+// closing bar.sync passes that on to the block.  A block that polls
+// spin_limit times raises gb->error and returns false, and so does a block
+// that finds the flag raised by another while it waits.
+__device__ __forceinline__ void barrier_arrive(unsigned int* p) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+__device__ __forceinline__ unsigned int barrier_count(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks,
+                                          unsigned int& target,
                                           long long spin_limit = BARRIER_SPIN_LIMIT) {
     __shared__ int ok;
-    __threadfence();
+    target += nblocks;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = &gb->gen;
-        const unsigned int g = *vgen;
         int good = 1;
-        const unsigned int arrived = atomicAdd(&gb->count, 1u);
-        if (arrived == nblocks - 1) {
-            gb->count = 0;
-            __threadfence();
-            atomicAdd(&gb->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*vgen == g) {
-                if (++spins > spin_limit) {
-                    atomicExch(&gb->error, 1);
-                    good = 0;
-                    break;
-                }
-                __nanosleep(32);
+        barrier_arrive(&gb->count);
+        long long spins = 0;
+        while (barrier_count(&gb->count) < target) {
+            if (++spins > spin_limit) {
+                atomicExch(&gb->error, 1);
+                good = 0;
+                break;
             }
+            if ((spins & 255) == 0 && *((volatile int*)&gb->error) != 0) {
+                good = 0;
+                break;
+            }
+            __nanosleep(32);
         }
-        __threadfence();
-        ok = good && (*((volatile int*)&gb->error) == 0);
+        ok = good;
     }
     __syncthreads();
     return ok != 0;
@@ -694,6 +706,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                       PcgScalars* s, GridBarrier* gb, int chunk) {
     __shared__ double sh[32];
     const unsigned int B = gridDim.x;
+    unsigned int bar_target = 0;  // grid_sync's running arrival target
     const int64_t nb0 = n_nodes * int64_t(blockIdx.x) / B;
     const int64_t nb1 = n_nodes * int64_t(blockIdx.x + 1) / B;
     const int64_t r0 = nb0 * ND, r1 = nb1 * ND;
@@ -729,7 +742,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         }
         double bs = block_sum(dot, sh);
         if (threadIdx.x == 0) part_a[blockIdx.x] = bs;
-        if (!grid_sync(gb, B)) return;
+        if (!grid_sync(gb, B, bar_target)) return;
         const double pap = sum_partials_cg(part_a, int(B), 1, 0, sh);
         if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
             if (writer) {
@@ -762,7 +775,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
             part_b[2 * blockIdx.x] = brr;
             part_b[2 * blockIdx.x + 1] = brz;
         }
-        if (!grid_sync(gb, B)) return;
+        if (!grid_sync(gb, B, bar_target)) return;
         const double rr_new = sum_partials_cg(part_b, int(B), 2, 0, sh);
         const double rz_new = sum_partials_cg(part_b, int(B), 2, 1, sh);
         it += 1;
@@ -788,7 +801,7 @@ pcg_persistent_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         const V bt = V(beta);
         for (int64_t row = r0 + threadIdx.x; row < r1; row += PBLOCK)
             p[row] = __ldcg(r + row) * inv_diag[row] + bt * __ldcg(p + row);
-        if (!grid_sync(gb, B)) return;
+        if (!grid_sync(gb, B, bar_target)) return;
     }
     if (writer) {
         s->it = it;
@@ -873,6 +886,7 @@ pcg_persistent2_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
                        GridBarrier* gb, int chunk) {
     __shared__ double sh[32];
     const unsigned int B = gridDim.x;
+    unsigned int bar_target = 0;  // grid_sync's running arrival target
     const int64_t nb0 = n_nodes * int64_t(blockIdx.x) / B;
     const int64_t nb1 = n_nodes * int64_t(blockIdx.x + 1) / B;
     const int64_t r0 = nb0 * ND, r1 = nb1 * ND;
@@ -916,7 +930,7 @@ pcg_persistent2_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         }
         double bs = block_sum(dot, sh);
         if (threadIdx.x == 0) part_a[blockIdx.x] = bs;
-        if (!grid_sync(gb, B)) return;
+        if (!grid_sync(gb, B, bar_target)) return;
         const double pap = sum_partials_cg(part_a, int(B), 1, 0, sh);
         if (!(pap > 0.0)) {  // pap <= 0 or NaN: breakdown
             if (writer) {
@@ -949,7 +963,7 @@ pcg_persistent2_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
             part_b[2 * blockIdx.x] = brr;
             part_b[2 * blockIdx.x + 1] = brz;
         }
-        if (!grid_sync(gb, B)) return;
+        if (!grid_sync(gb, B, bar_target)) return;
         const double rr_new = sum_partials_cg(part_b, int(B), 2, 0, sh);
         const double rz_new = sum_partials_cg(part_b, int(B), 2, 1, sh);
         it += 1;
@@ -1312,11 +1326,15 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
 #ifndef SVX_CLUSTER_MIXED_MIN_THREADS
 #define SVX_CLUSTER_MIXED_MIN_THREADS 768
 #endif
+#ifndef SVX_CLUSTER_MIN_THREADS
+#define SVX_CLUSTER_MIN_THREADS 1024
+#endif
 constexpr int CLUSTER_MIXED_MIN_THREADS = SVX_CLUSTER_MIXED_MIN_THREADS;
+constexpr int CLUSTER_MIN_THREADS = SVX_CLUSTER_MIN_THREADS;
 template <int ND, int G, int BS, int CS, bool MIXED>
 __global__ void __launch_bounds__(
-    BS, (MIXED ? CLUSTER_MIXED_MIN_THREADS : BATCH_MIN_THREADS) / BS > 0
-            ? (MIXED ? CLUSTER_MIXED_MIN_THREADS : BATCH_MIN_THREADS) / BS
+    BS, (MIXED ? CLUSTER_MIXED_MIN_THREADS : CLUSTER_MIN_THREADS) / BS > 0
+            ? (MIXED ? CLUSTER_MIXED_MIN_THREADS : CLUSTER_MIN_THREADS) / BS
             : 1)
 batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
                          const int64_t* __restrict__ node_off,
@@ -1697,6 +1715,8 @@ struct PcgRun {
             if (launch >= launches_max)
                 throw ModelFail{SVX_CUDA_ERROR, 0, -1,
                                 "PCG status did not leave RUNNING within max_iter"};
+            // the barrier's arrival count starts from zero in every launch
+            SVX_CUDA(cudaMemsetAsync(&gbp->count, 0, sizeof(unsigned int), st));
             SVX_CUDA(cudaLaunchCooperativeKernel(fn, dim3(B), dim3(PBLOCK), args, 0, st));
             g_launches.fetch_add(1, std::memory_order_relaxed);
             SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
@@ -2641,7 +2661,8 @@ namespace {
 // One block meets a barrier that expects two: nothing ever releases it, so
 // the wait must run out, raise the error flag and return.
 __global__ void barrier_timeout_kernel(GridBarrier* gb, long long spin_limit, int* out) {
-    const bool ok = grid_sync(gb, 2u, spin_limit);
+    unsigned int target = 0;
+    const bool ok = grid_sync(gb, 2u, target, spin_limit);
     if (threadIdx.x == 0) out[0] = ok ? 1 : 0;
 }
 

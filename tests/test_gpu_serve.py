@@ -124,6 +124,8 @@ def test_served_bad_request_does_not_affect_the_others():
     for k in range(6):
         assert got[k]["status"] == abi.SVX_OK
         assert rel(got[k]["u"], alone[k]["u"]) <= 1e-12
+        # the member's own nonzero count, the same alone and in the batch
+        assert got[k]["nnz"] == alone[k]["nnz"] > 0
 
 
 def test_served_admission_keeps_within_the_budget():
