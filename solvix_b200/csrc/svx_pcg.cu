@@ -586,7 +586,10 @@ __global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restri
 // per node for 3D models (2D models use 16).  Measured on the 160x16x16
 // C3D8 case (us per iteration): 512 x 2 with 32 lanes 34.9, with 16 lanes
 // 39.2, with 8 lanes 36.6; 1024 x 1 35.6-37.5; 256 x 4 41.9; 256 x 6 47.7;
-// 128 x 8 54.7 (more CTAs make every grid barrier dearer).
+// 128 x 8 54.7 (more CTAs make every grid barrier dearer).  With the
+// release/acquire barrier below: 512 x 2 with 32 lanes 30.5-30.7, with 16
+// lanes 36.0; 1024 x 1 30.8; 256 x 4 33.4; a poll back-off of 0, 32 or
+// 100 ns the same.
 #ifndef SVX_PBLOCK
 #define SVX_PBLOCK 512
 #endif
@@ -599,6 +602,10 @@ __global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restri
 constexpr int PBLOCK = SVX_PBLOCK;
 constexpr int PBLOCKS_PER_SM = SVX_PBLOCKS_PER_SM;
 constexpr long long BARRIER_SPIN_LIMIT = 1LL << 25;
+// back-off between two polls of a grid barrier's arrival count
+#ifndef SVX_BARRIER_SLEEP_NS
+#define SVX_BARRIER_SLEEP_NS 32
+#endif
 
 template <int ND, int G, class M, class V>
 __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr,
@@ -680,7 +687,9 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks,
                 good = 0;
                 break;
             }
-            __nanosleep(32);
+#if SVX_BARRIER_SLEEP_NS > 0
+            __nanosleep(SVX_BARRIER_SLEEP_NS);
+#endif
         }
         ok = good;
     }
