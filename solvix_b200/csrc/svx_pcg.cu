@@ -2396,7 +2396,8 @@ std::vector<BatchMixedConfig> batch_mixed_candidates(int ndof) {
                 batch_mixed_config<3, 8, 512>()};
     return {batch_mixed_config<2, 8, 128>(), batch_mixed_config<2, 8, 256>(),
             batch_mixed_config<2, 8, 512>(), batch_mixed_config<2, 16, 256>(),
-            batch_mixed_config<2, 16, 512>()};
+            batch_mixed_config<2, 16, 512>(), batch_mixed_config<2, 4, 256>(),
+            batch_mixed_config<2, 4, 512>()};
 }
 
 int batch_default_choice(int ndof) { return ndof == 3 ? 1 : 2; }
@@ -2490,7 +2491,8 @@ std::vector<BatchConfig> batch_candidates(int ndof) {
                 batch_config<3, 32, 256>(), batch_config<3, 32, 512>(), batch_config<3, 8, 256>(),
                 batch_config<3, 8, 512>()};
     return {batch_config<2, 8, 128>(), batch_config<2, 8, 256>(), batch_config<2, 8, 512>(),
-            batch_config<2, 16, 256>(), batch_config<2, 16, 512>()};
+            batch_config<2, 16, 256>(), batch_config<2, 16, 512>(), batch_config<2, 4, 256>(),
+            batch_config<2, 4, 512>()};
 }
 
 }  // namespace
