@@ -9,6 +9,7 @@
 #include <mutex>
 #include <thread>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -836,6 +837,11 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         std::unique_ptr<svx_ctx> ctx(new svx_ctx());
         ctx->device = device;
         ctx->sm_count = prop.multiProcessorCount;
+        if (const char* e = std::getenv("SVX_SHARED_ADJ_MAX")) {
+            char* end = nullptr;
+            const long long v = std::strtoll(e, &end, 10);
+            if (end != e && v >= 0) ctx->shared_adj_max = v;
+        }
         // the main stream (uploads, assembly, stress, plain solves) has the
         // highest priority; the long batched PCG kernels run on the lowest,
         // so a served lane's assembly gets SMs while another lane's batch

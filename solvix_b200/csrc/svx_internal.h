@@ -172,6 +172,10 @@ struct svx_ctx {
     std::string last_error;
     cudaEvent_t ev[8] = {};
     void* h_scalars = nullptr;  // page-locked PcgScalars of the context's solves
+    // largest per-block shared-memory adjacency of the persistent PCG kernels
+    // (bytes; 0 keeps it in global memory); SVX_SHARED_ADJ_MAX in the
+    // environment at svx_ctx_create overrides the build's default
+    long long shared_adj_max = -1;
 };
 
 namespace svx {

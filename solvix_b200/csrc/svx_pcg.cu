@@ -1794,7 +1794,8 @@ struct PcgRun {
         // blocks per SM
         int nodes_cap = int((op->n_nodes + B - 1) / B);
         size_t smem = shared_adj_bytes(nodes_cap, op->pat.max_deg);
-        if (smem <= size_t(SHARED_ADJ_MAX)) {
+        const long long adj_max = ctx->shared_adj_max >= 0 ? ctx->shared_adj_max : SHARED_ADJ_MAX;
+        if (smem <= size_t(adj_max)) {
             void* fs = pick(true);
             if (smem > 48 * 1024)
                 SVX_CUDA(cudaFuncSetAttribute(fs, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -260,6 +260,25 @@ def test_runs_are_bitwise_deterministic(ctx):
     assert np.array_equal(bits(a.von_mises), bits(b.von_mises))
 
 
+@pytest.mark.parametrize("precision", [abi.SVX_FP64, abi.SVX_MIXED])
+def test_shared_and_global_adjacency_agree_bitwise(ctx, monkeypatch, precision):
+    """The persistent kernels with each block's adjacency in shared memory
+    (the default at these sizes) and in global memory (SVX_SHARED_ADJ_MAX=0
+    when the context is created) do the same arithmetic in the same order."""
+    from solvix_b200 import Context
+    flats = [workloads.cantilever_c3d8(16, 4, 4, lx=1.6, ly=0.4, lz=0.4, seed=9),
+             workloads.cantilever_cps4(60, 8, seed=3)]
+    monkeypatch.setenv("SVX_SHARED_ADJ_MAX", "0")
+    with Context(0) as plain_ctx:
+        monkeypatch.delenv("SVX_SHARED_ADJ_MAX")
+        for flat in flats:
+            a = ctx.solve_flat(flat, precision=precision)
+            b = plain_ctx.solve_flat(flat, precision=precision)
+            assert a.iterations == b.iterations
+            assert np.array_equal(bits(a.u), bits(b.u))
+            assert np.array_equal(bits(a.von_mises), bits(b.von_mises))
+
+
 def test_mixed_precision_meets_1e8(ctx):
     flat = workloads.cantilever_c3d8(24, 4, 4, lx=1.2, ly=0.2, lz=0.2, seed=2)
     ref = oracle.solve_flat(flat)
