@@ -166,7 +166,8 @@ void svx_server::lane_loop(int lane) {
     // arena batches 1,078 (no pool time), whole-arena 969 (0.8 s in the
     // driver's allocator), half-arena 650; 3 lanes whole-arena 939, 4 lanes
     // 725 / 537 (whole / half): large batches on two lanes fill the device
-    // best.
+    // best.  With 4/5 batches and the faster batched kernels: 2 lanes 1,116,
+    // 3 lanes 1,106, 4 lanes 1,008.
     const int64_t lane_cap =
         opts.max_batch_bytes > 0
             ? opts.max_batch_bytes
