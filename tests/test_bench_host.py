@@ -1,0 +1,52 @@
+"""bench.py's host side (no GPU): the reference arm's JSON line and the
+readers of the peak and ncu-traffic figures that the GPU arm's roofline
+uses."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_traffic_reader_takes_the_profile_figure():
+    per_iteration = bench.ncu_traffic()
+    assert per_iteration is not None
+    with open(bench.TRAFFIC_FILE) as fh:
+        line = next(l for l in fh if l.startswith("dram_bytes_per_iteration:"))
+    assert per_iteration == float(line.split(":", 1)[1].split()[0])
+    # DRAM bytes of an L2-resident iteration stay below its algorithmic bytes
+    assert 0 < per_iteration < 104149180
+
+
+def test_peak_reader_falls_back_or_reads_the_measured_file():
+    peak, kind = bench.measured_peaks()
+    assert kind in ("measured", "fallback")
+    if kind == "fallback":
+        assert peak == bench.HBM_FALLBACK_GBS
+    assert peak > 1000.0
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_prints_one_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
+                         timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["value"] > 0 and d["higher_is_better"] is True
+    assert d["steps"] == 1 and d["warmup"] == 0 and d["n_gpus"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert "workload" in d["config"]
