@@ -13,9 +13,10 @@
 // by that lane's queued kernels, so it is reused only on that lane's
 // streams).  Each lane's pool reserves budget / lanes as its arena.  A free
 // lane takes every waiting request, in arrival order, that has the ndof of
-// the oldest one, until max_batch, until its batch would exceed its arena,
-// or until the next one's estimated device bytes do not fit what is left of
-// the admission budget; it then solves them as one
+// the oldest one, until max_batch, until its batch would exceed
+// max_batch_bytes (default 4/5 of its arena), or until the next one's
+// estimated device bytes do not fit what is left of the admission budget;
+// it then solves them as one
 // block-diagonal batch (run_batch: per-model checks, per-model convergence,
 // a failed member isolated from the others) and publishes one result per
 // request.  While one lane's batch runs, other lanes start the requests
