@@ -40,6 +40,7 @@ METRIC = "PCG DOF-iters/s & solves/s: mixed/batched vs FP64 at 1e-8 err; p50/p99
 UNIT = "DOF*iter/s"
 HBM_FALLBACK_GBS = 6650.0
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "pcg_persistent_fp64_c3d8_160x16x16.txt")
+BATCH_TRAFFIC_FILE = os.path.join(ROOT, "profiles", "batch_pcg_fp64_plates4096_dram.txt")
 
 
 def parse_args():
@@ -85,16 +86,25 @@ def measured_peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per iteration of the persistent PCG kernel (ncu summary)."""
+def _profile_figure(path, key):
     try:
-        with open(TRAFFIC_FILE) as fh:
+        with open(path) as fh:
             for line in fh:
-                if line.startswith("dram_bytes_per_iteration:"):
+                if line.startswith(key + ":"):
                     return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None
+
+
+def ncu_traffic():
+    """DRAM bytes per iteration of the persistent PCG kernel (ncu summary)."""
+    return _profile_figure(TRAFFIC_FILE, "dram_bytes_per_iteration")
+
+
+def batch_ncu_traffic():
+    """DRAM bytes of the full 4,096-plate FP64 batch launch (ncu summary)."""
+    return _profile_figure(BATCH_TRAFFIC_FILE, "dram_bytes_per_launch")
 
 
 class ClockSampler:
@@ -494,7 +504,10 @@ def run_batched(args, rank, world, local_rank):
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": int(bytes_alg),
-                     "launch_ms": solve_ms, "traffic": None},
+                     "launch_ms": solve_ms,
+                     # the ncu capture covers the whole 4,096-plate FP64 launch on one GPU
+                     "traffic": (batch_ncu_traffic()
+                                 if world == 1 and prec == abi.SVX_FP64 else None)},
         "clocks": clk,
     }
     if rank == 0:

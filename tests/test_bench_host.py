@@ -24,6 +24,15 @@ def test_traffic_reader_takes_the_profile_figure():
     assert 0 < per_iteration < 104149180
 
 
+def test_batch_traffic_reader_takes_the_full_launch_figure():
+    traffic = bench.batch_ncu_traffic()
+    assert traffic is not None
+    with open(bench.BATCH_TRAFFIC_FILE) as fh:
+        alg = next(float(l.split(":", 1)[1].split()[0]) for l in fh
+                   if l.startswith("algorithmic_bytes_per_launch:"))
+    assert 0.5 * alg < traffic < 1.5 * alg
+
+
 def test_peak_reader_falls_back_or_reads_the_measured_file():
     peak, kind = bench.measured_peaks()
     assert kind in ("measured", "fallback")
