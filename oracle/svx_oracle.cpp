@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -652,11 +653,175 @@ int material_check(const svx_flat_model_t* m, int64_t e) {
     return 0;
 }
 
+// ---------------------------------------------------------------- conduction
+// heat.rs:140-145: CPS3 constant-gradient ingredients (b_i, c_i, signed 2A).
+void tri_constants(const double p[3][2], double b[3], double c[3], double* two_a) {
+    b[0] = p[1][1] - p[2][1];
+    b[1] = p[2][1] - p[0][1];
+    b[2] = p[0][1] - p[1][1];
+    c[0] = p[2][0] - p[1][0];
+    c[1] = p[0][0] - p[2][0];
+    c[2] = p[1][0] - p[0][0];
+    *two_a = b[0] * c[1] - b[1] * c[0];
+}
+
+// element.rs:175-182
+void quad_shapes(double xi, double eta, double n[4]) {
+    for (int i = 0; i < 4; ++i)
+        n[i] = 0.25 * (1.0 + xi * QUAD_CORNERS[i][0]) * (1.0 + eta * QUAD_CORNERS[i][1]);
+}
+
+// element.rs:525-531
+void hex_shapes(double xi, double eta, double zeta, double n[8]) {
+    for (int i = 0; i < 8; ++i)
+        n[i] = 0.125 * (1.0 + xi * HEX_CORNERS[i][0]) * (1.0 + eta * HEX_CORNERS[i][1]) *
+               (1.0 + zeta * HEX_CORNERS[i][2]);
+}
+
+// heat.rs:149-296 (conduction_element) for CPS3, CPS4 / CPE4 and C3D8:
+// C_e into ke (row-major N x N) and the consistent heat-source load into fe.
+// fe_used is false when the reference adds nothing to f for this element
+// (CPS3 without a source); otherwise it adds fe, zeros included.
+int conduction_ke(int kind, const double* coords, double k, double t, bool has_q, double q,
+                  double* ke, double* fe, bool* fe_used) {
+    const double qq = has_q ? q : 0.0;
+    if (kind == SVX_CPS3) {
+        double p[3][2], b[3], c[3], two_a;
+        for (int i = 0; i < 3; ++i) {
+            p[i][0] = coords[3 * i];
+            p[i][1] = coords[3 * i + 1];
+        }
+        tri_constants(p, b, c, &two_a);
+        if (two_a == 0.0) return SVX_REASON_DEGENERATE_TRI;
+        const double w = k * t / (2.0 * std::fabs(two_a));
+        for (int i = 0; i < 3; ++i) {
+            fe[i] = has_q ? q * t * std::fabs(two_a) / 6.0 : 0.0;
+            for (int j = 0; j < 3; ++j) ke[i * 3 + j] = w * (b[i] * b[j] + c[i] * c[j]);
+        }
+        *fe_used = has_q;
+        return 0;
+    }
+    if (kind == SVX_CPS4 || kind == SVX_CPE4) {
+        double xy[4][2];
+        for (int i = 0; i < 4; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        const double g = 1.0 / std::sqrt(3.0);
+        const double pts[2] = {-g, g};
+        for (int i = 0; i < 16; ++i) ke[i] = 0.0;
+        for (int i = 0; i < 4; ++i) fe[i] = 0.0;
+        for (double xi : pts)
+            for (double eta : pts) {
+                double bm[3][8], detj;
+                if (!quad_b(xy, xi, eta, bm, &detj)) return SVX_REASON_BAD_JACOBIAN;
+                double n[4];
+                quad_shapes(xi, eta, n);
+                for (int i = 0; i < 4; ++i) {
+                    fe[i] += qq * t * detj * n[i];
+                    for (int j = 0; j < 4; ++j)
+                        ke[i * 4 + j] += k * t * detj *
+                                         (bm[0][2 * i] * bm[0][2 * j] +
+                                          bm[1][2 * i + 1] * bm[1][2 * j + 1]);
+                }
+            }
+        *fe_used = true;
+        return 0;
+    }
+    if (kind == SVX_C3D8) {
+        double xyz[8][3];
+        for (int i = 0; i < 8; ++i)
+            for (int a = 0; a < 3; ++a) xyz[i][a] = coords[3 * i + a];
+        const double g = 1.0 / std::sqrt(3.0);
+        const double pts[2] = {-g, g};
+        for (int i = 0; i < 64; ++i) ke[i] = 0.0;
+        for (int i = 0; i < 8; ++i) fe[i] = 0.0;
+        for (double xi : pts)
+            for (double eta : pts)
+                for (double zeta : pts) {
+                    double bm[6][24], detj;
+                    if (!hex_b(xyz, xi, eta, zeta, bm, &detj)) return SVX_REASON_BAD_JACOBIAN;
+                    double n[8];
+                    hex_shapes(xi, eta, zeta, n);
+                    for (int i = 0; i < 8; ++i) {
+                        fe[i] += qq * detj * n[i];
+                        for (int j = 0; j < 8; ++j) {
+                            double v = 0.0;
+                            for (int r = 0; r < 3; ++r) v += bm[r][3 * i + r] * bm[r][3 * j + r];
+                            ke[i * 8 + j] += k * detj * v;
+                        }
+                    }
+                }
+        *fe_used = true;
+        return 0;
+    }
+    return SVX_REASON_UNSUPPORTED_KIND;
+}
+
+// The reference's Debug names of ElemKind (in its flux error texts).
+const char* kind_debug(int kind) {
+    static const char* names[] = {"Cps3", "Cps4", "Cps8", "Cpe4", "Cpe8", "C3d8", "C3d4", "B31"};
+    return (kind >= 0 && kind < 8) ? names[kind] : "Unknown";
+}
+
 }  // namespace
 
 extern "C" void svx_oracle_spmv(const svx_oracle_csr_t* k, const double* x, double* y, int threads);
 
 namespace {
+
+// assembly.rs:87-116 csr_from_triplets: bucket by row in stream order,
+// sort each row by column (the reference's unstable sort restated, or a
+// stable one), sum runs left to right starting from 0.0.  Allocates
+// out->row_ptr, col_idx, vals and an n-long out->f the caller fills.
+void csr_from_triplets(int64_t n, const std::vector<int64_t>& tr, const std::vector<int64_t>& tc,
+                       const std::vector<double>& tv, svx_oracle_csr_t* out) {
+    const int64_t nt = int64_t(tr.size());
+    std::vector<int64_t> rcount(n + 1, 0);
+    for (int64_t t = 0; t < nt; ++t) rcount[tr[t] + 1]++;
+    for (int64_t i = 0; i < n; ++i) rcount[i + 1] += rcount[i];
+    std::vector<int64_t> pos(rcount.begin(), rcount.end() - 1);
+    std::vector<int64_t> perm(nt);
+    for (int64_t t = 0; t < nt; ++t) perm[pos[tr[t]]++] = t;
+    std::vector<int64_t> rp(n + 1, 0);
+    std::vector<int64_t> ci;
+    std::vector<double> cv;
+    ci.reserve(nt / 2 + n);
+    cv.reserve(nt / 2 + n);
+    std::vector<Trip> row;
+    for (int64_t i = 0; i < n; ++i) {
+        row.clear();
+        for (int64_t q = rcount[i]; q < rcount[i + 1]; ++q) {
+            int64_t t = perm[q];
+            row.push_back(Trip{tc[t], tv[t]});
+        }
+        if (g_sort_mode == 0)
+            rust_sort_unstable(row.data(), int64_t(row.size()));
+        else
+            std::stable_sort(row.begin(), row.end(), trip_less);
+        size_t k = 0;
+        while (k < row.size()) {
+            int64_t c = row[k].c;
+            double v = 0.0;
+            while (k < row.size() && row[k].c == c) {
+                v += row[k].v;
+                ++k;
+            }
+            ci.push_back(c);
+            cv.push_back(v);
+        }
+        rp[i + 1] = int64_t(ci.size());
+    }
+    out->n = n;
+    out->nnz = int64_t(ci.size());
+    out->row_ptr = (int64_t*)std::malloc(sizeof(int64_t) * (n + 1));
+    out->col_idx = (int64_t*)std::malloc(sizeof(int64_t) * (ci.size() + 1));
+    out->vals = (double*)std::malloc(sizeof(double) * (cv.size() + 1));
+    out->f = (double*)std::malloc(sizeof(double) * (n + 1));
+    std::memcpy(out->row_ptr, rp.data(), sizeof(int64_t) * (n + 1));
+    std::memcpy(out->col_idx, ci.data(), sizeof(int64_t) * ci.size());
+    std::memcpy(out->vals, cv.data(), sizeof(double) * cv.size());
+}
 
 // stress.rs:22-118: centroid von Mises, nodal (extrapolated, averaged)
 // von Mises and reactions K_orig u - f_orig at the constrained rows.
@@ -786,52 +951,7 @@ int svx_oracle_assemble(const svx_flat_model_t* m, int threads, svx_oracle_csr_t
             set_error(err, SVX_INVALID_MODEL, fail[e], e, msg);
             return SVX_INVALID_MODEL;
         }
-    // csr_from_triplets: bucket by row in stream order, stable-sort each row
-    // by column, sum runs left to right starting from 0.0.
-    std::vector<int64_t> rcount(n + 1, 0);
-    for (int64_t t = 0; t < nt; ++t) rcount[tr[t] + 1]++;
-    for (int64_t i = 0; i < n; ++i) rcount[i + 1] += rcount[i];
-    std::vector<int64_t> pos(rcount.begin(), rcount.end() - 1);
-    std::vector<int64_t> perm(nt);
-    for (int64_t t = 0; t < nt; ++t) perm[pos[tr[t]]++] = t;
-    std::vector<int64_t> rp(n + 1, 0);
-    std::vector<int64_t> ci;
-    std::vector<double> cv;
-    ci.reserve(nt / 2 + n);
-    cv.reserve(nt / 2 + n);
-    std::vector<Trip> row;
-    for (int64_t i = 0; i < n; ++i) {
-        row.clear();
-        for (int64_t q = rcount[i]; q < rcount[i + 1]; ++q) {
-            int64_t t = perm[q];
-            row.push_back(Trip{tc[t], tv[t]});
-        }
-        if (g_sort_mode == 0)
-            rust_sort_unstable(row.data(), int64_t(row.size()));
-        else
-            std::stable_sort(row.begin(), row.end(), trip_less);
-        size_t k = 0;
-        while (k < row.size()) {
-            int64_t c = row[k].c;
-            double v = 0.0;
-            while (k < row.size() && row[k].c == c) {
-                v += row[k].v;
-                ++k;
-            }
-            ci.push_back(c);
-            cv.push_back(v);
-        }
-        rp[i + 1] = int64_t(ci.size());
-    }
-    out->n = n;
-    out->nnz = int64_t(ci.size());
-    out->row_ptr = (int64_t*)std::malloc(sizeof(int64_t) * (n + 1));
-    out->col_idx = (int64_t*)std::malloc(sizeof(int64_t) * (ci.size() + 1));
-    out->vals = (double*)std::malloc(sizeof(double) * (cv.size() + 1));
-    out->f = (double*)std::malloc(sizeof(double) * (n + 1));
-    std::memcpy(out->row_ptr, rp.data(), sizeof(int64_t) * (n + 1));
-    std::memcpy(out->col_idx, ci.data(), sizeof(int64_t) * ci.size());
-    std::memcpy(out->vals, cv.data(), sizeof(double) * cv.size());
+    csr_from_triplets(n, tr, tc, tv, out);
     for (int64_t i = 0; i < n; ++i) out->f[i] = m->f ? m->f[i] : 0.0;
     if (err) set_error(err, SVX_OK, 0, -1, "");
     return SVX_OK;
@@ -1009,6 +1129,150 @@ int svx_oracle_stress(const svx_flat_model_t* m, const double* u, int threads, d
     if (st != SVX_OK) return st;
     recover(m, u, &k, k.f, threads, vm, vm_node, reactions);
     svx_oracle_csr_free(&k);
+    return SVX_OK;
+}
+
+int svx_oracle_conduction_element(int kind, const double* coords, double conductivity,
+                                  double thickness, int has_source, double source, double* ke,
+                                  double* fe) {
+    bool used = false;
+    return conduction_ke(kind, coords, conductivity, thickness, has_source != 0, source, ke, fe,
+                         &used);
+}
+
+// heat.rs:52-98 solve_thermal, elements of the linear-static path (CPS3,
+// CPS4 / CPE4, C3D8): seeds and conduction triplets in element order, flux
+// loads, csr_from_triplets, apply_temperatures (heat.rs:361-407), PCG.
+int svx_oracle_solve_thermal(const svx_oracle_thermal_t* m, int threads, double tol,
+                             double* temperatures, int64_t* iterations, double* residual,
+                             svx_error_t* err) {
+    auto fail = [&](int code, int reason, int64_t elem, const std::string& msg) {
+        set_error(err, code, reason, elem, msg.c_str());
+        return code;
+    };
+    auto eid = [&](int64_t e) { return m->elem_id ? m->elem_id[e] : uint32_t(e + 1); };
+    if (m->n_nodes == 0 || m->n_elem == 0) return fail(SVX_EMPTY_MESH, 0, -1, "empty mesh");
+    for (int64_t e = 0; e < m->n_elem; ++e)
+        if (m->kind[e] == SVX_B31)
+            return fail(SVX_INVALID_MODEL, 0, -1,
+                        "beam elements have no conduction formulation (v1: plane and solid "
+                        "only)");
+    if (m->n_temp == 0) return fail(SVX_NO_CONSTRAINTS, 0, -1, "no constraints");
+    if (!(m->thickness > 0.0) || !(m->conductivity > 0.0))
+        return fail(SVX_INVALID_MODEL, 0, -1, "thickness and conductivity must be positive");
+    const int64_t n = m->n_nodes;
+    std::vector<int64_t> tr, tc;
+    std::vector<double> tv;
+    tr.reserve(size_t(n) + size_t(m->n_elem) * 64);
+    tc.reserve(tr.capacity());
+    tv.reserve(tr.capacity());
+    for (int64_t i = 0; i < n; ++i) {
+        tr.push_back(i);
+        tc.push_back(i);
+        tv.push_back(0.0);
+    }
+    std::vector<double> f(size_t(n), 0.0);
+    double ke[64], fe[8], coords[24];
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        const int kind = m->kind[e];
+        const int nn = node_count(kind);
+        const int32_t* cn = m->conn + m->conn_ptr[e];
+        for (int i = 0; i < nn && i < 8; ++i)
+            for (int a = 0; a < 3; ++a) coords[3 * i + a] = m->xyz[3 * int64_t(cn[i]) + a];
+        bool used = false;
+        const int r = conduction_ke(kind, coords, m->conductivity, m->thickness,
+                                    m->has_source != 0, m->source, ke, fe, &used);
+        if (r) {
+            char msg[300];
+            std::snprintf(msg, sizeof msg, "element %u: %s", eid(e), reason_text(r));
+            return fail(SVX_INVALID_MODEL, r, e, msg);
+        }
+        for (int i = 0; i < nn; ++i) {
+            if (used) f[cn[i]] += fe[i];
+            for (int j = 0; j < nn; ++j) {
+                tr.push_back(cn[i]);
+                tc.push_back(cn[j]);
+                tv.push_back(ke[i * nn + j]);
+            }
+        }
+    }
+    // heat.rs:298-358: linear plane edges only on this path
+    for (int64_t q = 0; q < m->n_flux; ++q) {
+        const int64_t e = m->flux_elem[q];
+        const int kind = m->kind[e];
+        int max_face = 0;
+        if (kind == SVX_CPS3)
+            max_face = 3;
+        else if (kind == SVX_CPS4 || kind == SVX_CPE4)
+            max_face = 4;
+        char msg[300];
+        if (!max_face) {
+            std::snprintf(msg, sizeof msg,
+                          "heat flux on element %u (%s) unsupported (plane edges only)", eid(e),
+                          kind_debug(kind));
+            return fail(SVX_INVALID_MODEL, 0, e, msg);
+        }
+        const int face = m->flux_face[q];
+        if (face <= 0 || face > max_face) {
+            std::snprintf(msg, sizeof msg, "element %u (%s) has no face %d", eid(e),
+                          kind_debug(kind), face);
+            return fail(SVX_INVALID_MODEL, 0, e, msg);
+        }
+        const int32_t* cn = m->conn + m->conn_ptr[e];
+        const int corners = node_count(kind);
+        const int32_t na = cn[face - 1], nb = cn[face % corners];
+        const double* pa = m->xyz + 3 * int64_t(na);
+        const double* pb = m->xyz + 3 * int64_t(nb);
+        const double dx = pb[0] - pa[0], dy = pb[1] - pa[1];
+        const double len = std::sqrt(dx * dx + dy * dy);
+        if (len == 0.0) {
+            std::snprintf(msg, sizeof msg, "zero-length flux edge on element %u", eid(e));
+            return fail(SVX_INVALID_MODEL, 0, e, msg);
+        }
+        const double total = m->flux_value[q] * m->thickness * len;
+        f[na] += total / 2.0;
+        f[nb] += total / 2.0;
+    }
+    svx_oracle_csr_t c;
+    csr_from_triplets(n, tr, tc, tv, &c);
+    // heat.rs:361-407: later constraints win; free rows carry K[r,c] T_c to
+    // the right-hand side, prescribed rows become identity rows
+    std::vector<double> pres(size_t(n), NAN);
+    for (int64_t q = 0; q < m->n_temp; ++q) pres[m->temp_node[q]] = m->temp_value[q];
+    for (int64_t r = 0; r < n; ++r) {
+        if (!std::isnan(pres[r])) continue;
+        for (int64_t ii = c.row_ptr[r]; ii < c.row_ptr[r + 1]; ++ii) {
+            const int64_t col = c.col_idx[ii];
+            if (!std::isnan(pres[col])) {
+                f[r] -= c.vals[ii] * pres[col];
+                c.vals[ii] = 0.0;
+            }
+        }
+    }
+    for (int64_t r = 0; r < n; ++r) {
+        if (std::isnan(pres[r])) continue;
+        for (int64_t ii = c.row_ptr[r]; ii < c.row_ptr[r + 1]; ++ii)
+            c.vals[ii] = (c.col_idx[ii] == r) ? 1.0 : 0.0;
+        f[r] = pres[r];
+    }
+    const int64_t max_iter = std::max<int64_t>(1000, 10 * n);
+    int64_t it = 0;
+    double res = 0.0;
+    const int st = svx_oracle_pcg(&c, f.data(), tol, max_iter, threads, temperatures, &it, &res);
+    svx_oracle_csr_free(&c);
+    *iterations = it;
+    *residual = res;
+    if (st != SVX_OK) {
+        char msg[200];
+        std::snprintf(msg, sizeof msg, "not converged after %lld iterations", (long long)it);
+        set_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
+        if (err) {
+            err->iterations = it;
+            err->residual = res;
+        }
+        return st;
+    }
+    if (err) set_error(err, SVX_OK, 0, -1, "");
     return SVX_OK;
 }
 
