@@ -272,6 +272,46 @@ int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol
  * (stress.rs:22-118) and the displacement packaging of lib.rs:689-698. */
 int svx_op_stress(svx_op_t* op, svx_solution_t* sol);
 
+/* ---- steady heat conduction (one temperature dof per node) ----------- */
+/* The model heat::solve_thermal reads (crates/solvix-core/src/heat.rs:52-98)
+ * from a Model and its last Step, flattened like svx_flat_model_t (0-based
+ * node indices).  Temperature constraints apply in array order, a later one
+ * for the same node winning (heat.rs:367-375); heat fluxes act on the plane
+ * edge `face` (1-based) of element flux_elem[i], positive into the element
+ * (heat.rs:298-358). */
+typedef struct svx_thermal_model {
+    int64_t n_nodes;
+    const double* xyz;          /* [3 * n_nodes] */
+    int64_t n_elem;
+    const uint8_t* kind;        /* [n_elem] enum svx_elem_kind */
+    const int64_t* conn_ptr;    /* [n_elem + 1] */
+    const int32_t* conn;        /* 0-based node indices */
+    const uint32_t* elem_id;    /* [n_elem] ids for messages; NULL = e + 1 */
+    double thickness;           /* model-wide (2D elements) */
+    double conductivity;        /* model-wide */
+    int32_t has_source;         /* the step's volumetric heat source is set */
+    double source;
+    int64_t n_temp;
+    const int64_t* temp_node;   /* [n_temp] node indices */
+    const double* temp_value;   /* [n_temp] */
+    int64_t n_flux;
+    const int64_t* flux_elem;   /* [n_flux] element indices */
+    const int32_t* flux_face;   /* [n_flux] 1-based edge */
+    const double* flux_value;   /* [n_flux] */
+} svx_thermal_model_t;
+
+/* Replaces heat::solve_thermal (heat.rs:52-98): conduction matrices of
+ * CPS3, CPS4 / CPE4 and C3D8 elements (heat.rs:149-296) assembled on the
+ * device in the mechanical path's fixed order, source and flux loads,
+ * nonhomogeneous temperature rows (heat.rs:361-407) and the FP64 Jacobi-PCG
+ * (opts: tol, max_iter <= 0 for max(1000, 10 * nodes), check_every; the
+ * precision must be SVX_FP64).  temperatures: [n_nodes].  Errors and their
+ * texts follow the reference (EmptyMesh, NoConstraints, InvalidModel,
+ * NotConverged). */
+int svx_solve_thermal_flat(svx_ctx_t* ctx, const svx_thermal_model_t* model,
+                           const svx_solve_opts_t* opts, double* temperatures,
+                           int64_t* iterations, double* residual, svx_error_t* err);
+
 /* ---- batched solves (many independent models in one launch) -------- */
 typedef struct svx_batch_result {
     int64_t iterations;    /* PCG iterations of this model */

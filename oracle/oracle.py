@@ -31,7 +31,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 from solvix_b200 import abi  # noqa: E402  (struct layouts only)
-from solvix_b200.marshal import FlatModel  # noqa: E402
+from solvix_b200.marshal import FlatModel, ThermalModel  # noqa: E402
 from solvix_b200.model import (ElemKind, EmptyMesh, InvalidModel, Model,  # noqa: E402
                                NoConstraints, NotConverged, SolveError)
 
@@ -46,30 +46,6 @@ class OracleCsr(C.Structure):
         ("col_idx", abi.c_int64_p),
         ("vals", abi.c_double_p),
         ("f", abi.c_double_p),
-    ]
-
-
-class OracleThermal(C.Structure):
-    """svx_oracle_thermal_t (oracle/svx_oracle.h)."""
-    _fields_ = [
-        ("n_nodes", C.c_int64),
-        ("xyz", abi.c_double_p),
-        ("n_elem", C.c_int64),
-        ("kind", C.POINTER(C.c_uint8)),
-        ("conn_ptr", abi.c_int64_p),
-        ("conn", C.POINTER(C.c_int32)),
-        ("elem_id", C.POINTER(C.c_uint32)),
-        ("thickness", C.c_double),
-        ("conductivity", C.c_double),
-        ("has_source", C.c_int32),
-        ("source", C.c_double),
-        ("n_temp", C.c_int64),
-        ("temp_node", abi.c_int64_p),
-        ("temp_value", abi.c_double_p),
-        ("n_flux", C.c_int64),
-        ("flux_elem", abi.c_int64_p),
-        ("flux_face", C.POINTER(C.c_int32)),
-        ("flux_value", abi.c_double_p),
     ]
 
 
@@ -90,9 +66,9 @@ _SIG = {
     "svx_oracle_stress": (C.c_int, [C.POINTER(abi.SvxFlatModel), abi.c_double_p, C.c_int,
                                     abi.c_double_p, abi.c_double_p, abi.c_double_p,
                                     C.POINTER(abi.SvxError)]),
-    "svx_oracle_solve_thermal": (C.c_int, [C.POINTER(OracleThermal), C.c_int, C.c_double,
-                                           abi.c_double_p, abi.c_int64_p, abi.c_double_p,
-                                           C.POINTER(abi.SvxError)]),
+    "svx_oracle_solve_thermal": (C.c_int, [C.POINTER(abi.SvxThermalModel), C.c_int,
+                                           C.c_double, abi.c_double_p, abi.c_int64_p,
+                                           abi.c_double_p, C.POINTER(abi.SvxError)]),
     "svx_oracle_conduction_element": (C.c_int, [C.c_int, abi.c_double_p, C.c_double,
                                                 C.c_double, C.c_int, C.c_double,
                                                 abi.c_double_p, abi.c_double_p]),
@@ -404,44 +380,6 @@ def solve(model: Model, tol=1e-10, threads: int | None = None):
 
 
 # ------------------------------------------------------------------ thermal
-class ThermalModel:
-    """Flat steady-conduction model (heat.rs:52-98 reads these from Model
-    and its last Step): 0-based node indices, temperature constraints in
-    order (a later one wins), plane-edge heat fluxes by element index."""
-
-    def __init__(self, xyz, kind, conn_ptr, conn, conductivity, thickness=1.0, elem_id=None,
-                 source=None, temp_node=(), temp_value=(), flux_elem=(), flux_face=(),
-                 flux_value=()):
-        self.xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
-        self.kind = np.ascontiguousarray(kind, dtype=np.uint8)
-        self.conn_ptr = np.ascontiguousarray(conn_ptr, dtype=np.int64)
-        self.conn = np.ascontiguousarray(conn, dtype=np.int32)
-        self.elem_id = None if elem_id is None else np.ascontiguousarray(elem_id, dtype=np.uint32)
-        self.conductivity = float(conductivity)
-        self.thickness = float(thickness)
-        self.source = source
-        self.temp_node = np.ascontiguousarray(temp_node, dtype=np.int64)
-        self.temp_value = np.ascontiguousarray(temp_value, dtype=np.float64)
-        self.flux_elem = np.ascontiguousarray(flux_elem, dtype=np.int64)
-        self.flux_face = np.ascontiguousarray(flux_face, dtype=np.int32)
-        self.flux_value = np.ascontiguousarray(flux_value, dtype=np.float64)
-
-    @property
-    def n_nodes(self):
-        return self.xyz.shape[0]
-
-    def struct(self) -> OracleThermal:
-        def p(a, t):
-            return a.ctypes.data_as(C.POINTER(t)) if a is not None and a.size else None
-        return OracleThermal(
-            self.n_nodes, p(self.xyz, C.c_double), self.kind.shape[0], p(self.kind, C.c_uint8),
-            p(self.conn_ptr, C.c_int64), p(self.conn, C.c_int32), p(self.elem_id, C.c_uint32),
-            self.thickness, self.conductivity, int(self.source is not None),
-            float(self.source or 0.0), self.temp_node.shape[0], p(self.temp_node, C.c_int64),
-            p(self.temp_value, C.c_double), self.flux_elem.shape[0], p(self.flux_elem, C.c_int64),
-            p(self.flux_face, C.c_int32), p(self.flux_value, C.c_double))
-
-
 def solve_thermal(tm: ThermalModel, tol=1e-10, threads: int | None = None):
     """heat::solve_thermal restated; returns (temperatures, iterations,
     residual) or raises the reference's SolveError."""
@@ -449,7 +387,7 @@ def solve_thermal(tm: ThermalModel, tol=1e-10, threads: int | None = None):
     it = C.c_int64(0)
     res = C.c_double(0.0)
     err = abi.SvxError()
-    s = tm.struct()
+    s = tm.as_struct()
     st = lib().svx_oracle_solve_thermal(C.byref(s), default_threads() if threads is None
                                         else int(threads), float(tol), abi.ptr(t, C.c_double),
                                         C.byref(it), C.byref(res), C.byref(err))

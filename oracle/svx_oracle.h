@@ -70,32 +70,8 @@ int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t
 int svx_oracle_stress(const svx_flat_model_t* m, const double* u, int threads, double* vm,
                       double* vm_node, double* reactions, svx_error_t* err);
 
-/* Steady heat conduction: the model solve_thermal reads (heat.rs:52-98),
- * flattened like svx_flat_model_t (0-based node indices).  One temperature
- * dof per node.  Temperature constraints are applied in array order (a
- * later entry for the same node wins, heat.rs:367-375); heat fluxes act on
- * the plane edge `face` (1-based) of element flux_elem[i] with magnitude
- * flux_value[i], positive into the element (heat.rs:298-358). */
-typedef struct svx_oracle_thermal {
-    int64_t n_nodes;
-    const double* xyz;        /* [3 * n_nodes] */
-    int64_t n_elem;
-    const uint8_t* kind;      /* enum svx_elem_kind */
-    const int64_t* conn_ptr;  /* [n_elem + 1] */
-    const int32_t* conn;      /* 0-based node indices */
-    const uint32_t* elem_id;  /* [n_elem] ids for messages; NULL = e + 1 */
-    double thickness;
-    double conductivity;
-    int32_t has_source;       /* the step's volumetric heat source is set */
-    double source;
-    int64_t n_temp;
-    const int64_t* temp_node; /* [n_temp] node indices */
-    const double* temp_value; /* [n_temp] */
-    int64_t n_flux;
-    const int64_t* flux_elem; /* [n_flux] element indices */
-    const int32_t* flux_face; /* [n_flux] 1-based face */
-    const double* flux_value; /* [n_flux] */
-} svx_oracle_thermal_t;
+/* Steady heat conduction: the public svx_thermal_model_t (solvix_gpu.h). */
+typedef svx_thermal_model_t svx_oracle_thermal_t;
 
 /* heat::solve_thermal restated (heat.rs:52-98) for CPS3, CPS4, CPE4 and
  * C3D8 elements: conduction matrices (heat.rs:149-296), flux loads

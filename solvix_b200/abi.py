@@ -175,6 +175,30 @@ class SvxBatchStats(C.Structure):
     ]
 
 
+class SvxThermalModel(C.Structure):
+    """svx_thermal_model_t (steady conduction, heat.rs:52-98)."""
+    _fields_ = [
+        ("n_nodes", C.c_int64),
+        ("xyz", c_double_p),
+        ("n_elem", C.c_int64),
+        ("kind", c_uint8_p),
+        ("conn_ptr", c_int64_p),
+        ("conn", c_int32_p),
+        ("elem_id", c_uint32_p),
+        ("thickness", C.c_double),
+        ("conductivity", C.c_double),
+        ("has_source", C.c_int32),
+        ("source", C.c_double),
+        ("n_temp", C.c_int64),
+        ("temp_node", c_int64_p),
+        ("temp_value", c_double_p),
+        ("n_flux", C.c_int64),
+        ("flux_elem", c_int64_p),
+        ("flux_face", c_int32_p),
+        ("flux_value", c_double_p),
+    ]
+
+
 class SvxServeOpts(C.Structure):
     _fields_ = [
         ("hbm_budget_bytes", C.c_int64),
@@ -273,6 +297,9 @@ SIGNATURES = {
                                  C.POINTER(SvxSolution), C.POINTER(SvxError)]),
     "svx_solve_resolved": (C.c_int, [_VP, _VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),
                                      C.POINTER(SvxError)]),
+    "svx_solve_thermal_flat": (C.c_int, [_VP, C.POINTER(SvxThermalModel),
+                                         C.POINTER(SvxSolveOpts), c_double_p, c_int64_p,
+                                         c_double_p, C.POINTER(SvxError)]),
 }
 
 _lib = None

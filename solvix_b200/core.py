@@ -15,7 +15,7 @@ from typing import Optional
 import numpy as np
 
 from . import abi
-from .marshal import FlatModel, model_desc
+from .marshal import FlatModel, ThermalModel, model_desc
 from .model import (DeviceError, EmptyMesh, InvalidModel, Method, Model, NoConstraints,
                     NotConverged, Reaction, SolveError, Solution)
 
@@ -88,6 +88,24 @@ class Context:
         op = Operator(self, h, flat)
         self._ops.add(op)
         return op
+
+    def solve_thermal(self, tm: ThermalModel, tol: float = 1e-10, max_iter: int = 0,
+                      check_every: int = 0):
+        """Steady conduction on the device (svx_solve_thermal_flat, the
+        reference's heat::solve_thermal); returns (temperatures, iterations,
+        residual) or raises the reference's SolveError."""
+        t = np.zeros(tm.n_nodes)
+        it = C.c_int64(0)
+        res = C.c_double(0.0)
+        err = abi.SvxError()
+        opts = abi.default_opts(tol=tol, max_iter=max_iter, check_every=check_every)
+        s = tm.as_struct()
+        st = self.lib.svx_solve_thermal_flat(self.handle, C.byref(s), C.byref(opts),
+                                             abi.ptr(t, C.c_double), C.byref(it), C.byref(res),
+                                             C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        return t, int(it.value), float(res.value)
 
     def solve_flat(self, flat: FlatModel, tol: float = 1e-10, max_iter: int = 0,
                    precision: int = abi.SVX_FP64, inner_tol: float = 1e-5,

@@ -1103,4 +1103,160 @@ int svx_solve_flat(svx_ctx_t* ctx, const svx_flat_model_t* model, const svx_solv
     });
 }
 
+// heat::solve_thermal (heat.rs:52-98) on the device: the checks in the
+// reference's order, conduction matrices (K1 form), the pattern and the
+// fixed-order assembly at one dof per node (K3, K2), source and flux loads,
+// temperature rows, the Jacobi diagonal and the FP64 PCG.
+int svx_solve_thermal_flat(svx_ctx_t* ctx, const svx_thermal_model_t* m,
+                           const svx_solve_opts_t* o, double* temperatures, int64_t* iterations,
+                           double* residual, svx_error_t* err) {
+    if (!ctx || !m) return SVX_BAD_ARGUMENT;
+    return guarded(ctx, err, [&]() -> int {
+        SVX_CUDA(cudaSetDevice(ctx->device));
+        auto bad = [](const std::string& msg) { throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, msg}; };
+        if (m->n_nodes < 0 || m->n_elem < 0 || m->n_temp < 0 || m->n_flux < 0)
+            bad("negative size");
+        if (m->n_nodes > 0 && !m->xyz) bad("null xyz");
+        if (m->n_elem > 0 && (!m->kind || !m->conn_ptr || !m->conn)) bad("null element array");
+        if (m->n_temp > 0 && (!m->temp_node || !m->temp_value)) bad("null temperature array");
+        if (m->n_flux > 0 && (!m->flux_elem || !m->flux_face || !m->flux_value))
+            bad("null flux array");
+        if (m->n_elem > 0 && m->conn_ptr[0] != 0) bad("conn_ptr[0] must be 0");
+        auto eid = [&](int64_t e) { return m->elem_id ? m->elem_id[e] : uint32_t(e + 1); };
+        int max_nn = 1;
+        for (int64_t e = 0; e < m->n_elem; ++e) {
+            const int nn = node_count(m->kind[e]);
+            if (nn < 0) bad("unknown element kind " + std::to_string(int(m->kind[e])));
+            if (m->conn_ptr[e + 1] - m->conn_ptr[e] != nn)
+                bad("element " + std::to_string(eid(e)) + " has " +
+                    std::to_string(m->conn_ptr[e + 1] - m->conn_ptr[e]) + " nodes, kind needs " +
+                    std::to_string(nn));
+            for (int64_t q = m->conn_ptr[e]; q < m->conn_ptr[e + 1]; ++q)
+                if (m->conn[q] < 0 || m->conn[q] >= m->n_nodes)
+                    bad("element " + std::to_string(eid(e)) + " references node index " +
+                        std::to_string(m->conn[q]) + " out of range");
+            max_nn = std::max(max_nn, nn);
+        }
+        for (int64_t q = 0; q < m->n_temp; ++q)
+            if (m->temp_node[q] < 0 || m->temp_node[q] >= m->n_nodes)
+                bad("temperature node index out of range");
+        for (int64_t q = 0; q < m->n_flux; ++q)
+            if (m->flux_elem[q] < 0 || m->flux_elem[q] >= m->n_elem)
+                bad("flux element index out of range");
+        // heat.rs:53-79
+        if (m->n_nodes == 0 || m->n_elem == 0) throw ModelFail{SVX_EMPTY_MESH, 0, -1, "empty mesh"};
+        for (int64_t e = 0; e < m->n_elem; ++e)
+            if (m->kind[e] == SVX_B31)
+                throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                                "beam elements have no conduction formulation (v1: plane and "
+                                "solid only)"};
+        if (m->n_temp == 0) throw ModelFail{SVX_NO_CONSTRAINTS, 0, -1, "no constraints"};
+        if (!(m->thickness > 0.0) || !(m->conductivity > 0.0))
+            throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                            "thickness and conductivity must be positive"};
+        svx_solve_opts_t opts;
+        svx_default_opts(&opts);
+        if (o) opts = *o;
+        if (opts.precision != SVX_FP64) bad("the conduction solve runs in FP64 only");
+
+        std::unique_ptr<svx_op> op(new svx_op());
+        op->ctx = ctx;
+        op->n_nodes = m->n_nodes;
+        op->n_elem = m->n_elem;
+        op->ndof = 1;
+        op->n = m->n_nodes;
+        op->thickness = m->thickness;
+        cudaStream_t st = ctx->stream;
+        SVX_CUDA(cudaEventRecord(ctx->ev[6], st));
+        upload(ctx, op->xyz, m->xyz, size_t(3 * m->n_nodes));
+        upload(ctx, op->kind, m->kind, size_t(m->n_elem));
+        upload(ctx, op->conn_ptr, m->conn_ptr, size_t(m->n_elem + 1));
+        upload(ctx, op->conn, m->conn, size_t(m->conn_ptr[m->n_elem]));
+        op->pat.max_nn = max_nn;
+        op->pat.ke_stride = max_nn * max_nn;
+        DBuf<double> ke, fe;
+        ke.alloc(ctx->pool, size_t(m->n_elem) * op->pat.ke_stride + 1);
+        fe.alloc(ctx->pool, size_t(m->n_elem) * max_nn + 1);
+        // conduction_element runs first: its errors precede the flux checks
+        const uint64_t g = integrate_conduction(ctx, op.get(), m->conductivity, m->has_source,
+                                                m->source, ke.p, op->pat.ke_stride, fe.p);
+        if (g != ~uint64_t(0)) {
+            const int64_t e = int64_t(g >> 8);
+            const int reason = int(g & 0xff);
+            throw ModelFail{SVX_INVALID_MODEL, reason, e,
+                            "element " + std::to_string(eid(e)) + ": " + reason_text(reason)};
+        }
+        // heat.rs:300-338: kinds, faces, edge lengths (host, flux order)
+        static const char* debug_names[] = {"Cps3", "Cps4", "Cps8", "Cpe4",
+                                            "Cpe8", "C3d8", "C3d4", "B31"};
+        for (int64_t q = 0; q < m->n_flux; ++q) {
+            const int64_t e = m->flux_elem[q];
+            const int kd = m->kind[e];
+            const int max_face = kd == SVX_CPS3 ? 3 : (kd == SVX_CPS4 || kd == SVX_CPE4) ? 4 : 0;
+            if (!max_face)
+                throw ModelFail{SVX_INVALID_MODEL, 0, e,
+                                "heat flux on element " + std::to_string(eid(e)) + " (" +
+                                    debug_names[kd] + ") unsupported (plane edges only)"};
+            const int face = m->flux_face[q];
+            if (face <= 0 || face > max_face)
+                throw ModelFail{SVX_INVALID_MODEL, 0, e,
+                                "element " + std::to_string(eid(e)) + " (" + debug_names[kd] +
+                                    ") has no face " + std::to_string(face)};
+            const int32_t* cn = m->conn + m->conn_ptr[e];
+            const double* pa = m->xyz + 3 * int64_t(cn[face - 1]);
+            const double* pb = m->xyz + 3 * int64_t(cn[face % max_face]);
+            const double dx = pb[0] - pa[0], dy = pb[1] - pa[1];
+            if (std::sqrt(dx * dx + dy * dy) == 0.0)
+                throw ModelFail{SVX_INVALID_MODEL, 0, e,
+                                "zero-length flux edge on element " + std::to_string(eid(e))};
+        }
+        build_pattern(ctx, op.get());
+        op->vals.alloc(ctx->pool, op->pat.nnz + 1);
+        assemble_values(ctx, op.get(), ke.p, op->pat.ke_stride, op->vals.p);
+        ke.reset();
+        DBuf<int64_t> d_fe_elem;
+        DBuf<int32_t> d_face;
+        DBuf<double> d_flux;
+        if (m->n_flux > 0) {
+            upload(ctx, d_fe_elem, m->flux_elem, size_t(m->n_flux));
+            upload(ctx, d_face, m->flux_face, size_t(m->n_flux));
+            upload(ctx, d_flux, m->flux_value, size_t(m->n_flux));
+        }
+        op->f.alloc(ctx->pool, size_t(op->n) + 1);
+        thermal_loads(ctx, op.get(), fe.p, m->has_source, m->n_flux, d_fe_elem.p, d_face.p,
+                      d_flux.p, op->f.p);
+        fe.reset();
+        // heat.rs:367-375: prescribed temperature per node, the last wins
+        std::vector<double> pres(size_t(op->n), std::nan(""));
+        for (int64_t q = 0; q < m->n_temp; ++q) pres[m->temp_node[q]] = m->temp_value[q];
+        DBuf<double> d_pres;
+        upload(ctx, d_pres, pres.data(), pres.size());
+        apply_temperatures(ctx, op.get(), d_pres.p);
+        jacobi_diagonal(ctx, op.get());
+        SVX_CUDA(cudaEventRecord(ctx->ev[7], st));
+        op->ms_assemble = elapsed_ms(ctx->ev[6], ctx->ev[7]);
+        const long long max_iter = opts.max_iter > 0 ? opts.max_iter : default_max_iter(op->n);
+        op->u.alloc(ctx->pool, size_t(op->n) + 1);
+        const PcgResult r = pcg_fp64(ctx, op.get(), opts.tol, max_iter, opts.check_every, op->u.p);
+        if (temperatures)
+            SVX_CUDA(cudaMemcpyAsync(temperatures, op->u.p, sizeof(double) * size_t(op->n),
+                                     cudaMemcpyDeviceToHost, st));
+        SVX_CUDA(cudaStreamSynchronize(st));
+        if (iterations) *iterations = r.iterations;
+        if (residual) *residual = r.residual;
+        if (r.status != PCG_CONVERGED) {
+            std::string msg = "not converged after " + std::to_string(r.iterations) + " iterations";
+            fill_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
+            if (err) {
+                err->iterations = r.iterations;
+                err->residual = r.residual;
+            }
+            ctx->last_error = msg;
+            return SVX_NOT_CONVERGED;
+        }
+        clear_error(err);
+        return SVX_OK;
+    });
+}
+
 }  // extern "C"

@@ -247,7 +247,14 @@ void apply_dirichlet(svx_ctx* ctx, svx_op* op) {
             n, P.row_ptr.p, P.col_idx.p, op->is_fixed.p, op->vals.p, op->f.p);
         SVX_LAUNCH_CHECK();
     }
-    // Jacobi inverse diagonal and cond estimate of the modified K
+    jacobi_diagonal(ctx, op);
+}
+
+// Jacobi inverse diagonal and cond estimate of the modified K
+void jacobi_diagonal(svx_ctx* ctx, svx_op* op) {
+    cudaStream_t st = ctx->stream;
+    const Pattern& P = op->pat;
+    const int64_t n = op->n;
     op->inv_diag.alloc(ctx->pool, n + 1);
     const int64_t nb = (n + 255) / 256;
     DBuf<double> bhi, blo;

@@ -639,6 +639,230 @@ __global__ void displacements_kernel(int64_t n_nodes, int ndof, const double* __
     disp3[3 * i + 2] = ndof == 3 ? u[i * ndof + 2] : 0.0;
 }
 
+// ---------------------------------------------------------------- conduction
+// Steady heat conduction (heat.rs:149-296), one thread per element: the
+// conduction matrix k * integral of grad N . grad N (N x N, N = nodes) into
+// the element's Ke slot, and the consistent heat-source load into fe.  The
+// gradients are built exactly as quad_b / hex_b build the first rows of B
+// (element.rs:147-171, 479-521), in the reference's loop and sum order, so
+// the values are bit-identical to the oracle's.  Kinds outside CPS3, CPS4 /
+// CPE4 and C3D8 flag SVX_REASON_UNSUPPORTED_KIND.
+__global__ void conduction_kernel(int64_t n_elem, const uint8_t* __restrict__ kind,
+                                  const int64_t* __restrict__ conn_ptr,
+                                  const int32_t* __restrict__ conn,
+                                  const double* __restrict__ xyz, double k, double t, int has_q,
+                                  double q, double* __restrict__ ke, int ke_stride,
+                                  double* __restrict__ fe, int max_nn,
+                                  unsigned long long* first_fail) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= n_elem) return;
+    const int kd = kind[e];
+    const int64_t q0 = conn_ptr[e];
+    double* ke_e = ke + e * int64_t(ke_stride);
+    double* fe_e = fe + e * int64_t(max_nn);
+    const double qq = has_q ? q : 0.0;
+    auto fail = [&](int reason) {
+        atomicMin(first_fail, (unsigned long long)(e << 8) | (unsigned long long)reason);
+    };
+    if (kd == SVX_CPS3) {
+        double p[3][2];
+        for (int i = 0; i < 3; ++i) {
+            const int64_t nd = conn[q0 + i];
+            p[i][0] = xyz[nd * 3];
+            p[i][1] = xyz[nd * 3 + 1];
+        }
+        // heat.rs:140-145
+        const double b[3] = {p[1][1] - p[2][1], p[2][1] - p[0][1], p[0][1] - p[1][1]};
+        const double c[3] = {p[2][0] - p[1][0], p[0][0] - p[2][0], p[1][0] - p[0][0]};
+        const double two_a = b[0] * c[1] - b[1] * c[0];
+        if (two_a == 0.0) {
+            fail(SVX_REASON_DEGENERATE_TRI);
+            return;
+        }
+        const double w = k * t / (2.0 * fabs(two_a));
+        for (int i = 0; i < 3; ++i) {
+            fe_e[i] = has_q ? q * t * fabs(two_a) / 6.0 : 0.0;
+            for (int j = 0; j < 3; ++j) ke_e[i * 3 + j] = w * (b[i] * b[j] + c[i] * c[j]);
+        }
+        return;
+    }
+    const double g = 1.0 / sqrt(3.0);
+    if (kd == SVX_CPS4 || kd == SVX_CPE4) {
+        double x[8];
+        for (int i = 0; i < 4; ++i) {
+            const int64_t nd = conn[q0 + i];
+            x[2 * i] = xyz[nd * 3];
+            x[2 * i + 1] = xyz[nd * 3 + 1];
+        }
+        double kl[16], fl[4];
+        for (int i = 0; i < 16; ++i) kl[i] = 0.0;
+        for (int i = 0; i < 4; ++i) fl[i] = 0.0;
+        for (int a = 0; a < 2; ++a)
+            for (int bq = 0; bq < 2; ++bq) {
+                const double xi = a ? g : -g, eta = bq ? g : -g;
+                double dxi[4], deta[4];
+                for (int i = 0; i < 4; ++i) {
+                    const double xi_i = quadc(i, 0), eta_i = quadc(i, 1);
+                    dxi[i] = 0.25 * xi_i * (1.0 + eta * eta_i);
+                    deta[i] = 0.25 * eta_i * (1.0 + xi * xi_i);
+                }
+                double j00 = 0.0, j01 = 0.0, j10 = 0.0, j11 = 0.0;
+                for (int i = 0; i < 4; ++i) {
+                    j00 += dxi[i] * x[2 * i];
+                    j01 += dxi[i] * x[2 * i + 1];
+                    j10 += deta[i] * x[2 * i];
+                    j11 += deta[i] * x[2 * i + 1];
+                }
+                const double detj = j00 * j11 - j01 * j10;
+                if (detj <= 0.0) {
+                    fail(SVX_REASON_BAD_JACOBIAN);
+                    return;
+                }
+                const double inv = 1.0 / detj;
+                double dnx[4], dny[4], n[4];
+                for (int i = 0; i < 4; ++i) {
+                    dnx[i] = inv * (j11 * dxi[i] - j01 * deta[i]);
+                    dny[i] = inv * (j00 * deta[i] - j10 * dxi[i]);
+                    n[i] = 0.25 * (1.0 + xi * quadc(i, 0)) * (1.0 + eta * quadc(i, 1));
+                }
+                for (int i = 0; i < 4; ++i) {
+                    fl[i] += qq * t * detj * n[i];
+                    for (int j = 0; j < 4; ++j)
+                        kl[i * 4 + j] += k * t * detj * (dnx[i] * dnx[j] + dny[i] * dny[j]);
+                }
+            }
+        for (int i = 0; i < 16; ++i) ke_e[i] = kl[i];
+        for (int i = 0; i < 4; ++i) fe_e[i] = fl[i];
+        return;
+    }
+    if (kd == SVX_C3D8) {
+        double x[24];
+        for (int i = 0; i < 8; ++i) {
+            const int64_t nd = conn[q0 + i];
+            for (int b = 0; b < 3; ++b) x[i * 3 + b] = xyz[nd * 3 + b];
+        }
+        double kl[64], fl[8];
+        for (int i = 0; i < 64; ++i) kl[i] = 0.0;
+        for (int i = 0; i < 8; ++i) fl[i] = 0.0;
+        for (int gp = 0; gp < 8; ++gp) {
+            const double xi = (gp & 4) ? g : -g, eta = (gp & 2) ? g : -g,
+                         zeta = (gp & 1) ? g : -g;
+            double dn[3][8];
+            for (int i = 0; i < 8; ++i) {
+                const double a = hexc(i, 0), b = hexc(i, 1), c = hexc(i, 2);
+                dn[0][i] = 0.125 * a * (1.0 + eta * b) * (1.0 + zeta * c);
+                dn[1][i] = 0.125 * b * (1.0 + xi * a) * (1.0 + zeta * c);
+                dn[2][i] = 0.125 * c * (1.0 + xi * a) * (1.0 + eta * b);
+            }
+            double J[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    double sum = 0.0;
+                    for (int i = 0; i < 8; ++i) sum += dn[a][i] * x[i * 3 + b];
+                    J[a * 3 + b] = sum;
+                }
+            const double detj = det3(J);
+            if (detj <= 0.0) {
+                fail(SVX_REASON_BAD_JACOBIAN);
+                return;
+            }
+            const double id = 1.0 / detj;
+            double inv[9];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) inv[i * 3 + j] = inv3_entry(J, id, i, j);
+            double gr[8][3], n[8];
+            for (int i = 0; i < 8; ++i) {
+                for (int b = 0; b < 3; ++b) {
+                    double sum = 0.0;
+                    for (int a = 0; a < 3; ++a) sum += inv[b * 3 + a] * dn[a][i];
+                    gr[i][b] = sum;
+                }
+                n[i] = 0.125 * (1.0 + xi * hexc(i, 0)) * (1.0 + eta * hexc(i, 1)) *
+                       (1.0 + zeta * hexc(i, 2));
+            }
+            for (int i = 0; i < 8; ++i) {
+                fl[i] += qq * detj * n[i];
+                for (int j = 0; j < 8; ++j) {
+                    double v = 0.0;
+                    for (int r = 0; r < 3; ++r) v += gr[i][r] * gr[j][r];
+                    kl[i * 8 + j] += k * detj * v;
+                }
+            }
+        }
+        for (int i = 0; i < 64; ++i) ke_e[i] = kl[i];
+        for (int i = 0; i < 8; ++i) fe_e[i] = fl[i];
+        return;
+    }
+    fail(SVX_REASON_UNSUPPORTED_KIND);
+}
+
+// Element source loads summed per node over its incident (element, local)
+// slots in ascending element order: the reference's f[idx[i]] += fe[i] in
+// element enumeration order (heat.rs:207-212, 283-288).
+__global__ void node_source_kernel(int64_t n_nodes, const int64_t* __restrict__ slot_ptr,
+                                   const int32_t* __restrict__ slot_elem,
+                                   const uint8_t* __restrict__ slot_local,
+                                   const double* __restrict__ fe, int max_nn,
+                                   double* __restrict__ f) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) return;
+    double s = 0.0;
+    for (int64_t sl = slot_ptr[i]; sl < slot_ptr[i + 1]; ++sl)
+        s += fe[int64_t(slot_elem[sl]) * max_nn + slot_local[sl]];
+    f[i] = s;
+}
+
+// heat.rs:298-358 for linear plane edges, one thread in flux order (the
+// host has checked kinds, faces and edge lengths).
+__global__ void flux_load_kernel(int64_t n_flux, const int64_t* __restrict__ flux_elem,
+                                 const int32_t* __restrict__ flux_face,
+                                 const double* __restrict__ flux_value,
+                                 const uint8_t* __restrict__ kind,
+                                 const int64_t* __restrict__ conn_ptr,
+                                 const int32_t* __restrict__ conn,
+                                 const double* __restrict__ xyz, double t, double* f) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int64_t q = 0; q < n_flux; ++q) {
+        const int64_t e = flux_elem[q];
+        const int face = flux_face[q];
+        const int corners = (kind[e] == SVX_CPS3) ? 3 : 4;
+        const int64_t q0 = conn_ptr[e];
+        const int64_t na = conn[q0 + face - 1], nb = conn[q0 + face % corners];
+        const double dx = xyz[nb * 3] - xyz[na * 3], dy = xyz[nb * 3 + 1] - xyz[na * 3 + 1];
+        const double len = sqrt(dx * dx + dy * dy);
+        const double total = flux_value[q] * t * len;
+        f[na] += total / 2.0;
+        f[nb] += total / 2.0;
+    }
+}
+
+// heat.rs:361-407, one thread per row: a free row moves K_rc T_c of every
+// prescribed column to its right-hand side in column order and zeroes the
+// entry; a prescribed row becomes an identity row with T on the right.
+__global__ void temperature_rows_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
+                                        const int32_t* __restrict__ col_idx,
+                                        const double* __restrict__ pres,
+                                        double* __restrict__ vals, double* __restrict__ f) {
+    const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const double tr = pres[r];
+    if (isnan(tr)) {
+        double fr = f[r];
+        for (int32_t ii = row_ptr[r]; ii < row_ptr[r + 1]; ++ii) {
+            const double tc = pres[col_idx[ii]];
+            if (!isnan(tc)) {
+                fr -= vals[ii] * tc;
+                vals[ii] = 0.0;
+            }
+        }
+        f[r] = fr;
+    } else {
+        for (int32_t ii = row_ptr[r]; ii < row_ptr[r + 1]; ++ii)
+            vals[ii] = (col_idx[ii] == r) ? 1.0 : 0.0;
+        f[r] = tr;
+    }
+}
+
 inline unsigned blocks_for(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 
 }  // namespace
@@ -697,6 +921,52 @@ void recover_stress(svx_ctx* ctx, svx_op* op, const double* u, double* vm_elem, 
     if (disp3 && op->n_nodes > 0) {
         displacements_kernel<<<blocks_for(op->n_nodes, 256), 256, 0, st>>>(op->n_nodes,
                                                                            op->ndof, u, disp3);
+        SVX_LAUNCH_CHECK();
+    }
+}
+
+uint64_t integrate_conduction(svx_ctx* ctx, svx_op* op, double conductivity, int has_source,
+                              double source, double* ke, int ke_stride, double* fe) {
+    DBuf<unsigned long long> fail;
+    fail.alloc(ctx->pool, 1);
+    SVX_CUDA(cudaMemsetAsync(fail.p, 0xff, sizeof(unsigned long long), ctx->stream));
+    if (op->n_elem > 0) {
+        conduction_kernel<<<blocks_for(op->n_elem, 128), 128, 0, ctx->stream>>>(
+            op->n_elem, op->kind.p, op->conn_ptr.p, op->conn.p, op->xyz.p, conductivity,
+            op->thickness, has_source, source, ke, ke_stride, fe, op->pat.max_nn, fail.p);
+        SVX_LAUNCH_CHECK();
+    }
+    unsigned long long h = 0;
+    SVX_CUDA(cudaMemcpyAsync(&h, fail.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return h;
+}
+
+void thermal_loads(svx_ctx* ctx, svx_op* op, const double* fe, int has_source, int64_t n_flux,
+                   const int64_t* flux_elem, const int32_t* flux_face, const double* flux_value,
+                   double* f) {
+    cudaStream_t st = ctx->stream;
+    const Pattern& P = op->pat;
+    if (has_source && op->n_nodes > 0) {
+        node_source_kernel<<<blocks_for(op->n_nodes, 256), 256, 0, st>>>(
+            op->n_nodes, P.slot_ptr.p, P.slot_elem.p, P.slot_local.p, fe, P.max_nn, f);
+        SVX_LAUNCH_CHECK();
+    } else if (op->n_nodes > 0) {
+        SVX_CUDA(cudaMemsetAsync(f, 0, sizeof(double) * size_t(op->n_nodes), st));
+    }
+    if (n_flux > 0) {
+        flux_load_kernel<<<1, 32, 0, st>>>(n_flux, flux_elem, flux_face, flux_value, op->kind.p,
+                                           op->conn_ptr.p, op->conn.p, op->xyz.p, op->thickness,
+                                           f);
+        SVX_LAUNCH_CHECK();
+    }
+}
+
+void apply_temperatures(svx_ctx* ctx, svx_op* op, const double* pres) {
+    const Pattern& P = op->pat;
+    if (op->n > 0) {
+        temperature_rows_kernel<<<blocks_for(op->n, 256), 256, 0, ctx->stream>>>(
+            op->n, P.row_ptr.p, P.col_idx.p, pres, op->vals.p, op->f.p);
         SVX_LAUNCH_CHECK();
     }
 }

@@ -297,6 +297,19 @@ uint64_t integrate_elements(svx_ctx* ctx, svx_op* op, double* ke, int ke_stride)
 void assemble_values(svx_ctx* ctx, svx_op* op, const double* ke, int ke_stride, double* vals);
 // Dirichlet + inverse diagonal + condition estimate (svx_assemble.cu).
 void apply_dirichlet(svx_ctx* ctx, svx_op* op);
+// Inverse diagonal and condition estimate of op->vals alone (svx_assemble.cu).
+void jacobi_diagonal(svx_ctx* ctx, svx_op* op);
+// Steady conduction (svx_element.cu): element conduction matrices into Ke
+// slots and source loads into fe ([n_elem * max_nn]); returns the first
+// failing element as (index << 8 | reason) or UINT64_MAX.
+uint64_t integrate_conduction(svx_ctx* ctx, svx_op* op, double conductivity, int has_source,
+                              double source, double* ke, int ke_stride, double* fe);
+// f = element source loads (node order of the slots) + plane-edge fluxes.
+void thermal_loads(svx_ctx* ctx, svx_op* op, const double* fe, int has_source, int64_t n_flux,
+                   const int64_t* flux_elem, const int32_t* flux_face, const double* flux_value,
+                   double* f);
+// Nonhomogeneous temperature rows on op->vals / op->f (pres: NaN = free).
+void apply_temperatures(svx_ctx* ctx, svx_op* op, const double* pres);
 // Stress recovery (svx_element.cu).
 void recover_stress(svx_ctx* ctx, svx_op* op, const double* u, double* vm_elem,
                     double* vm_node, double* reactions, double* disp3);

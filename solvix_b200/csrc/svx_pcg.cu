@@ -1722,10 +1722,14 @@ unsigned grid_nodes(const svx_ctx* ctx, int64_t n_nodes, int G) {
             if ((G_) == 8) { constexpr int ND = 3, GG = 8; KERNEL_CALL; } \
             else if ((G_) == 16) { constexpr int ND = 3, GG = 16; KERNEL_CALL; } \
             else { constexpr int ND = 3, GG = 32; KERNEL_CALL; }        \
-        } else {                                                        \
+        } else if ((ND_) == 2) {                                        \
             if ((G_) == 8) { constexpr int ND = 2, GG = 8; KERNEL_CALL; } \
             else if ((G_) == 16) { constexpr int ND = 2, GG = 16; KERNEL_CALL; } \
             else { constexpr int ND = 2, GG = 32; KERNEL_CALL; }        \
+        } else {                                                        \
+            if ((G_) == 8) { constexpr int ND = 1, GG = 8; KERNEL_CALL; } \
+            else if ((G_) == 16) { constexpr int ND = 1, GG = 16; KERNEL_CALL; } \
+            else { constexpr int ND = 1, GG = 32; KERNEL_CALL; }        \
         }                                                               \
     } while (0)
 
@@ -1777,6 +1781,13 @@ struct PcgRun {
                                   : (void*)pcg_persistent_kernel<3, SVX_PG3D, M, V, U, true>;
                 return narrow ? (void*)pcg_persistent_kernel<3, 8, M, V, U, false>
                               : (void*)pcg_persistent_kernel<3, SVX_PG3D, M, V, U, false>;
+            }
+            if (ND == 1) {  // one dof per node (conduction)
+                if (sadj)
+                    return narrow ? (void*)pcg_persistent2_kernel<1, 8, M, V, U, true>
+                                  : (void*)pcg_persistent2_kernel<1, 16, M, V, U, true>;
+                return narrow ? (void*)pcg_persistent2_kernel<1, 8, M, V, U, false>
+                              : (void*)pcg_persistent2_kernel<1, 16, M, V, U, false>;
             }
             if (sadj)
                 return narrow ? (void*)pcg_persistent2_kernel<2, 8, M, V, U, true>

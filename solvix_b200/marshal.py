@@ -229,3 +229,44 @@ def model_desc(model: Model):
     d.cload_dofs = abi.ptr(cd, C.c_int64)
     d.cload_values = abi.ptr(cv, C.c_double)
     return d, keep
+
+
+class ThermalModel:
+    """Flat steady-conduction model (svx_thermal_model_t): what
+    heat::solve_thermal (heat.rs:52-98) reads from a Model and its last
+    Step, with 0-based node indices, temperature constraints in order (a
+    later one for the same node wins) and plane-edge heat fluxes by element
+    index and 1-based face."""
+
+    def __init__(self, xyz, kind, conn_ptr, conn, conductivity, thickness=1.0, elem_id=None,
+                 source=None, temp_node=(), temp_value=(), flux_elem=(), flux_face=(),
+                 flux_value=()):
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self.kind = np.ascontiguousarray(kind, dtype=np.uint8)
+        self.conn_ptr = np.ascontiguousarray(conn_ptr, dtype=np.int64)
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32)
+        self.elem_id = None if elem_id is None else np.ascontiguousarray(elem_id, dtype=np.uint32)
+        self.conductivity = float(conductivity)
+        self.thickness = float(thickness)
+        self.source = source
+        self.temp_node = np.ascontiguousarray(temp_node, dtype=np.int64)
+        self.temp_value = np.ascontiguousarray(temp_value, dtype=np.float64)
+        self.flux_elem = np.ascontiguousarray(flux_elem, dtype=np.int64)
+        self.flux_face = np.ascontiguousarray(flux_face, dtype=np.int32)
+        self.flux_value = np.ascontiguousarray(flux_value, dtype=np.float64)
+
+    @property
+    def n_nodes(self) -> int:
+        return self.xyz.shape[0]
+
+    def as_struct(self) -> abi.SvxThermalModel:
+        """The C view of this model (valid while the model is alive)."""
+        def p(a, t):
+            return a.ctypes.data_as(C.POINTER(t)) if a is not None and a.size else None
+        return abi.SvxThermalModel(
+            self.n_nodes, p(self.xyz, C.c_double), self.kind.shape[0], p(self.kind, C.c_uint8),
+            p(self.conn_ptr, C.c_int64), p(self.conn, C.c_int32), p(self.elem_id, C.c_uint32),
+            self.thickness, self.conductivity, int(self.source is not None),
+            float(self.source or 0.0), self.temp_node.shape[0], p(self.temp_node, C.c_int64),
+            p(self.temp_value, C.c_double), self.flux_elem.shape[0], p(self.flux_elem, C.c_int64),
+            p(self.flux_face, C.c_int32), p(self.flux_value, C.c_double))

@@ -256,7 +256,8 @@ STRUCTS = [("svx_error_t", abi.SvxError), ("svx_model_desc_t", abi.SvxModelDesc)
            ("svx_flat_model_t", abi.SvxFlatModel), ("svx_solve_opts_t", abi.SvxSolveOpts),
            ("svx_solution_t", abi.SvxSolution), ("svx_batch_result_t", abi.SvxBatchResult),
            ("svx_batch_stats_t", abi.SvxBatchStats), ("svx_serve_opts_t", abi.SvxServeOpts),
-           ("svx_serve_result_t", abi.SvxServeResult), ("svx_serve_stats_t", abi.SvxServeStats)]
+           ("svx_serve_result_t", abi.SvxServeResult), ("svx_serve_stats_t", abi.SvxServeStats),
+           ("svx_thermal_model_t", abi.SvxThermalModel)]
 
 
 def test_ctypes_mirrors_match_the_c_header_layout(tmp_path):
