@@ -50,15 +50,15 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None,
-                    help="plain and batched forms: fp64 (default); served form: mixed "
-                         "(default, as its workload specifies)")
+                    help="plain, batched and served forms: fp64 (default) or the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batched", "precision", "served"],
+    ap.add_argument("--form", choices=["plain", "batched", "precision", "served", "thermal"],
                     default="plain",
                     help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
                          "2D plates in one launch; precision: FP64 vs mixed on the "
                          "480x48x48 heterogeneous C3D8 model; served: Poisson request "
-                         "stream through the continuous-batching server")
+                         "stream through the continuous-batching server; thermal: steady "
+                         "conduction in a 480x48x48 C3D8 block")
     ap.add_argument("--requests", type=int, default=20000,
                     help="served form: requests per rate point")
     ap.add_argument("--rates", type=str, default="",
@@ -785,6 +785,114 @@ def run_served(args, rank, world, local_rank):
     return line
 
 
+THERMAL_NAME = ("steady conduction in a C3D8 block 480x48x48 over 2.0x0.2x0.2 m (1,154,881 "
+                "nodes = DOF, 30,297,025 nnz), k=45, uniform source 1e5, T=20 on x=0 and T=80 "
+                "on x=L; relative residual 1e-10")
+
+
+def thermal_block(nx, ny, nz, lx, ly, lz, k=45.0, source=1e5):
+    """Structured C3D8 conduction block (k-major node order) with fixed
+    temperatures on the x = 0 and x = L faces."""
+    import numpy as np
+
+    from solvix_b200.marshal import ThermalModel
+
+    i, j, kk = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1),
+                           indexing="ij")
+    i, j, kk = (a.transpose(2, 1, 0).ravel() for a in (i, j, kk))
+    xyz = np.stack([lx * i / nx, ly * j / ny, lz * kk / nz], axis=1)
+    p = (ny + 1) * (nx + 1)
+    ei, ej, ek = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    base = (ek * p + ej * (nx + 1) + ei).transpose(2, 1, 0).ravel()
+    offs = np.array([0, 1, nx + 2, nx + 1, p, p + 1, p + nx + 2, p + nx + 1])
+    conn = (base[:, None] + offs[None, :]).ravel()
+    ne = nx * ny * nz
+    cold = np.flatnonzero(i == 0)
+    hot = np.flatnonzero(i == nx)
+    return ThermalModel(xyz, np.full(ne, 5, dtype=np.uint8), np.arange(ne + 1) * 8, conn, k,
+                        source=source, temp_node=np.concatenate([cold, hot]),
+                        temp_value=np.concatenate([np.full(cold.size, 20.0),
+                                                   np.full(hot.size, 80.0)]))
+
+
+def run_thermal(args, rank, world, local_rank):
+    """Steady conduction (svx_solve_thermal_flat) on one GPU: each step one
+    full solve from the host model to host temperatures (upload, conduction
+    matrices, pattern, assembly, loads, temperature rows, PCG, download),
+    wall clock.  The CPU leg times the oracle on a 120x12x12 block."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle
+    from solvix_b200 import Context
+    from solvix_b200.kernel_timer import pcg_iteration_bytes
+
+    torch.cuda.set_device(local_rank)
+    nx, ny, nz = 480, 48, 48
+    tm = thermal_block(nx, ny, nz, 2.0, 0.2, 0.2)
+    n = tm.n_nodes
+    nnz = (3 * (nx + 1) - 2) * (3 * (ny + 1) - 2) * (3 * (nz + 1) - 2)
+    ctx = Context(local_rank)
+    lib = ctx.lib
+    for _ in range(max(args.warmup, 0)):
+        ctx.solve_thermal(tm)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = lib.svx_launch_count()
+    walls, iters = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, it, res = ctx.solve_thermal(tm)
+        walls.append(time.perf_counter() - t0)
+        iters.append(it)
+    launches = lib.svx_launch_count() - launches0
+    clk = clocks.stop()
+    ctx.close()
+    wall = float(sum(walls))
+    dof_it = float(n * sum(iters))
+    value = dof_it / wall
+    peak, peak_kind = measured_peaks()
+    bytes_it = pcg_iteration_bytes(n, nnz, 1, n)
+    achieved = bytes_it * sum(iters) / wall / 1e9
+    line = {
+        "metric": METRIC, "form": "thermal", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (structured block; no public dataset exists for this path)",
+        "config": {"workload": THERMAL_NAME, "n_dof": n, "nnz": nnz,
+                   "l2": "K 256 MB per solve vs 126 MB L2"},
+        "solves_per_s": args.steps / wall, "iterations": int(np.median(iters)),
+        "residual": res,
+        "e2e": {"value": value, "unit": UNIT,
+                "note": "svx_solve_thermal_flat from host arrays to host temperatures; the "
+                        "value is this same wall-clock figure",
+                "h2d_bytes_per_step": int(tm.xyz.nbytes + tm.conn.nbytes + tm.conn_ptr.nbytes
+                                          + tm.kind.nbytes + tm.temp_node.nbytes
+                                          + tm.temp_value.nbytes),
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "pcg_persistent2_kernel<1, 16, double> and the "
+                     "assembly kernels, whole solve",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_iteration": bytes_it,
+                     "note": "PCG algorithmic bytes over the whole solve's wall clock (assembly "
+                             "and copies included): a lower bound of the kernel's rate",
+                     "traffic": None},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        small = thermal_block(120, 12, 12, 0.5, 0.05, 0.05)
+        threads = max(1, min(8, os.cpu_count() or 1))
+        t0 = time.perf_counter()
+        _, it_c, _ = oracle.solve_thermal(small, threads=threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": small.n_nodes * it_c / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one full oracle conduction solve of a 120x12x12 block ({small.n_nodes} "
+                      f"DOF, {it_c} PCG iterations) on {threads} threads in {dt:.2f} s"}
+    return line
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -808,6 +916,8 @@ def main():
             line = run_served(args, rank, world, local_rank)
         elif args.form == "precision":
             line = run_precision(args, rank, world, local_rank) if rank == 0 else None
+        elif args.form == "thermal":
+            line = run_thermal(args, rank, world, local_rank) if rank == 0 else None
         else:
             line = run_ours(args, rank, world, local_rank)
     finally:
