@@ -46,7 +46,8 @@ enum svx_status {
     SVX_OOM = 5,             /* device memory (or admission budget) exhausted */
     SVX_CUDA_ERROR = 6,      /* no device, launch failure, driver error */
     SVX_BAD_ARGUMENT = 7,    /* null pointer, inconsistent sizes */
-    SVX_QUEUE_EMPTY = 8      /* server poll: nothing completed yet */
+    SVX_QUEUE_EMPTY = 8,     /* server poll: nothing completed yet */
+    SVX_IO_ERROR = 9         /* a file could not be written (std::io::Error) */
 };
 
 /* Element kinds, in the order of the reference's ElemKind enum
@@ -311,6 +312,38 @@ typedef struct svx_thermal_model {
 int svx_solve_thermal_flat(svx_ctx_t* ctx, const svx_thermal_model_t* model,
                            const svx_solve_opts_t* opts, double* temperatures,
                            int64_t* iterations, double* residual, svx_error_t* err);
+
+/* ---- VTU output ---------------------------------------------------- */
+/* What the reference's writers read from a Model and a Solution
+ * (crates/solvix-io/src/vtu.rs), with node ids already resolved to 0-based
+ * indices.  Arrays shorter than the mesh print 0 beyond their length, as
+ * the reference's `.get(i).unwrap_or(0)` does. */
+typedef struct svx_vtu_data {
+    int64_t n_nodes;
+    const double* xyz;                  /* [3 * n_nodes] */
+    int64_t n_elem;
+    const uint8_t* kind;                /* [n_elem] enum svx_elem_kind */
+    const int64_t* conn_ptr;            /* [n_elem + 1] */
+    const int32_t* conn;                /* 0-based node indices */
+    int64_t n_disp;                     /* displacement triplets available */
+    const double* displacements;        /* [3 * n_disp] (Solution::displacements) */
+    int64_t n_von_mises;                /* centroid values available */
+    const double* von_mises;            /* [n_von_mises] */
+    int32_t n_extra;                    /* extra scalar PointData arrays (ASCII only) */
+    const char* const* extra_names;     /* [n_extra] */
+    const double* const* extra_values;  /* [n_extra] */
+    const int64_t* extra_len;           /* [n_extra] values available per array */
+} svx_vtu_data_t;
+
+/* Writes `path` byte for byte as the reference's ASCII writer
+ * (vtu.rs:14-115, write_vtu / write_vtu_ex) when binary == 0, or as its
+ * appended raw binary writer (vtu.rs:148-288, write_vtu_binary) when
+ * binary == 1.  The ASCII lines are formatted on `threads` host threads
+ * (<= 0: all cores); the bytes do not depend on the thread count.  Returns
+ * SVX_OK, SVX_BAD_ARGUMENT, SVX_OOM or SVX_IO_ERROR (with the reference's
+ * text when an appended block exceeds the Int32 byte-count header). */
+int svx_write_vtu(const char* path, const svx_vtu_data_t* data, int32_t binary, int32_t threads,
+                  svx_error_t* err);
 
 /* ---- batched solves (many independent models in one launch) -------- */
 typedef struct svx_batch_result {

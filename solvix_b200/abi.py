@@ -27,6 +27,7 @@ SVX_OOM = 5
 SVX_CUDA_ERROR = 6
 SVX_BAD_ARGUMENT = 7
 SVX_QUEUE_EMPTY = 8
+SVX_IO_ERROR = 9
 
 # enum svx_elem_kind (order of ElemKind, crates/solvix-core/src/lib.rs:54-73)
 SVX_CPS3, SVX_CPS4, SVX_CPS8, SVX_CPE4, SVX_CPE8, SVX_C3D8, SVX_C3D4, SVX_B31 = range(8)
@@ -199,6 +200,26 @@ class SvxThermalModel(C.Structure):
     ]
 
 
+class SvxVtuData(C.Structure):
+    """svx_vtu_data_t (what vtu.rs's writers read)."""
+    _fields_ = [
+        ("n_nodes", C.c_int64),
+        ("xyz", c_double_p),
+        ("n_elem", C.c_int64),
+        ("kind", c_uint8_p),
+        ("conn_ptr", c_int64_p),
+        ("conn", c_int32_p),
+        ("n_disp", C.c_int64),
+        ("displacements", c_double_p),
+        ("n_von_mises", C.c_int64),
+        ("von_mises", c_double_p),
+        ("n_extra", C.c_int32),
+        ("extra_names", C.POINTER(C.c_char_p)),
+        ("extra_values", C.POINTER(c_double_p)),
+        ("extra_len", c_int64_p),
+    ]
+
+
 class SvxServeOpts(C.Structure):
     _fields_ = [
         ("hbm_budget_bytes", C.c_int64),
@@ -297,6 +318,8 @@ SIGNATURES = {
                                  C.POINTER(SvxSolution), C.POINTER(SvxError)]),
     "svx_solve_resolved": (C.c_int, [_VP, _VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),
                                      C.POINTER(SvxError)]),
+    "svx_write_vtu": (C.c_int, [C.c_char_p, C.POINTER(SvxVtuData), C.c_int32, C.c_int32,
+                                C.POINTER(SvxError)]),
     "svx_solve_thermal_flat": (C.c_int, [_VP, C.POINTER(SvxThermalModel),
                                          C.POINTER(SvxSolveOpts), c_double_p, c_int64_p,
                                          c_double_p, C.POINTER(SvxError)]),
