@@ -47,7 +47,9 @@ enum svx_status {
     SVX_CUDA_ERROR = 6,      /* no device, launch failure, driver error */
     SVX_BAD_ARGUMENT = 7,    /* null pointer, inconsistent sizes */
     SVX_QUEUE_EMPTY = 8,     /* server poll: nothing completed yet */
-    SVX_IO_ERROR = 9         /* a file could not be written (std::io::Error) */
+    SVX_IO_ERROR = 9,        /* a file could not be written (std::io::Error) */
+    SVX_PARSE_ERROR = 10,    /* a deck the reference's parser rejects (ParseError) */
+    SVX_UNSUPPORTED = 11     /* a deck outside the linear-static reader's keywords */
 };
 
 /* Element kinds, in the order of the reference's ElemKind enum
@@ -312,6 +314,28 @@ typedef struct svx_thermal_model {
 int svx_solve_thermal_flat(svx_ctx_t* ctx, const svx_thermal_model_t* model,
                            const svx_solve_opts_t* opts, double* temperatures,
                            int64_t* iterations, double* residual, svx_error_t* err);
+
+/* ---- .inp reader (linear-static decks) ------------------------------ */
+/* The reference's parse_inp (crates/solvix-io/src/parser.rs:87-1370) for the
+ * keywords of linear-static decks (*HEADING, *NODE, *ELEMENT, *NSET, *ELSET
+ * [GENERATE], *MATERIAL, *ELASTIC, *SOLID SECTION, *STEP, *STATIC,
+ * *BOUNDARY, *CLOAD, *END STEP; unknown keywords are warned and skipped
+ * like the reference does), producing the model svx_resolve consumes with
+ * the BCs and loads of Model::load_state (lib.rs:388-403).  Returns SVX_OK,
+ * SVX_PARSE_ERROR (err->elem_index = the 1-based line, err->message the
+ * reference's ParseError message) or SVX_UNSUPPORTED (a keyword the
+ * reference reads with another meaning, or *STEP, NLGEOM=YES: parse that
+ * deck with the reference's parser). */
+typedef struct svx_inp svx_inp_t;
+int svx_inp_parse(const char* text, int64_t len, svx_inp_t** out, svx_error_t* err);
+/* The parsed model (valid until svx_inp_free). */
+const svx_model_desc_t* svx_inp_model(const svx_inp_t* inp);
+/* *STEP blocks read (the model's steps.len()). */
+int32_t svx_inp_step_count(const svx_inp_t* inp);
+/* ParseReport::warnings, in order. */
+int32_t svx_inp_warning_count(const svx_inp_t* inp);
+const char* svx_inp_warning(const svx_inp_t* inp, int32_t i);
+void svx_inp_free(svx_inp_t* inp);
 
 /* ---- VTU output ---------------------------------------------------- */
 /* What the reference's writers read from a Model and a Solution

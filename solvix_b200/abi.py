@@ -28,6 +28,8 @@ SVX_CUDA_ERROR = 6
 SVX_BAD_ARGUMENT = 7
 SVX_QUEUE_EMPTY = 8
 SVX_IO_ERROR = 9
+SVX_PARSE_ERROR = 10
+SVX_UNSUPPORTED = 11
 
 # enum svx_elem_kind (order of ElemKind, crates/solvix-core/src/lib.rs:54-73)
 SVX_CPS3, SVX_CPS4, SVX_CPS8, SVX_CPE4, SVX_CPE8, SVX_C3D8, SVX_C3D4, SVX_B31 = range(8)
@@ -320,6 +322,12 @@ SIGNATURES = {
                                      C.POINTER(SvxError)]),
     "svx_write_vtu": (C.c_int, [C.c_char_p, C.POINTER(SvxVtuData), C.c_int32, C.c_int32,
                                 C.POINTER(SvxError)]),
+    "svx_inp_parse": (C.c_int, [C.c_char_p, C.c_int64, C.POINTER(_VP), C.POINTER(SvxError)]),
+    "svx_inp_model": (C.POINTER(SvxModelDesc), [_VP]),
+    "svx_inp_step_count": (C.c_int32, [_VP]),
+    "svx_inp_warning_count": (C.c_int32, [_VP]),
+    "svx_inp_warning": (C.c_char_p, [_VP, C.c_int32]),
+    "svx_inp_free": (None, [_VP]),
     "svx_solve_thermal_flat": (C.c_int, [_VP, C.POINTER(SvxThermalModel),
                                          C.POINTER(SvxSolveOpts), c_double_p, c_int64_p,
                                          c_double_p, C.POINTER(SvxError)]),
