@@ -63,6 +63,13 @@ _SIG = {
                                  C.c_int, abi.c_double_p, abi.c_int64_p, abi.c_double_p]),
     "svx_oracle_solve": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_int, C.c_double, C.c_int64,
                                    C.POINTER(abi.SvxSolution), C.POINTER(abi.SvxError)]),
+    "svx_oracle_solve_method": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_int, C.c_double,
+                                          C.c_int64, C.c_int, C.POINTER(abi.SvxSolution),
+                                          C.POINTER(C.c_int), C.POINTER(abi.SvxError)]),
+    "svx_oracle_rcm": (None, [C.POINTER(OracleCsr), abi.c_int64_p]),
+    "svx_oracle_ldlt": (C.c_int, [C.POINTER(OracleCsr), abi.c_double_p, C.c_int, abi.c_double_p,
+                                  abi.c_double_p, abi.c_double_p, abi.c_double_p, abi.c_int64_p,
+                                  C.POINTER(abi.SvxError)]),
     "svx_oracle_stress": (C.c_int, [C.POINTER(abi.SvxFlatModel), abi.c_double_p, C.c_int,
                                     abi.c_double_p, abi.c_double_p, abi.c_double_p,
                                     C.POINTER(abi.SvxError)]),
@@ -319,6 +326,42 @@ def pcg(k: Csr, f, tol=1e-10, max_iter=1000, threads: int | None = None):
     return st, u, int(it.value), float(res.value)
 
 
+def rcm(k: Csr):
+    """Reverse Cuthill-McKee permutation, old -> new (ldl.rs:27-60)."""
+    perm = np.zeros(k.n, dtype=np.int64)
+    s = k.struct()
+    lib().svx_oracle_rcm(C.byref(s), abi.ptr(perm, C.c_int64))
+    return perm
+
+
+class LdltResult:
+    def __init__(self, u, residual, cond, d, nnz_l):
+        self.u, self.residual, self.cond, self.d, self.nnz_l = u, residual, cond, d, nnz_l
+
+
+def ldlt(k: Csr, f, threads: int | None = None) -> LdltResult:
+    """Factorize the (Dirichlet-modified) k and solve k u = f as the
+    reference's direct path (ldl.rs:144-265, lib.rs:645-663); raises
+    InvalidModel with the reference's pivot message."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    u = np.zeros(k.n)
+    d = np.zeros(k.n)
+    res = C.c_double(0.0)
+    cond = C.c_double(0.0)
+    nnz_l = C.c_int64(0)
+    err = abi.SvxError()
+    s = k.struct()
+    st = lib().svx_oracle_ldlt(C.byref(s), abi.ptr(f, C.c_double), threads or default_threads(),
+                               abi.ptr(u, C.c_double), C.byref(res), C.byref(cond),
+                               abi.ptr(d, C.c_double), C.byref(nnz_l), C.byref(err))
+    if st != abi.SVX_OK:
+        _raise_err(err)
+    return LdltResult(u, float(res.value), float(cond.value), d, int(nnz_l.value))
+
+
+METHODS = {"pcg": 0, "ldlt": 1, "auto": 2}
+
+
 class OracleSolution:
     def __init__(self, flat: FlatModel):
         n = flat.n_dof
@@ -330,10 +373,13 @@ class OracleSolution:
         self.iterations = 0
         self.final_residual = 0.0
         self.cond_estimate = 0.0
+        self.solver_method = "pcg"
 
 
-def solve_flat(flat: FlatModel, tol=1e-10, max_iter=0, threads: int | None = None):
-    """Full linear-static pipeline on a flat model; raises SolveError."""
+def solve_flat(flat: FlatModel, tol=1e-10, max_iter=0, threads: int | None = None,
+               method: str = "pcg"):
+    """Full linear-static pipeline on a flat model with the reference's
+    Method ("pcg", "ldlt" or "auto", lib.rs:664-686); raises SolveError."""
     out = OracleSolution(flat)
     sol = abi.SvxSolution()
     sol.u = abi.ptr(out.u, C.c_double)
@@ -343,10 +389,13 @@ def solve_flat(flat: FlatModel, tol=1e-10, max_iter=0, threads: int | None = Non
     sol.reactions = abi.ptr(out.reaction_values, C.c_double)
     err = abi.SvxError()
     s = flat.as_struct()
-    st = lib().svx_oracle_solve(C.byref(s), threads or default_threads(), tol, max_iter,
-                                C.byref(sol), C.byref(err))
+    used = C.c_int(0)
+    st = lib().svx_oracle_solve_method(C.byref(s), threads or default_threads(), tol, max_iter,
+                                       METHODS[method], C.byref(sol), C.byref(used),
+                                       C.byref(err))
     if st != abi.SVX_OK:
         _raise_err(err)
+    out.solver_method = "ldlt" if used.value == 1 else "pcg"
     out.iterations = int(sol.iterations)
     out.final_residual = float(sol.final_residual)
     out.cond_estimate = float(sol.cond_estimate)
@@ -369,14 +418,15 @@ def stress(flat: FlatModel, u, threads: int | None = None):
     return vm, vmn, re
 
 
-def solve(model: Model, tol=1e-10, threads: int | None = None):
-    """Reference-order solve of a reference-shaped model (Method::Pcg)."""
+def solve(model: Model, tol=1e-10, threads: int | None = None, method: str = "pcg"):
+    """Reference-order solve of a reference-shaped model (Method::Pcg by
+    default; "ldlt" and "auto" as in lib.rs:664-686)."""
     flat, pending = resolve(model)
     if pending is not None:
         # Element failures come first (assembly runs before the CLOAD loop).
         assemble(flat, threads)
         raise pending.err
-    return solve_flat(flat, tol=tol, threads=threads), flat
+    return solve_flat(flat, tol=tol, threads=threads, method=method), flat
 
 
 # ------------------------------------------------------------------ thermal

@@ -20,6 +20,7 @@
 #include "svx_oracle.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1058,8 +1059,252 @@ int svx_oracle_pcg(const svx_oracle_csr_t* k, const double* f, double tol, int64
 
 // lib.rs:593-716 (Method::Pcg): assemble -> keep K, f -> Dirichlet -> PCG
 // -> jacobi_cond -> displacements -> stresses -> reactions.
+namespace {
+
+// ------------------------------------------------------------------- LDL^T
+// ldl.rs restated: reverse Cuthill-McKee ordering, permuted copy, elimination
+// tree, up-looking LDL^T with L in CSR rows, and its solve.  Every loop keeps
+// the reference's order, so L, D and the solution are bit-identical.
+constexpr int64_t kNone = -1;  // usize::MAX of the reference (root / unset)
+
+// ldl.rs:27-60.  Returns perm (old index -> new index).
+std::vector<int64_t> rcm_perm(const svx_oracle_csr_t& k) {
+    const int64_t n = k.n;
+    std::vector<int64_t> perm(n, kNone), order;
+    order.reserve(n);
+    std::vector<char> visited(n, 0);
+    std::vector<int64_t> queue;
+    while (int64_t(order.size()) < n) {
+        // min_by_key keeps the first of equal minima
+        int64_t start = kNone, best = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            if (visited[i]) continue;
+            int64_t deg = k.row_ptr[i + 1] - k.row_ptr[i];
+            if (start == kNone || deg < best) {
+                start = i;
+                best = deg;
+            }
+        }
+        visited[start] = 1;
+        queue.assign(1, start);
+        for (size_t head = 0; head < queue.size(); ++head) {
+            int64_t u = queue[head];
+            order.push_back(u);
+            for (int64_t idx = k.row_ptr[u]; idx < k.row_ptr[u + 1]; ++idx) {
+                int64_t v = k.col_idx[idx];
+                if (!visited[v]) {
+                    visited[v] = 1;
+                    queue.push_back(v);
+                }
+            }
+        }
+    }
+    for (int64_t pos = 0; pos < n; ++pos) perm[order[n - 1 - pos]] = pos;
+    return perm;
+}
+
+struct HostCsr {
+    std::vector<int64_t> row_ptr, col_idx;
+    std::vector<double> vals;
+};
+
+// ldl.rs:63-85: out[r][c] = a[invp[r]][invp[c]], each row sorted by column
+// (columns are unique within a row, so the sort order is fully determined).
+HostCsr permuted(const svx_oracle_csr_t& k, const std::vector<int64_t>& perm,
+                 const std::vector<int64_t>& invp) {
+    HostCsr a;
+    a.row_ptr.reserve(k.n + 1);
+    a.row_ptr.push_back(0);
+    a.col_idx.reserve(k.nnz);
+    a.vals.reserve(k.nnz);
+    std::vector<std::pair<int64_t, double>> row;
+    for (int64_t old : invp) {
+        row.clear();
+        for (int64_t p = k.row_ptr[old]; p < k.row_ptr[old + 1]; ++p)
+            row.emplace_back(perm[k.col_idx[p]], k.vals[p]);
+        std::sort(row.begin(), row.end(),
+                  [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (const auto& cv : row) {
+            a.col_idx.push_back(cv.first);
+            a.vals.push_back(cv.second);
+        }
+        a.row_ptr.push_back(int64_t(a.col_idx.size()));
+    }
+    return a;
+}
+
+// ldl.rs:89-110 (path compression through `ancestor`).
+std::vector<int64_t> elimination_tree(const HostCsr& a) {
+    const int64_t n = int64_t(a.row_ptr.size()) - 1;
+    std::vector<int64_t> parent(n, kNone), ancestor(n, kNone);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t p = a.row_ptr[i]; p < a.row_ptr[i + 1]; ++p) {
+            int64_t node = a.col_idx[p];
+            while (node < i) {
+                int64_t next = ancestor[node];
+                ancestor[node] = i;
+                if (next == kNone) {
+                    parent[node] = i;
+                    break;
+                }
+                node = next;
+            }
+        }
+    return parent;
+}
+
+// ldl.rs:115-136 (cs_ereach): the pattern of row i of L, unsorted.
+void ereach(const HostCsr& a, const std::vector<int64_t>& parent, std::vector<int64_t>& seen,
+            int64_t i, std::vector<int64_t>& pattern) {
+    pattern.clear();
+    seen[i] = i;
+    for (int64_t p = a.row_ptr[i]; p < a.row_ptr[i + 1]; ++p) {
+        int64_t node = a.col_idx[p];
+        while (node < i && seen[node] != i) {
+            pattern.push_back(node);
+            seen[node] = i;
+            if (parent[node] == kNone) break;
+            node = parent[node];
+        }
+    }
+}
+
+struct Ldlt {
+    std::vector<int64_t> l_row_ptr, l_col_idx, invp;
+    std::vector<double> l_vals, d;
+};
+
+// ldl.rs:144-221.  Returns SVX_OK, or SVX_INVALID_MODEL with the reference's
+// pivot message in msg.
+int ldlt_factorize(const svx_oracle_csr_t& k, Ldlt& out, std::string& msg) {
+    const int64_t n = k.n;
+    std::vector<int64_t> perm = rcm_perm(k);
+    out.invp.assign(n, 0);
+    for (int64_t old = 0; old < n; ++old) out.invp[perm[old]] = old;
+    HostCsr a = permuted(k, perm, out.invp);
+    std::vector<int64_t> parent = elimination_tree(a);
+    out.l_row_ptr.assign(1, 0);
+    out.l_col_idx.clear();
+    out.l_vals.clear();
+    out.d.assign(n, 0.0);
+    std::vector<double> x(n, 0.0);
+    std::vector<int64_t> seen(n, kNone), pattern;
+    for (int64_t i = 0; i < n; ++i) {
+        ereach(a, parent, seen, i, pattern);
+        std::sort(pattern.begin(), pattern.end());
+        double aii = 0.0, row_max = 0.0;
+        for (int64_t p = a.row_ptr[i]; p < a.row_ptr[i + 1]; ++p) {
+            int64_t c = a.col_idx[p];
+            x[c] = a.vals[p];
+            row_max = std::fmax(row_max, std::fabs(a.vals[p]));
+            if (c == i) aii = a.vals[p];
+        }
+        for (int64_t kk : pattern) {
+            double w = x[kk];
+            for (int64_t p = out.l_row_ptr[kk]; p < out.l_row_ptr[kk + 1]; ++p)
+                w -= out.l_vals[p] * x[out.l_col_idx[p]];
+            x[kk] = w;
+            double lik = w / out.d[kk];
+            aii -= lik * w;
+            out.l_col_idx.push_back(kk);
+            out.l_vals.push_back(lik);
+        }
+        out.l_row_ptr.push_back(int64_t(out.l_col_idx.size()));
+        for (int64_t kk : pattern) x[kk] = 0.0;
+        for (int64_t p = a.row_ptr[i]; p < a.row_ptr[i + 1]; ++p) x[a.col_idx[p]] = 0.0;
+        if (!std::isfinite(aii) || aii <= 1e-13 * std::fmax(row_max, DBL_MIN)) {
+            msg = std::string("stiffness matrix is not positive definite (pivot ") +
+                  (aii < 0.0 ? "negative" : "near-zero") + " at equation " +
+                  std::to_string(i) + ")";
+            return SVX_INVALID_MODEL;
+        }
+        out.d[i] = aii;
+    }
+    return SVX_OK;
+}
+
+// ldl.rs:224-251.
+void ldlt_solve(const Ldlt& fa, const double* b, double* xout) {
+    const int64_t n = int64_t(fa.d.size());
+    std::vector<double> y(n);
+    for (int64_t i = 0; i < n; ++i) y[i] = b[fa.invp[i]];
+    for (int64_t i = 0; i < n; ++i) {
+        double s = y[i];
+        for (int64_t p = fa.l_row_ptr[i]; p < fa.l_row_ptr[i + 1]; ++p)
+            s -= fa.l_vals[p] * y[fa.l_col_idx[p]];
+        y[i] = s;
+    }
+    for (int64_t i = 0; i < n; ++i) y[i] /= fa.d[i];
+    for (int64_t i = n - 1; i >= 0; --i) {
+        double xi = y[i];
+        for (int64_t p = fa.l_row_ptr[i]; p < fa.l_row_ptr[i + 1]; ++p)
+            y[fa.l_col_idx[p]] -= fa.l_vals[p] * xi;
+    }
+    for (int64_t i = 0; i < n; ++i) xout[fa.invp[i]] = y[i];
+}
+
+// ldl.rs:256-265.
+double ldlt_cond(const Ldlt& fa) {
+    double lo = INFINITY, hi = 0.0;
+    for (double dv : fa.d) {
+        lo = std::fmin(lo, std::fabs(dv));
+        hi = std::fmax(hi, std::fabs(dv));
+    }
+    return hi / lo;
+}
+
+}  // namespace
+
+void svx_oracle_rcm(const svx_oracle_csr_t* k, int64_t* perm) {
+    std::vector<int64_t> p = rcm_perm(*k);
+    std::copy(p.begin(), p.end(), perm);
+}
+
+// The `direct` closure of lib.rs:645-663: factorize, solve, the relative
+// residual ||f - K u|| / ||f|| (0 when f is zero) and the D-based estimate.
+int svx_oracle_ldlt(const svx_oracle_csr_t* k, const double* f, int threads, double* u,
+                    double* residual, double* cond, double* d, int64_t* nnz_l,
+                    svx_error_t* err) {
+    Ldlt fa;
+    std::string msg;
+    int st = ldlt_factorize(*k, fa, msg);
+    if (st != SVX_OK) {
+        set_error(err, st, 0, -1, msg.c_str());
+        return st;
+    }
+    const int64_t n = k->n;
+    ldlt_solve(fa, f, u);
+    double b2 = 0.0;
+    for (int64_t i = 0; i < n; ++i) b2 += f[i] * f[i];
+    double b_norm = std::sqrt(b2);
+    double res = 0.0;
+    if (b_norm != 0.0) {
+        std::vector<double> r(n);
+        svx_oracle_spmv(k, u, r.data(), threads);
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            double v = f[i] - r[i];
+            s += v * v;
+        }
+        res = std::sqrt(s) / b_norm;
+    }
+    if (residual) *residual = res;
+    if (cond) *cond = ldlt_cond(fa);
+    if (d) std::copy(fa.d.begin(), fa.d.end(), d);
+    if (nnz_l) *nnz_l = int64_t(fa.l_vals.size());
+    if (err) set_error(err, SVX_OK, 0, -1, "");
+    return SVX_OK;
+}
+
 int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t max_iter,
                      svx_solution_t* sol, svx_error_t* err) {
+    return svx_oracle_solve_method(m, threads, tol, max_iter, SVX_ORACLE_METHOD_PCG, sol,
+                                   nullptr, err);
+}
+
+int svx_oracle_solve_method(const svx_flat_model_t* m, int threads, double tol,
+                            int64_t max_iter, int method, svx_solution_t* sol,
+                            int* method_used, svx_error_t* err) {
     svx_oracle_csr_t k;
     int st = svx_oracle_assemble(m, threads, &k, err);
     if (st != SVX_OK) return st;
@@ -1079,34 +1324,53 @@ int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t
     if (max_iter <= 0) max_iter = std::max<int64_t>(1000, 10 * n);
     std::vector<double> u(n, 0.0);
     int64_t iters = 0;
-    double res = 0.0;
-    st = svx_oracle_pcg(&k, f.data(), tol, max_iter, threads, u.data(), &iters, &res);
-    if (st != SVX_OK) {
-        char msg[200];
-        std::snprintf(msg, sizeof msg, "not converged after %lld iterations",
-                      (long long)iters);
-        set_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
-        if (err) {
-            err->iterations = iters;
-            err->residual = res;
-        }
-        svx_oracle_csr_free(&k);
-        return st;
-    }
-    // jacobi_cond (lib.rs:634-644): extreme |diag| of the modified K.
-    double hi = 0.0, lo = INFINITY;
-    for (int64_t i = 0; i < n; ++i)
-        for (int64_t idx = k.row_ptr[i]; idx < k.row_ptr[i + 1]; ++idx)
-            if (k.col_idx[idx] == i) {
-                double a = std::fabs(k.vals[idx]);
-                hi = std::fmax(hi, a);
-                lo = std::fmin(lo, a);
-                break;
+    double res = 0.0, cond = 0.0;
+    // lib.rs:664-686: Pcg, Ldlt, or Auto (PCG, then the direct path when
+    // PCG returns NotConverged).
+    bool direct = method == SVX_ORACLE_METHOD_LDLT;
+    if (!direct) {
+        st = svx_oracle_pcg(&k, f.data(), tol, max_iter, threads, u.data(), &iters, &res);
+        if (st != SVX_OK && method == SVX_ORACLE_METHOD_AUTO) {
+            direct = true;
+        } else if (st != SVX_OK) {
+            char msg[200];
+            std::snprintf(msg, sizeof msg, "not converged after %lld iterations",
+                          (long long)iters);
+            set_error(err, SVX_NOT_CONVERGED, 0, -1, msg);
+            if (err) {
+                err->iterations = iters;
+                err->residual = res;
             }
+            svx_oracle_csr_free(&k);
+            return st;
+        }
+    }
+    if (direct) {
+        iters = 0;
+        st = svx_oracle_ldlt(&k, f.data(), threads, u.data(), &res, &cond, nullptr, nullptr,
+                             err);
+        if (st != SVX_OK) {
+            svx_oracle_csr_free(&k);
+            return st;
+        }
+    } else {
+        // jacobi_cond (lib.rs:634-644): extreme |diag| of the modified K.
+        double hi = 0.0, lo = INFINITY;
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t idx = k.row_ptr[i]; idx < k.row_ptr[i + 1]; ++idx)
+                if (k.col_idx[idx] == i) {
+                    double a = std::fabs(k.vals[idx]);
+                    hi = std::fmax(hi, a);
+                    lo = std::fmin(lo, a);
+                    break;
+                }
+        cond = hi / lo;
+    }
+    if (method_used) *method_used = direct ? SVX_ORACLE_METHOD_LDLT : SVX_ORACLE_METHOD_PCG;
     sol->iterations = iters;
     sol->outer_iterations = 0;
     sol->final_residual = res;
-    sol->cond_estimate = hi / lo;
+    sol->cond_estimate = cond;
     if (sol->u) std::memcpy(sol->u, u.data(), sizeof(double) * n);
     if (sol->displacements)
         for (int64_t i = 0; i < m->n_nodes; ++i) {

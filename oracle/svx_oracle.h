@@ -59,10 +59,34 @@ void svx_oracle_apply_dirichlet(svx_oracle_csr_t* k, double* f, const int64_t* r
 int svx_oracle_pcg(const svx_oracle_csr_t* k, const double* f, double tol, int64_t max_iter,
                    int threads, double* u, int64_t* iterations, double* residual);
 
-/* Full linear-static pipeline (lib.rs:593-716 without the LDLT fallback;
- * Method::Pcg).  Output arrays of `sol` are caller-allocated. */
+/* Full linear-static pipeline (lib.rs:593-716) with Method::Pcg.  Output
+ * arrays of `sol` are caller-allocated. */
 int svx_oracle_solve(const svx_flat_model_t* m, int threads, double tol, int64_t max_iter,
                      svx_solution_t* sol, svx_error_t* err);
+
+/* lib.rs:525-535 Method. */
+enum { SVX_ORACLE_METHOD_PCG = 0, SVX_ORACLE_METHOD_LDLT = 1, SVX_ORACLE_METHOD_AUTO = 2 };
+
+/* The same pipeline with a Method (lib.rs:664-686): Ldlt factorizes directly,
+ * Auto runs the PCG and factorizes when it returns NotConverged.  On the
+ * direct path iterations is 0, final_residual ||f - K u|| / ||f|| and
+ * cond_estimate max|D| / min|D|.  *method_used (may be NULL) receives the
+ * method that produced u (PCG or LDLT). */
+int svx_oracle_solve_method(const svx_flat_model_t* m, int threads, double tol,
+                            int64_t max_iter, int method, svx_solution_t* sol,
+                            int* method_used, svx_error_t* err);
+
+/* Reverse Cuthill-McKee permutation of k's pattern, old -> new
+ * (ldl.rs:27-60). */
+void svx_oracle_rcm(const svx_oracle_csr_t* k, int64_t* perm);
+
+/* Ldlt::factorize + Ldlt::solve (ldl.rs:144-251) of a Dirichlet-modified k,
+ * then the residual and estimate of lib.rs:645-663.  d (optional, [n]) gets
+ * D in the permuted order, nnz_l (optional) the entries of L.  Returns SVX_OK
+ * or SVX_INVALID_MODEL with the reference's pivot message. */
+int svx_oracle_ldlt(const svx_oracle_csr_t* k, const double* f, int threads, double* u,
+                    double* residual, double* cond, double* d, int64_t* nnz_l,
+                    svx_error_t* err);
 
 /* Stress + reaction recovery for a given u (stress.rs:22-118); K_orig for
  * the reactions is assembled with the current sort mode.  Output arrays may
