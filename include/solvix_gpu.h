@@ -169,6 +169,15 @@ enum svx_precision {
                           with the FP64 operator once the FP32 one stops gaining) */
 };
 
+/* Linear solver selection (Method, lib.rs:523-534; dispatch lib.rs:664-686). */
+enum svx_method {
+    SVX_METHOD_PCG = 0,   /* Jacobi-PCG; a budget overrun returns SVX_NOT_CONVERGED */
+    SVX_METHOD_LDLT = 1,  /* the direct path: RCM-ordered band LDL^T factorized on the
+                             device (replaces Ldlt::factorize / solve, ldl.rs:144-251) */
+    SVX_METHOD_AUTO = 2   /* Jacobi-PCG, then the direct path when it returns
+                             SVX_NOT_CONVERGED (Method::Auto, the reference's default) */
+};
+
 typedef struct svx_solve_opts {
     double tol;            /* relative residual tolerance (reference: 1e-10) */
     int64_t max_iter;      /* <= 0: max(1000, 10 * ndof_total) like lib.rs:632 */
@@ -178,6 +187,7 @@ typedef struct svx_solve_opts {
                               select 0.1 */
     int32_t check_every;   /* iterations per graph launch between host checks (0: auto) */
     int32_t want_stress;   /* 1: compute von Mises + reactions */
+    int32_t method;        /* enum svx_method (svx_default_opts: SVX_METHOD_PCG) */
 } svx_solve_opts_t;
 
 /* Results of one static solve; arrays are caller-allocated (NULL skips). */
@@ -195,6 +205,12 @@ typedef struct svx_solution {
     double ms_solve;           /* device time of the PCG */
     double ms_stress;          /* device time of stress + reaction recovery */
     int64_t fp32_iterations;   /* mixed: iterations on the FP32 operator */
+    int32_t solver_method;     /* SVX_METHOD_PCG or SVX_METHOD_LDLT: what produced u.  After
+                                  the direct path iterations is 0, final_residual
+                                  ||f - K u|| / ||f|| and cond_estimate max|D| / min|D|
+                                  (lib.rs:645-663, ldl.rs:256-265) */
+    int64_t factor_bandwidth;  /* direct path: half-bandwidth of K in the RCM order */
+    double ms_factor;          /* direct path: device time of the factorization + solve */
 } svx_solution_t;
 
 typedef struct svx_ctx svx_ctx_t;
@@ -203,7 +219,7 @@ typedef struct svx_op svx_op_t;
 /* Library version string. */
 const char* svx_version(void);
 
-/* Default options: tol 1e-10, max_iter auto, FP64, inner_tol 1e-5. */
+/* Default options: tol 1e-10, max_iter auto, FP64, inner_tol 1e-5, method PCG. */
 void svx_default_opts(svx_solve_opts_t* opts);
 
 /* ---- context ----------------------------------------------------- */
@@ -263,9 +279,22 @@ int svx_op_set_solution(svx_op_t* op, const double* u);
 /* ---- K5-K7: PCG --------------------------------------------------- */
 /* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644);
  * with opts->want_stress also K9-K10 (device-side, copied to the non-NULL
- * arrays of sol). */
+ * arrays of sol).  opts->method selects the Method dispatch of
+ * lib.rs:664-686: SVX_METHOD_LDLT and the fallback of SVX_METHOD_AUTO run
+ * the direct path on the device (Ldlt::factorize / solve, ldl.rs:144-265),
+ * whose failed pivot returns SVX_INVALID_MODEL with the reference's text
+ * ("stiffness matrix is not positive definite (pivot near-zero at equation
+ * 12)") and whose band (half-bandwidth x rows doubles) must fit in the
+ * device's free memory, else SVX_OOM. */
 int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol,
                  svx_error_t* err);
+
+/* The equation ordering of the direct path: the reverse Cuthill-McKee
+ * permutation (old row -> new row) of a symmetric CSR pattern, as the
+ * reference's rcm (ldl.rs:27-60) computes it, and the half-bandwidth
+ * max |perm[r] - perm[c]| over the pattern's entries.  Host only. */
+int svx_order_rcm(int64_t n, const int64_t* row_ptr, const int32_t* col_idx, int32_t* perm,
+                  int64_t* bandwidth);
 
 /* ---- K9-K10: stress + reactions ----------------------------------- */
 /* svx_op_solve with opts->want_stress = 1 also recovers the stresses into

@@ -40,6 +40,9 @@ SVX_NOALLOC_MAX_DOF = 262144
 # enum svx_precision
 SVX_FP64 = 0
 SVX_MIXED = 1
+SVX_METHOD_PCG = 0
+SVX_METHOD_LDLT = 1
+SVX_METHOD_AUTO = 2
 
 c_double_p = C.POINTER(C.c_double)
 c_int64_p = C.POINTER(C.c_int64)
@@ -130,6 +133,7 @@ class SvxSolveOpts(C.Structure):
         ("inner_tol", C.c_double),
         ("check_every", C.c_int32),
         ("want_stress", C.c_int32),
+        ("method", C.c_int32),
     ]
 
 
@@ -148,6 +152,9 @@ class SvxSolution(C.Structure):
         ("ms_solve", C.c_double),
         ("ms_stress", C.c_double),
         ("fp32_iterations", C.c_int64),
+        ("solver_method", C.c_int32),
+        ("factor_bandwidth", C.c_int64),
+        ("ms_factor", C.c_double),
     ]
 
 
@@ -298,6 +305,7 @@ SIGNATURES = {
     "svx_op_get_vectors": (C.c_int, [_VP, C.c_int, c_double_p, c_double_p]),
     "svx_op_spmv": (C.c_int, [_VP, c_double_p, c_double_p]),
     "svx_op_set_solution": (C.c_int, [_VP, c_double_p]),
+    "svx_order_rcm": (C.c_int, [C.c_int64, c_int64_p, c_int32_p, c_int32_p, c_int64_p]),
     "svx_op_solve": (C.c_int, [_VP, C.POINTER(SvxSolveOpts), C.POINTER(SvxSolution),
                                C.POINTER(SvxError)]),
     "svx_op_stress": (C.c_int, [_VP, C.POINTER(SvxSolution)]),
@@ -375,6 +383,7 @@ def default_opts(**kw) -> SvxSolveOpts:
     o.inner_tol = 1e-5
     o.check_every = 0
     o.want_stress = 1
+    o.method = SVX_METHOD_PCG
     for k, v in kw.items():
         setattr(o, k, v)
     return o

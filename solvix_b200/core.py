@@ -109,11 +109,15 @@ class Context:
 
     def solve_flat(self, flat: FlatModel, tol: float = 1e-10, max_iter: int = 0,
                    precision: int = abi.SVX_FP64, inner_tol: float = 1e-5,
-                   want_stress: bool = True, check_every: int = 0) -> Solution:
+                   want_stress: bool = True, check_every: int = 0,
+                   method: int = abi.SVX_METHOD_PCG) -> Solution:
+        """method: abi.SVX_METHOD_PCG (default), SVX_METHOD_LDLT (the direct
+        path on the device) or SVX_METHOD_AUTO (PCG, then the direct path
+        when it does not converge), lib.rs:664-686."""
         out = _SolutionBuffers(flat.n_nodes, flat.ndof, flat.n_elem, flat.fixed_row.shape[0])
         opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
                                 inner_tol=inner_tol, want_stress=int(want_stress),
-                                check_every=check_every)
+                                check_every=check_every, method=int(method))
         err = abi.SvxError()
         s = flat.as_struct()
         st = self.lib.svx_solve_flat(self.handle, C.byref(s), C.byref(opts),
@@ -161,7 +165,7 @@ class Context:
         return out, st_d
 
     def solve_model(self, model: Model, tol: float = 1e-10, precision: int = abi.SVX_FP64,
-                    inner_tol: float = 1e-5) -> Solution:
+                    inner_tol: float = 1e-5, method: int = abi.SVX_METHOD_AUTO) -> Solution:
         """The reference-shaped path: resolve ids / sets on the host (C++),
         then assemble, solve and recover stresses on the device."""
         _bcs, _cl, dloads, gravity = model.load_state()
@@ -178,7 +182,8 @@ class Context:
             flat_s = self.lib.svx_resolved_flat(res).contents
             n_nodes, ndof = int(flat_s.n_nodes), int(flat_s.ndof)
             out = _SolutionBuffers(n_nodes, ndof, int(flat_s.n_elem), int(flat_s.n_fixed))
-            opts = abi.default_opts(tol=tol, precision=precision, inner_tol=inner_tol)
+            opts = abi.default_opts(tol=tol, precision=precision, inner_tol=inner_tol,
+                                    method=int(method))
             st = self.lib.svx_solve_resolved(self.handle, res, C.byref(opts),
                                              C.byref(out.struct), C.byref(err))
             if st != abi.SVX_OK:
@@ -215,10 +220,12 @@ class _SolutionBuffers:
             displacements=self.disp, von_mises=self.vm, nodal_von_mises=self.vm_node,
             reactions=reactions, iterations=int(s.iterations),
             final_residual=float(s.final_residual),
-            solver_method="pcg" if precision == abi.SVX_FP64 else "pcg-mixed",
+            solver_method="ldlt" if s.solver_method == abi.SVX_METHOD_LDLT else
+            "pcg" if precision == abi.SVX_FP64 else "pcg-mixed",
             cond_estimate=float(s.cond_estimate), u=self.u, reaction_values=self.react,
             outer_iterations=int(s.outer_iterations), ms_assemble=float(s.ms_assemble),
-            ms_solve=float(s.ms_solve), ms_stress=float(s.ms_stress))
+            ms_solve=float(s.ms_solve), ms_stress=float(s.ms_stress),
+            factor_bandwidth=int(s.factor_bandwidth), ms_factor=float(s.ms_factor))
 
     def solution(self, flat: FlatModel, precision) -> Solution:
         node_ids = flat.node_id if flat.node_id is not None else \
@@ -355,14 +362,14 @@ def default_context(device: int = 0) -> Context:
 
 def solve_with_method(model: Model, method: Method = Method.Auto,
                       ctx: Optional[Context] = None) -> Solution:
-    """Linear-static solve of a reference-shaped model on the GPU.
-
-    ``Method.Auto`` and ``Method.Pcg`` run the FP64 Jacobi-PCG; a budget
-    overrun surfaces as ``NotConverged`` (no direct CPU fallback).
-    """
-    if method == Method.Ldlt:
-        raise InvalidModel("the direct LDLT solver is outside the GPU path (Jacobi-PCG only)")
-    return (ctx or default_context()).solve_model(model)
+    """Linear-static solve of a reference-shaped model on the GPU
+    (lib.rs:586-716): ``Method.Pcg`` runs the FP64 Jacobi-PCG and surfaces a
+    budget overrun as ``NotConverged``; ``Method.Ldlt`` runs the direct path
+    (RCM-ordered band LDLT on the device); ``Method.Auto`` runs the PCG and
+    falls back to the direct path when it does not converge."""
+    code = {Method.Auto: abi.SVX_METHOD_AUTO, Method.Pcg: abi.SVX_METHOD_PCG,
+            Method.Ldlt: abi.SVX_METHOD_LDLT}[method]
+    return (ctx or default_context()).solve_model(model, method=code)
 
 
 def solve(model: Model, ctx: Optional[Context] = None) -> Solution:

@@ -511,21 +511,40 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
     svx_default_opts(&opts);
     if (o) opts = *o;
     long long max_iter = opts.max_iter > 0 ? opts.max_iter : default_max_iter(op->n);
+    if (opts.method < SVX_METHOD_PCG || opts.method > SVX_METHOD_AUTO)
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "unknown solver method"};
     op->u.alloc(ctx->pool, op->n + 1);
-    PcgResult r;
+    PcgResult r{PCG_CONVERGED, 0, 0.0, 0.0};
     long long outer = 0;
-    if (opts.precision == SVX_MIXED)
-        r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol, opts.check_every, op->u.p,
-                      &outer);
-    else
-        r = pcg_fp64(ctx, op, opts.tol, max_iter, opts.check_every, op->u.p);
+    if (opts.method != SVX_METHOD_LDLT) {
+        if (opts.precision == SVX_MIXED)
+            r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol, opts.check_every,
+                          op->u.p, &outer);
+        else
+            r = pcg_fp64(ctx, op, opts.tol, max_iter, opts.check_every, op->u.p);
+    }
+    // lib.rs:664-686: Ldlt factorizes; Auto factorizes when the PCG returns
+    // NotConverged (budget overrun or breakdown).
+    const bool direct = opts.method == SVX_METHOD_LDLT ||
+                        (opts.method == SVX_METHOD_AUTO && r.status != PCG_CONVERGED);
+    LdltOutcome dres;
+    if (direct) {
+        op->has_solution = false;
+        dres = ldlt_direct(ctx, op, op->u.p);
+        r = PcgResult{PCG_CONVERGED, 0, dres.residual, dres.ms};
+        outer = 0;
+    }
     op->has_solution = true;
     if (sol) {
         sol->iterations = r.iterations;
         sol->outer_iterations = outer;
-        sol->fp32_iterations = opts.precision == SVX_MIXED ? op->mixed_sloppy_iters : 0;
+        sol->fp32_iterations =
+            (opts.precision == SVX_MIXED && !direct) ? op->mixed_sloppy_iters : 0;
         sol->final_residual = r.residual;
-        sol->cond_estimate = op->cond_estimate;
+        sol->cond_estimate = direct ? dres.cond : op->cond_estimate;
+        sol->solver_method = direct ? SVX_METHOD_LDLT : SVX_METHOD_PCG;
+        sol->factor_bandwidth = direct ? dres.bandwidth : 0;
+        sol->ms_factor = direct ? dres.ms : 0.0;
         sol->ms_assemble = op->ms_assemble;
         sol->ms_solve = r.ms;
         if (sol->u)
@@ -816,6 +835,7 @@ void svx_default_opts(svx_solve_opts_t* opts) {
     opts->inner_tol = 1e-5;
     opts->check_every = 0;
     opts->want_stress = 1;
+    opts->method = SVX_METHOD_PCG;
 }
 
 int svx_ctx_create(int device, svx_ctx_t** out) {

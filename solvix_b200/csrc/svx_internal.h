@@ -326,6 +326,17 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps);
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y);
+
+// Direct path (svx_ldlt.cu): LDL^T of op->vals in the reverse Cuthill-McKee
+// order, u_dev = K^-1 op->f.  Throws ModelFail with the reference's text on a
+// failed pivot, SVX_OOM when the band does not fit on the device.
+struct LdltOutcome {
+    double residual = 0.0;   // ||f - K u|| / ||f|| (0 when f is zero)
+    double cond = 0.0;       // max|D| / min|D|
+    int64_t bandwidth = 0;   // half-bandwidth of K in the RCM order
+    double ms = 0.0;         // device time: band fill, factorization, solves, residual
+};
+LdltOutcome ldlt_direct(svx_ctx* ctx, svx_op* op, double* u_dev);
 int choose_spmv_group(const svx_op* op);
 // Average device time (ms) of the three FP64 PCG iteration kernels
 // (spmv_dot, update, p_update) over `reps` back-to-back launches each.

@@ -1,7 +1,7 @@
 """Device timing of the PCG iteration kernels on a synthetic workload.
 
     python -m solvix_b200.kernel_timer [--workload c3d8_160|c3d8_480|cps4_200] [--reps N]
-                                       [--solve] [--batch N | --batch-3d N]
+                                       [--solve | --direct] [--batch N | --batch-3d N]
 
 Assembles the workload on cuda:0, then times the three FP64 iteration
 kernels (node-block SpMV + p.Kp, u/r update + dots, p update) with CUDA
@@ -12,7 +12,10 @@ PCG kernel, one launch per chunk of iterations) and prints its device time
 and per-iteration algorithmic bytes.  With ``--batch N`` it runs one
 batched FP64 solve of the first N plates of the 4,096-plate mix, with
 ``--batch-3d N`` of the first N C3D8 cantilevers of the served request
-stream (the cluster kernel's members).  Small and
+stream (the cluster kernel's members).  With ``--direct`` it runs the
+direct path (RCM-ordered band LDL^T on the device) twice and prints the
+second run's device time, half-bandwidth and band arithmetic rate
+(n * bandwidth^2 flops, the leading term of a band LDL^T).  Small and
 self-contained, so it is also the command to profile a single kernel with
 ncu.
 """
@@ -29,6 +32,8 @@ WORKLOADS = {
     "c3d8_480": lambda: workloads.heterogeneous_c3d8(480, 48, 48),
     "c3d8_240": lambda: workloads.heterogeneous_c3d8(240, 24, 24),
     "cps4_200": lambda: workloads.cantilever_cps4(200, 20),
+    "c3d8_40x4x4": lambda: workloads.cantilever_c3d8(40, 4, 4, lx=2.0, ly=0.1, lz=0.1),
+    "c3d8_80x8x8": lambda: workloads.cantilever_c3d8(80, 8, 8, lx=2.0, ly=0.2, lz=0.2),
 }
 
 
@@ -37,6 +42,8 @@ def main(argv=None):
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3d8_160")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--solve", action="store_true", help="one full persistent FP64 solve")
+    ap.add_argument("--direct", action="store_true",
+                    help="the direct path (band LDL^T) instead of the PCG")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead: one batched solve of this many plates of the 4,096-plate mix")
     ap.add_argument("--batch-3d", type=int, default=0,
@@ -79,6 +86,16 @@ def main(argv=None):
                                   "batched_speedup": ms / st["ms_solve"]}))
         return
     flat = WORKLOADS[args.workload]()
+    if args.direct:
+        with Context(0) as ctx:
+            for _ in range(2):
+                sol = ctx.solve_flat(flat, want_stress=False, method=abi.SVX_METHOD_LDLT)
+            n, bw = flat.n_dof, sol.factor_bandwidth
+            print(json.dumps({"workload": args.workload, "n": n, "bandwidth": bw,
+                              "direct_ms": sol.ms_factor, "residual": sol.final_residual,
+                              "cond_estimate": sol.cond_estimate,
+                              "band_gflops": n * bw * bw / (sol.ms_factor * 1e-3) / 1e9}))
+        return
     with Context(0) as ctx:
         op = ctx.assemble(flat)
         n, nnz = op.n, op.nnz

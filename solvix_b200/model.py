@@ -194,6 +194,8 @@ class Solution:
     ms_assemble: float = 0.0
     ms_solve: float = 0.0
     ms_stress: float = 0.0
+    factor_bandwidth: int = 0   # direct path: half-bandwidth of K in the RCM order
+    ms_factor: float = 0.0      # direct path: device time of factorization + solves
 
 
 class SolveError(Exception):
@@ -233,12 +235,9 @@ class DeviceError(SolveError):
 
 
 class Method(enum.Enum):
-    """Linear solver selection (lib.rs:523-534).
-
-    The device path is Jacobi-PCG only: ``Auto`` and ``Pcg`` both run it and
-    surface ``NotConverged``; ``Ldlt`` (the reference's direct CPU fallback)
-    is rejected as outside the path.
-    """
+    """Linear solver selection (lib.rs:523-534): ``Pcg`` (Jacobi-PCG),
+    ``Ldlt`` (the direct path) or ``Auto`` (PCG, then the direct path when
+    the PCG does not converge; the default of ``solve``)."""
 
     Auto = "auto"
     Pcg = "pcg"
