@@ -18,6 +18,10 @@ of 1e-10 and von Mises / reaction recovery.
 * ``cpu_baseline`` - the oracle (the C++ restatement of the reference's
   Rust path) solving the same model on the host cores.
 
+``--form direct`` times the direct path (RCM-ordered band LDL^T on the
+device, the reference's Method::Ldlt) on the mesh of the reference's own
+LDL^T timing test, against the oracle's serial LDL^T.
+
 ``--impl reference`` times only the oracle port on the host cores (rank 0).
 Multi-GPU runs (torchrun) solve independent replicas per GPU ("replicas
 only": the plain solve does not shard); ``value`` sums all ranks.
@@ -52,13 +56,18 @@ def parse_args():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None,
                     help="plain, batched and served forms: fp64 (default) or the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=["plain", "batched", "precision", "served", "thermal"],
+    ap.add_argument("--form",
+                    choices=["plain", "batched", "precision", "served", "thermal", "direct"],
                     default="plain",
                     help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
                          "2D plates in one launch; precision: FP64 vs mixed on the "
                          "480x48x48 heterogeneous C3D8 model; served: Poisson request "
                          "stream through the continuous-batching server; thermal: steady "
-                         "conduction in a 480x48x48 C3D8 block")
+                         "conduction in a 480x48x48 C3D8 block; direct: the band LDL^T "
+                         "direct path")
+    ap.add_argument("--direct-workload", choices=["hex40", "c2"], default="hex40",
+                    help="direct form: the 40x4x4 hex cantilever of the reference's LDL^T "
+                         "test (default) or the 160x16x16 C3D8 cantilever")
     ap.add_argument("--requests", type=int, default=20000,
                     help="served form: requests per rate point")
     ap.add_argument("--rates", type=str, default="",
@@ -186,6 +195,8 @@ def run_reference(args, rank):
     """--impl reference: the oracle port on the host cores, rank 0 only."""
     if rank != 0:
         return None
+    if args.form == "direct":
+        return run_reference_direct(args)
     flat = workload()
     from oracle import oracle
     oracle.build()
@@ -893,6 +904,144 @@ def run_thermal(args, rank, world, local_rank):
     return line
 
 
+DIRECT_NAMES = {
+    "hex40": ("C3D8 hex cantilever 40x4x4 over 2.0x0.1x0.1 m (the mesh of the reference's LDLT "
+              "timing test, ldl.rs:361-434; 1,025 nodes, 3,075 DOF), E=210e9, nu=0.3, tip-face "
+              "load; direct path (Method::Ldlt)"),
+    "c2": ("C3D8 cantilever 160x16x16 over 2.0x0.2x0.2 m (139,587 DOF, 10,393,929 nnz), "
+           "seeded jitter; direct path (Method::Ldlt)"),
+}
+
+
+def direct_workload(which):
+    from solvix_b200 import workloads
+    if which == "c2":
+        return workload()
+    return workloads.cantilever_c3d8(40, 4, 4, lx=2.0, ly=0.1, lz=0.1, jitter=0.0, E=210e9,
+                                     nu=0.3)
+
+
+def direct_cpu(flat, min_seconds=2.0, max_solves=20):
+    """The oracle's full direct solve (assembly, RCM, up-looking LDL^T,
+    solve, residual, stress) repeated until min_seconds or max_solves
+    (exactly max_solves when min_seconds <= 0)."""
+    from oracle import oracle
+    oracle.build()
+    threads = oracle.default_threads()
+    times = []
+    while len(times) < max_solves and (min_seconds <= 0 or sum(times) < min_seconds):
+        t0 = time.perf_counter()
+        ref = oracle.solve_flat(flat, threads=threads, method="ldlt")
+        times.append(time.perf_counter() - t0)
+    return len(times) / sum(times), times, threads, ref
+
+
+def run_reference_direct(args):
+    flat = direct_workload(args.direct_workload)
+    for _ in range(max(0, args.warmup)):
+        direct_cpu(flat, min_seconds=0.0, max_solves=1)
+    value, times, threads, _ = direct_cpu(flat, min_seconds=0.0, max_solves=args.steps)
+    sample = (f"{len(times)} full oracle direct solves (assembly on {threads} threads, serial "
+              f"RCM + up-looking LDLT as in ldl.rs) of the same model")
+    return {
+        "impl": "reference", "metric": "direct solves/s (Method::Ldlt)", "form": "direct",
+        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (structured mesh; no public dataset exists for this path)",
+        "config": {"workload": DIRECT_NAMES[args.direct_workload], "parallelism": "host"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def run_direct(args, rank, world, local_rank):
+    """The direct path on one GPU.  value: svx_op_solve with SVX_METHOD_LDLT
+    on the assembled operator (host RCM ordering, band fill, factorization,
+    solves, residual), CUDA events on the library's stream around the steps;
+    e2e: svx_solve_flat with the same method from host arrays (upload,
+    assembly, direct solve, stress, download), wall clock."""
+    import torch
+
+    from solvix_b200 import Context, abi
+
+    torch.cuda.set_device(local_rank)
+    flat = direct_workload(args.direct_workload)
+    ctx = Context(local_rank)
+    lib = ctx.lib
+    op = ctx.assemble(flat)
+    for _ in range(max(args.warmup, 0)):
+        op.solve(method=abi.SVX_METHOD_LDLT)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = lib.svx_launch_count()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        _u, _it, res, cond = op.solve(method=abi.SVX_METHOD_LDLT)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.svx_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    # the factorization's own device time and bandwidth, from one more solve
+    sol = ctx.solve_flat(flat, method=abi.SVX_METHOD_LDLT, want_stress=False)
+    for _ in range(max(args.warmup, 0)):
+        ctx.solve_flat(flat, method=abi.SVX_METHOD_LDLT)
+    walls = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.solve_flat(flat, method=abi.SVX_METHOD_LDLT)
+        walls.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    op.free()
+    ctx.close()
+    n, bw = flat.n_dof, sol.factor_bandwidth
+    value = args.steps / (ms * 1e-3)
+    flops = float(n) * bw * bw
+    line = {
+        "metric": "direct solves/s (Method::Ldlt)", "form": "direct", "value": value,
+        "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (structured mesh; no public dataset exists for this path)",
+        "config": {"workload": DIRECT_NAMES[args.direct_workload], "n_dof": n,
+                   "half_bandwidth_rcm": bw,
+                   "band_bytes": 8 * 1024 * ((n + 31) // 32) * ((bw + 31) // 32 + 1),
+                   "l2": "band resident in L2 when under 126 MB (hex40: 0.8 MB)"},
+        "residual": res, "cond_estimate": cond,
+        "e2e": {"value": args.steps / sum(walls), "unit": "solves/s",
+                "note": "svx_solve_flat (method LDLT, stress on) from host arrays, wall clock",
+                "h2d_bytes_per_step": int(flat.xyz.nbytes + flat.conn.nbytes +
+                                          flat.conn_ptr.nbytes + flat.kind.nbytes +
+                                          flat.youngs.nbytes + flat.poisson.nbytes +
+                                          flat.fixed_row.nbytes + flat.f.nbytes),
+                "d2h_bytes_per_step": int(8 * (2 * n + 3 * flat.n_nodes + flat.n_elem +
+                                               flat.n_nodes + flat.fixed_row.shape[0]))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "fp64", "kernel": "ldlt_update_kernel + ldlt_panel_kernel "
+                     "(whole direct solve)", "achieved": flops / (sol.ms_factor * 1e-3) / 1e12,
+                     "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                     "device_ms": sol.ms_factor,
+                     "note": "n * bandwidth^2 flops (the band LDLT's leading term) over the "
+                             "device time from band fill to residual; no measured FP64 peak "
+                             "exists for this pool, so no fraction is given"},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        cps, times, threads, _ = direct_cpu(flat)
+        line["cpu_baseline"] = {
+            "value": cps, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} full oracle direct solves of the same model "
+                      f"(assembly on {threads} threads, serial up-looking LDLT) in "
+                      f"{sum(times):.2f} s"}
+    return line
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -918,6 +1067,8 @@ def main():
             line = run_precision(args, rank, world, local_rank) if rank == 0 else None
         elif args.form == "thermal":
             line = run_thermal(args, rank, world, local_rank) if rank == 0 else None
+        elif args.form == "direct":
+            line = run_direct(args, rank, world, local_rank) if rank == 0 else None
         else:
             line = run_ours(args, rank, world, local_rank)
     finally:

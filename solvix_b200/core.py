@@ -325,12 +325,13 @@ class Operator:
             float(sol.ms_stress), float(sol.ms_assemble)
 
     def solve(self, tol=1e-10, max_iter=0, precision=abi.SVX_FP64, inner_tol=1e-5,
-              check_every=0):
+              check_every=0, method=abi.SVX_METHOD_PCG):
         u = np.zeros(self.n)
         sol = abi.SvxSolution()
         sol.u = abi.ptr(u, C.c_double)
         opts = abi.default_opts(tol=tol, max_iter=max_iter, precision=precision,
-                                inner_tol=inner_tol, check_every=check_every, want_stress=0)
+                                inner_tol=inner_tol, check_every=check_every, want_stress=0,
+                                method=int(method))
         err = abi.SvxError()
         st = self.lib.svx_op_solve(self.handle, C.byref(opts), C.byref(sol), C.byref(err))
         if st != abi.SVX_OK:

@@ -59,3 +59,24 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_of_the_direct_form():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--form", "direct", "--steps", "2", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["form"] == "direct" and d["unit"] == "solves/s"
+    assert d["value"] > 0 and d["steps"] == 2 and d["warmup"] == 1
+    assert d["config"]["workload"] == bench.DIRECT_NAMES["hex40"]
+    assert d["cpu_baseline"]["value"] == d["value"]
+
+
+def test_direct_workload_is_the_reference_test_mesh():
+    flat = bench.direct_workload("hex40")
+    assert (flat.n_nodes, flat.n_elem, flat.n_dof) == (1025, 640, 3075)
+    assert float(flat.youngs[0]) == 210e9 and float(flat.poisson[0]) == 0.3
