@@ -9,9 +9,10 @@
 // one block column per step:
 //
 //   panel kernel   every block factors the diagonal tile (J, J) into L_JJ and
-//                  D_J in shared memory; block 0 stores them apart from the
-//                  band (the other blocks are still reading tile (J, J));
-//                  block g solves the panel tile (J+1+g, J): W = A L_JJ^-T,
+//                  D_J (one warp, rows in registers, columns exchanged by
+//                  shuffles); block 0 stores them apart from the band (the
+//                  other blocks are still reading tile (J, J)); block g
+//                  solves the panel tile (J+1+g, J): W = A L_JJ^-T,
 //                  L = W D_J^-1;
 //   update kernel  one block per tile pair J < K <= I <= J + w:
 //                  A_IK -= W_IJ L_KJ^T (W keeps the product L D).
@@ -127,27 +128,33 @@ ldlt_panel_kernel(int64_t J, int64_t n, int w, int wj, double* __restrict__ band
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     if (warp == 0) {
-        // Right-looking LDL^T of the tile: lane r owns row r.  Column c's
-        // entries below the diagonal hold W = L D until every lane has used
-        // them for its trailing update, then become L.
+        // Right-looking LDL^T of the tile in registers: lane r holds row r.
+        // At column c every lane takes W[k][c] (k > c) from lane k by a
+        // shuffle before any lane replaces its own W[r][c] by L[r][c], so
+        // each entry gets A[r][k] - sum_c L[r][c] W[k][c] in column order.
         const int r = lane;
+        double a[LT];
+#pragma unroll
+        for (int k = 0; k < LT; ++k) a[k] = s_l[r][k];
+#pragma unroll
         for (int c = 0; c < LT; ++c) {
-            const double dc = s_l[c][c];
+            const double dc = __shfl_sync(0xffffffffu, a[c], c);
             const int64_t eq = J * LT + c;
             if (r == 0 && blockIdx.x == 0 && eq < n) {
                 const double lim = 1e-13 * fmax(row_max[eq], DBL_MIN);
                 if (!isfinite(dc) || dc <= lim)
                     atomicMin(fail, (unsigned long long)(eq) << 1 | (dc < 0.0 ? 1ull : 0ull));
             }
-            double l = 0.0;
-            if (r > c) {
-                l = s_l[r][c] / dc;
-                for (int k = c + 1; k <= r; ++k) s_l[r][k] -= l * s_l[k][c];
+            const double l = r > c ? a[c] / dc : 0.0;
+#pragma unroll
+            for (int k = c + 1; k < LT; ++k) {
+                const double wkc = __shfl_sync(0xffffffffu, a[c], k);
+                if (r >= k) a[k] -= l * wkc;
             }
-            __syncwarp();
-            if (r > c) s_l[r][c] = l;
-            __syncwarp();
+            if (r > c) a[c] = l;
         }
+#pragma unroll
+        for (int k = 0; k < LT; ++k) s_l[r][k] = a[k];
     }
     __syncthreads();
     if (blockIdx.x == 0) {
@@ -157,18 +164,32 @@ ldlt_panel_kernel(int64_t J, int64_t n, int w, int wj, double* __restrict__ band
     }
     const int d = 1 + int(blockIdx.x);
     if (d > wj) return;
-    // Panel tile (J + d, J): warp w takes rows w, w + 8, ...; lane c' ends
-    // with W[row][c'] = A[row][c'] - sum_{c < c'} W[row][c] L_JJ[c'][c].
+    // Panel tile (J + d, J): warp w takes rows w, w + 8, w + 16, w + 24
+    // together; lane c' keeps row c' of L_JJ in registers and ends with
+    // W[row][c'] = A[row][c'] - sum_{c < c'} W[row][c] L_JJ[c'][c].
+    static_assert(LT == 4 * (LBLOCK / 32), "four panel rows per warp");
+    double lrow[LT];
+#pragma unroll
+    for (int k = 0; k < LT; ++k) lrow[k] = s_l[lane][k];
+    const double dl = s_l[lane][lane];
     double* tile = band + tile_off(J + d, d, w);
     double* wt = panel + size_t(d - 1) * LT2;
-    for (int row = warp; row < LT; row += LBLOCK / 32) {
-        double x = tile[row * LT + lane];
-        for (int c = 0; c < LT; ++c) {
-            const double v = __shfl_sync(0xffffffffu, x, c);
-            if (lane > c) x -= v * s_l[lane][c];
+    double x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = tile[(warp + 8 * q) * LT + lane];
+#pragma unroll
+    for (int c = 0; c < LT; ++c) {
+        const double lc = lrow[c];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double v = __shfl_sync(0xffffffffu, x[q], c);
+            if (lane > c) x[q] -= v * lc;
         }
-        wt[row * LT + lane] = x;
-        tile[row * LT + lane] = x / s_l[lane][lane];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        wt[(warp + 8 * q) * LT + lane] = x[q];
+        tile[(warp + 8 * q) * LT + lane] = x[q] / dl;
     }
 }
 
