@@ -556,8 +556,8 @@ void rs_quicksort(Trip* v, int64_t len, const Trip* ancestor, uint32_t limit) {
         --limit;
         int64_t pivot_pos = rs_choose_pivot(v, len);
         if (ancestor && !trip_less(*ancestor, v[pivot_pos])) {
-            int64_t num_lt = rs_partition(v, len, pivot_pos,
-                                          [](const Trip& a, const Trip& b) { return !trip_less(b, a); });
+            int64_t num_lt = rs_partition(
+                v, len, pivot_pos, [](const Trip& a, const Trip& b) { return !trip_less(b, a); });
             v += num_lt + 1;
             len -= num_lt + 1;
             ancestor = nullptr;

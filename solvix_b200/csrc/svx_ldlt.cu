@@ -232,12 +232,13 @@ ldlt_update_kernel(int64_t J, int w, int wj, double* __restrict__ band,
 }
 
 // L y = P f, y /= D, L^T x = y, u = P^T x in one block (y: nb * LT
-// scratch; the diagonal tiles' L in dfac).  Warp p sums the off-diagonal tiles d = p + 1, p + 33, ... of a
-// block row; warp 0 adds the partials in a fixed order and solves the
-// diagonal tile with shuffles.
+// scratch; the diagonal tiles' L in dfac).  Warp p sums the off-diagonal
+// tiles d = p + 1, p + 33, ... of a block row; warp 0 adds the partials in
+// a fixed order and solves the diagonal tile with shuffles.
 __global__ void __launch_bounds__(SBLOCK)
 ldlt_solve_kernel(int64_t n, int64_t nb, int w, const double* __restrict__ band,
-                  const double* __restrict__ dfac, const double* __restrict__ dvec, const int32_t* __restrict__ perm,
+                  const double* __restrict__ dfac, const double* __restrict__ dvec,
+                  const int32_t* __restrict__ perm,
                   const double* __restrict__ f, double* y, double* __restrict__ u,
                   const unsigned long long* fail) {
     __shared__ double s_part[SBLOCK / 32][LT + 1];

@@ -25,7 +25,8 @@ void rcm_order_impl(int64_t n, const P* row_ptr, const int32_t* col_idx,
     bandwidth = 0;
     if (n <= 0) return;
     int64_t max_deg = 0;
-    for (int64_t i = 0; i < n; ++i) max_deg = std::max<int64_t>(max_deg, row_ptr[i + 1] - row_ptr[i]);
+    for (int64_t i = 0; i < n; ++i)
+        max_deg = std::max<int64_t>(max_deg, row_ptr[i + 1] - row_ptr[i]);
     std::vector<int64_t> start(size_t(max_deg) + 2, 0);
     for (int64_t i = 0; i < n; ++i) ++start[size_t(row_ptr[i + 1] - row_ptr[i]) + 1];
     for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
