@@ -67,6 +67,10 @@ _SIG = {
                                           C.c_int64, C.c_int, C.POINTER(abi.SvxSolution),
                                           C.POINTER(C.c_int), C.POINTER(abi.SvxError)]),
     "svx_oracle_rcm": (None, [C.POINTER(OracleCsr), abi.c_int64_p]),
+    "svx_oracle_element_mass": (C.c_int, [C.c_int, abi.c_double_p, C.c_double, C.c_double,
+                                          abi.c_double_p]),
+    "svx_oracle_assemble_mass": (C.c_int, [C.POINTER(abi.SvxFlatModel), C.c_double,
+                                           C.POINTER(OracleCsr), C.POINTER(abi.SvxError)]),
     "svx_oracle_ldlt": (C.c_int, [C.POINTER(OracleCsr), abi.c_double_p, C.c_int, abi.c_double_p,
                                   abi.c_double_p, abi.c_double_p, abi.c_double_p, abi.c_int64_p,
                                   C.POINTER(abi.SvxError)]),
@@ -324,6 +328,31 @@ def pcg(k: Csr, f, tol=1e-10, max_iter=1000, threads: int | None = None):
                               threads or default_threads(), abi.ptr(u, C.c_double),
                               C.byref(it), C.byref(res))
     return st, u, int(it.value), float(res.value)
+
+
+def element_mass(kind: int, coords, rho: float, t: float = 1.0):
+    """Consistent mass of one element (modal.rs:82-146); returns (reason, me)."""
+    coords = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1, 3))
+    N = {0: 6, 1: 8, 3: 8, 5: 24}[int(kind)]
+    me = np.zeros((N, N))
+    r = lib().svx_oracle_element_mass(int(kind), abi.ptr(coords, C.c_double), float(rho),
+                                      float(t), abi.ptr(me, C.c_double))
+    return r, me
+
+
+def assemble_mass(flat: FlatModel, rho: float) -> Csr:
+    """assemble_mass (modal.rs:203-271) on a flat model; raises
+    InvalidModel with the reference's text for a failing element."""
+    s = flat.as_struct()
+    out = OracleCsr()
+    err = abi.SvxError()
+    st = lib().svx_oracle_assemble_mass(C.byref(s), float(rho), C.byref(out), C.byref(err))
+    if st != abi.SVX_OK:
+        _raise_err(err)
+    try:
+        return Csr(out)
+    finally:
+        lib().svx_oracle_csr_free(C.byref(out))
 
 
 def rcm(k: Csr):

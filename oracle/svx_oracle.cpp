@@ -1255,6 +1255,123 @@ double ldlt_cond(const Ldlt& fa) {
 
 }  // namespace
 
+namespace {
+
+// ------------------------------------------------------------ consistent mass
+// modal.rs:82-99 (CPS3, closed form rho t A / 12 x [2 1 1; 1 2 1; 1 1 2]),
+// :103-121 (CPS4 / CPE4, 2x2 Gauss, xi outer), :125-146 (C3D8, 2x2x2 Gauss):
+// rho [t] detJ N_i N_j on every dof pair (d, d) of nodes i, j, into me
+// (row-major N x N, zeros elsewhere).  Returns 0 or the svx_elem_reason:
+// zero area, or det J <= 0 at a Gauss point (the stiffness's triggers, but
+// no centroid check).
+int element_me(int kind, const double* coords, double rho, double t, double* me) {
+    const double g = 1.0 / std::sqrt(3.0);
+    const double pts[2] = {-g, g};
+    if (kind == SVX_CPS3) {
+        const double two_a = (coords[3] - coords[0]) * (coords[7] - coords[1]) -
+                             (coords[6] - coords[0]) * (coords[4] - coords[1]);
+        if (two_a == 0.0) return SVX_REASON_DEGENERATE_TRI;
+        const double w = rho * t * std::fabs(two_a) / 24.0;
+        std::memset(me, 0, sizeof(double) * 36);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int d = 0; d < 2; ++d)
+                    me[(2 * i + d) * 6 + 2 * j + d] = w * (i == j ? 2.0 : 1.0);
+        return 0;
+    }
+    if (kind == SVX_CPS4 || kind == SVX_CPE4) {
+        double xy[4][2];
+        for (int i = 0; i < 4; ++i) {
+            xy[i][0] = coords[3 * i];
+            xy[i][1] = coords[3 * i + 1];
+        }
+        std::memset(me, 0, sizeof(double) * 64);
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b) {
+                double bm[3][8], detj, nsh[4];
+                if (!quad_b(xy, pts[a], pts[b], bm, &detj)) return SVX_REASON_BAD_JACOBIAN;
+                quad_shapes(pts[a], pts[b], nsh);
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j) {
+                        const double v = rho * t * detj * nsh[i] * nsh[j];
+                        for (int d = 0; d < 2; ++d) me[(2 * i + d) * 8 + 2 * j + d] += v;
+                    }
+            }
+        return 0;
+    }
+    if (kind == SVX_C3D8) {
+        double xyz[8][3];
+        for (int i = 0; i < 8; ++i)
+            for (int k = 0; k < 3; ++k) xyz[i][k] = coords[3 * i + k];
+        std::memset(me, 0, sizeof(double) * 576);
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 2; ++c) {
+                    double bm[6][24], detj, nsh[8];
+                    if (!hex_b(xyz, pts[a], pts[b], pts[c], bm, &detj))
+                        return SVX_REASON_BAD_JACOBIAN;
+                    hex_shapes(pts[a], pts[b], pts[c], nsh);
+                    for (int i = 0; i < 8; ++i)
+                        for (int j = 0; j < 8; ++j) {
+                            const double v = rho * detj * nsh[i] * nsh[j];
+                            for (int d = 0; d < 3; ++d) me[(3 * i + d) * 24 + 3 * j + d] += v;
+                        }
+                }
+        return 0;
+    }
+    return SVX_REASON_UNSUPPORTED_KIND;
+}
+
+}  // namespace
+
+int svx_oracle_element_mass(int kind, const double* coords, double rho, double t,
+                            double* me) {
+    return element_me(kind, coords, rho, t, me);
+}
+
+// assemble_mass (modal.rs:203-271): n zero diagonal seeds, then every
+// element's N x N consistent mass in enumeration order, summed by
+// csr_from_triplets; the first failing element raises "element {id}: ...".
+int svx_oracle_assemble_mass(const svx_flat_model_t* m, double rho, svx_oracle_csr_t* out,
+                             svx_error_t* err) {
+    std::memset(out, 0, sizeof(*out));
+    const int ndof = m->ndof;
+    const int64_t n = m->n_nodes * ndof;
+    std::vector<int64_t> tr, tc;
+    std::vector<double> tv;
+    for (int64_t i = 0; i < n; ++i) {
+        tr.push_back(i);
+        tc.push_back(i);
+        tv.push_back(0.0);
+    }
+    double me[576], coords[24];
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        const int kind = m->kind[e];
+        const int nn = int(m->conn_ptr[e + 1] - m->conn_ptr[e]);
+        const int32_t* cn = m->conn + m->conn_ptr[e];
+        for (int i = 0; i < nn && i < 8; ++i)
+            for (int k = 0; k < 3; ++k) coords[3 * i + k] = m->xyz[3 * int64_t(cn[i]) + k];
+        const int r = element_me(kind, coords, rho, m->thickness, me);
+        if (r) {
+            char msg[400];
+            std::snprintf(msg, sizeof msg, "element %u: %s", elem_id_of(m, e), reason_text(r));
+            set_error(err, SVX_INVALID_MODEL, r, e, msg);
+            return SVX_INVALID_MODEL;
+        }
+        const int N = nn * ndof;
+        for (int a = 0; a < N; ++a)
+            for (int c = 0; c < N; ++c) {
+                tr.push_back(int64_t(cn[a / ndof]) * ndof + a % ndof);
+                tc.push_back(int64_t(cn[c / ndof]) * ndof + c % ndof);
+                tv.push_back(me[a * N + c]);
+            }
+    }
+    csr_from_triplets(n, tr, tc, tv, out);
+    for (int64_t i = 0; i < n; ++i) out->f[i] = 0.0;
+    if (err) set_error(err, SVX_OK, 0, -1, "");
+    return SVX_OK;
+}
+
 void svx_oracle_rcm(const svx_oracle_csr_t* k, int64_t* perm) {
     std::vector<int64_t> p = rcm_perm(*k);
     std::copy(p.begin(), p.end(), perm);

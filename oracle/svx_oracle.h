@@ -76,6 +76,17 @@ int svx_oracle_solve_method(const svx_flat_model_t* m, int threads, double tol,
                             int64_t max_iter, int method, svx_solution_t* sol,
                             int* method_used, svx_error_t* err);
 
+/* Consistent mass of one element (modal.rs:82-146: CPS3 closed form, CPS4 /
+ * CPE4 2x2 and C3D8 2x2x2 Gauss of rho [t] detJ N^T N), row-major N x N into
+ * me; returns 0 or the svx_elem_reason of the failure. */
+int svx_oracle_element_mass(int kind, const double* coords, double rho, double t, double* me);
+
+/* assemble_mass (modal.rs:203-271): the consistent mass matrix on the
+ * stiffness's pattern (diagonal seeds, then elements in order, summed in the
+ * current sort mode); density rho is model-wide, thickness the model's. */
+int svx_oracle_assemble_mass(const svx_flat_model_t* m, double rho, svx_oracle_csr_t* out,
+                             svx_error_t* err);
+
 /* Reverse Cuthill-McKee permutation of k's pattern, old -> new
  * (ldl.rs:27-60). */
 void svx_oracle_rcm(const svx_oracle_csr_t* k, int64_t* perm);
