@@ -359,3 +359,34 @@ def test_example_decks_through_the_direct_path(name):
     assert sol.solver_method == "ldlt" and sol.final_residual <= 1e-8
     assert fmt_mm(max_disp(sol.displacements)) == g["max_disp_mm"]
     assert fmt_mpa(max(0.0, sol.von_mises.max())) == g["max_von_mises_mpa"]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_ldlt_agrees_with_a_dense_factorization_in_the_same_order(seed):
+    """Random sparse SPD systems: the oracle's u solves the system like a
+    dense solve, and its D is the squared diagonal of the dense Cholesky
+    factor of the RCM-permuted matrix (so the condition estimate is the
+    same), independently of the reference's own tests."""
+    import scipy.sparse as sp
+    rng = np.random.Generator(np.random.PCG64(100 + seed))
+    n = int(rng.integers(20, 120))
+    a = sp.random(n, n, density=min(1.0, 6.0 / n), random_state=int(rng.integers(1 << 30)))
+    a = a + a.T
+    a = a + sp.diags(np.abs(a).sum(axis=1).A1 + rng.uniform(0.5, 2.0, n))
+    a = sp.csr_matrix(a)
+    a.sort_indices()
+    k = csr_from_rows([[(int(c), float(v)) for c, v in
+                        zip(a.indices[a.indptr[r]:a.indptr[r + 1]],
+                            a.data[a.indptr[r]:a.indptr[r + 1]])] for r in range(n)])
+    b = rng.normal(size=n)
+    r = oracle.ldlt(k, b, threads=1)
+    dense = a.toarray()
+    want = np.linalg.solve(dense, b)
+    assert np.linalg.norm(r.u - want) <= 1e-12 * np.linalg.norm(want)
+    perm = oracle.rcm(k)
+    invp = np.empty_like(perm)
+    invp[perm] = np.arange(n)
+    chol = np.linalg.cholesky(dense[np.ix_(invp, invp)])
+    d_dense = np.diag(chol) ** 2
+    assert np.allclose(r.d, d_dense, rtol=1e-12, atol=0.0)
+    assert abs(r.cond - d_dense.max() / d_dense.min()) <= 1e-12 * r.cond
