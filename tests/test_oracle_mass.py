@@ -99,3 +99,51 @@ def test_assembly_error_text():
     flat, _ = oracle.resolve(m)
     with pytest.raises(InvalidModel, match=r"^element 9: degenerate \(zero-area\) triangle$"):
         oracle.assemble_mass(flat, RHO)
+
+
+def _quad_n(xi, eta):
+    s = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], dtype=float)
+    n = 0.25 * (1 + xi * s[:, 0]) * (1 + eta * s[:, 1])
+    dn = 0.25 * np.stack([s[:, 0] * (1 + eta * s[:, 1]), s[:, 1] * (1 + xi * s[:, 0])])
+    return n, dn
+
+
+def _hex_n(xi, eta, zeta):
+    s = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                  [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=float)
+    a, b, c = 1 + xi * s[:, 0], 1 + eta * s[:, 1], 1 + zeta * s[:, 2]
+    n = 0.125 * a * b * c
+    dn = 0.125 * np.stack([s[:, 0] * b * c, s[:, 1] * a * c, s[:, 2] * a * b])
+    return n, dn
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_element_mass_matches_an_independent_gauss_integration(seed):
+    """rho [t] sum_gp detJ N^T N on randomly distorted elements, computed
+    here with numpy, against the oracle's element mass."""
+    rng = np.random.Generator(np.random.PCG64(40 + seed))
+    g = 1.0 / np.sqrt(3.0)
+    quad = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], float) + rng.uniform(-0.2, 0.2, (4, 2))
+    want = np.zeros((8, 8))
+    for xi in (-g, g):
+        for eta in (-g, g):
+            n, dn = _quad_n(xi, eta)
+            detj = np.linalg.det(dn @ quad)
+            block = RHO * T * detj * np.outer(n, n)
+            want[0::2, 0::2] += block
+            want[1::2, 1::2] += block
+    _, got = oracle.element_mass(ElemKind.Cps4, np.c_[quad, np.zeros(4)], RHO, T)
+    assert np.allclose(got, want, rtol=1e-13, atol=1e-13 * np.abs(want).max())
+    hexc = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1],
+                     [1, 1, 1], [0, 1, 1]], float) + rng.uniform(-0.15, 0.15, (8, 3))
+    want = np.zeros((24, 24))
+    for xi in (-g, g):
+        for eta in (-g, g):
+            for zeta in (-g, g):
+                n, dn = _hex_n(xi, eta, zeta)
+                detj = np.linalg.det(dn @ hexc)
+                block = RHO * detj * np.outer(n, n)
+                for d in range(3):
+                    want[d::3, d::3] += block
+    _, got = oracle.element_mass(ElemKind.C3d8, hexc, RHO, 1.0)
+    assert np.allclose(got, want, rtol=1e-13, atol=1e-13 * np.abs(want).max())
