@@ -602,7 +602,35 @@ def run_precision(args, rank, world, local_rank):
     }
     op.free()
     ctx.close()
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = precision_cpu_baseline(f64["iterations"], n)
     return line
+
+
+def precision_cpu_baseline(gpu_fp64_iterations, n_c3, iterations=200):
+    """The CPU leg of the precision form: a full oracle solve of C3 takes
+    hours (and its triplet assembly about 20 GB of host memory), so this
+    times `iterations` oracle PCG iterations on the 160x16x16 model of the
+    same kind (heterogeneous C3D8, seed 3) for the CPU's DOF.iter/s, and
+    projects C3's CPU solves/s from the GPU's FP64 iteration count."""
+    from oracle import oracle
+    from solvix_b200 import workloads
+    flat = workloads.heterogeneous_c3d8(160, 16, 16, seed=3)
+    threads = oracle.default_threads()
+    k = oracle.assemble(flat, threads)
+    f = flat.f.copy()
+    oracle.apply_dirichlet(k, f, flat.fixed_row)
+    t0 = time.perf_counter()
+    _st, _u, it, _res = oracle.pcg(k, f, tol=1e-300, max_iter=iterations, threads=threads)
+    dt = time.perf_counter() - t0
+    rate = flat.n_dof * it / dt
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"{it} oracle PCG iterations on the 160x16x16 heterogeneous C3D8 model "
+                       f"({flat.n_dof} DOF, {k.nnz} nnz) on {threads} threads in {dt:.2f} s; "
+                       "C3 itself is not solved on the CPU"),
+            "projected_c3_solves_per_s": (rate / (n_c3 * gpu_fp64_iterations)
+                                          if gpu_fp64_iterations else None),
+            "projected": True}
 
 
 SERVED_NAME = ("Poisson stream of solve requests: 70% 2D plates of the batched mix, 30% "

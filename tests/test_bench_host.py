@@ -80,3 +80,13 @@ def test_direct_workload_is_the_reference_test_mesh():
     flat = bench.direct_workload("hex40")
     assert (flat.n_nodes, flat.n_elem, flat.n_dof) == (1025, 640, 3075)
     assert float(flat.youngs[0]) == 210e9 and float(flat.poisson[0]) == 0.3
+
+
+def test_precision_cpu_sample_is_bounded_and_labelled():
+    import time
+    t0 = time.perf_counter()
+    cb = bench.precision_cpu_baseline(7688, 3464643, iterations=20)
+    assert time.perf_counter() - t0 < 120
+    assert cb["kind"] == "port" and cb["unit"] == bench.UNIT and cb["value"] > 0
+    assert cb["projected"] is True and cb["projected_c3_solves_per_s"] > 0
+    assert "not solved on the CPU" in cb["sample"]
