@@ -412,6 +412,29 @@ BATCH_NAME = ("4,096 independent 2D plates (nx~U{10..160}, ny~U{4..40}, h=1, CPS
               "Jacobi-PCG to 1e-10 per model, centroid von Mises")
 
 
+def mix_cpu_baseline(flats, what, max_seconds=20.0):
+    """The oracle's full solves of the sampled models of a mix, one after
+    another on min(8, cores) threads, stopping after max_seconds; the mix's
+    CPU rate is extrapolated from the models solved."""
+    from oracle import oracle
+    oracle.build()
+    threads = oracle.default_threads()
+    dof_it, done, t_all = 0.0, 0, 0.0
+    for f in flats:
+        t0 = time.perf_counter()
+        ref = oracle.solve_flat(f, threads=threads)
+        t_all += time.perf_counter() - t0
+        dof_it += f.n_dof * ref.iterations
+        done += 1
+        if t_all >= max_seconds:
+            break
+    return {"value": dof_it / t_all, "unit": UNIT, "cores": threads, "kind": "port",
+            "solves_per_s": done / t_all, "extrapolated": True,
+            "sample": (f"oracle full solves (assembly, PCG, stress) of {done} of the {what}, "
+                       f"one after another on {threads} threads in {t_all:.2f} s; the mix's "
+                       "CPU rate is extrapolated from them")}
+
+
 def one_at_a_time(ctx, flats):
     """The one-at-a-time plain FP64 GPU path on a sample: every model through
     svx_solve_flat, one after another, wall clock.  Two passes over the
@@ -533,6 +556,9 @@ def run_batched(args, rank, world, local_rank):
                       "(wall clock, faster of two passes), projected to the set",
             "speedup_device": line["solves_per_s"] * per,
             "speedup_e2e": line["e2e"]["solves_per_s"] * per}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = mix_cpu_baseline(
+                [flats[int(k)] for k in idx], "64 sampled models of the plate mix")
     ctx.close()
     return line
 
@@ -765,6 +791,9 @@ def run_served(args, rank, world, local_rank):
         errs.append(float(np.linalg.norm(served_u[k] - ref.u) / np.linalg.norm(ref.u)))
     one_per, one_dev_ms = one_at_a_time(ctx, [reqs[k] for k in idx])
     ctx.close()
+    cpu_leg = (mix_cpu_baseline([reqs[k] for k in idx],
+                                f"{len(idx)} sampled requests of the served mix")
+               if rank == 0 and not args.no_cpu_baseline else None)
     rows = [sat] + sweep
     if world > 1:
         gathered = [None] * world
@@ -821,6 +850,8 @@ def run_served(args, rank, world, local_rank):
                      "traffic": None},
         "clocks": clk,
     }
+    if cpu_leg is not None:
+        line["cpu_baseline"] = cpu_leg
     return line
 
 

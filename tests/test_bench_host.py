@@ -90,3 +90,14 @@ def test_precision_cpu_sample_is_bounded_and_labelled():
     assert cb["kind"] == "port" and cb["unit"] == bench.UNIT and cb["value"] > 0
     assert cb["projected"] is True and cb["projected_c3_solves_per_s"] > 0
     assert "not solved on the CPU" in cb["sample"]
+
+
+def test_mix_cpu_sample_is_bounded_and_labelled():
+    import numpy as np
+    from solvix_b200 import workloads
+    rng = np.random.Generator(np.random.PCG64(4))
+    flats = [workloads.plate(rng) for _ in range(6)]
+    cb = bench.mix_cpu_baseline(flats, "6 plates", max_seconds=5.0)
+    assert cb["kind"] == "port" and cb["unit"] == bench.UNIT and cb["value"] > 0
+    assert cb["extrapolated"] is True and cb["solves_per_s"] > 0
+    assert "extrapolated" in cb["sample"]
