@@ -244,6 +244,10 @@ int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len);
 int svx_resolve(const svx_model_desc_t* desc, svx_resolved_t** out, svx_error_t* err);
 /* Borrowed view of the resolved flat model (valid until svx_resolved_free). */
 const svx_flat_model_t* svx_resolved_flat(const svx_resolved_t* res);
+/* The CLOAD / BC error the reference raises after the element loop, if
+ * any (SVX_OK when none): callers that solve the flat view themselves
+ * (svx_serve_submit) report it when no element fails first. */
+int svx_resolved_pending(const svx_resolved_t* res, svx_error_t* err);
 int svx_resolved_free(svx_resolved_t* res);
 
 /* ---- K1-K4: assembly on the device ------------------------------- */

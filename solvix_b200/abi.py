@@ -296,6 +296,7 @@ SIGNATURES = {
     "svx_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
     "svx_resolve": (C.c_int, [C.POINTER(SvxModelDesc), C.POINTER(_VP), C.POINTER(SvxError)]),
     "svx_resolved_flat": (C.POINTER(SvxFlatModel), [_VP]),
+    "svx_resolved_pending": (C.c_int, [_VP, C.POINTER(SvxError)]),
     "svx_resolved_free": (C.c_int, [_VP]),
     "svx_assemble": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.c_uint32, C.POINTER(_VP),
                                C.POINTER(SvxError)]),

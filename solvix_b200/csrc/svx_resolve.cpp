@@ -229,6 +229,17 @@ int svx_resolve(const svx_model_desc_t* desc, svx_resolved_t** out, svx_error_t*
     }
 }
 
+int svx_resolved_pending(const svx_resolved_t* res, svx_error_t* err) {
+    if (!res) return SVX_BAD_ARGUMENT;
+    if (err) {
+        std::memset(err, 0, sizeof(*err));
+        err->code = res->pending_code;
+        err->elem_index = -1;
+        std::snprintf(err->message, sizeof(err->message), "%s", res->pending_msg.c_str());
+    }
+    return res->pending_code;
+}
+
 const svx_flat_model_t* svx_resolved_flat(const svx_resolved_t* res) {
     return res ? &res->flat : nullptr;
 }

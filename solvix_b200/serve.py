@@ -18,7 +18,15 @@ has finished) with exit code 0.  A request line is
      "loads": [[row, value], ...]}}
 
 (0-based node indices, element kinds in the reference's ElemKind order,
-rows = node * ndof + dof).  A result line carries the fields of the
+rows = node * ndof + dof), or a deck as it arrives:
+
+    {"id": <any>, "deck": "<.inp text>"}
+
+read by the linear-static .inp reader (svx_inp_parse) and resolved on the
+host (svx_resolve): a parse error answers {"ok": false, "stage": "parse",
+"error": "line 7: ..."} as the reference's CLI does (main.rs:1150-1163),
+and a CLOAD / BC error the reference raises after the element loop is
+reported only when the solve finds no failing element.  A result line carries the fields of the
 reference's success envelope (crates/solvix-cli/src/main.rs:889-938:
 iterations, solver_method, cond_estimate, residual, solve_ms, max_disp_mm,
 max_von_mises_mpa) plus latency_ms and batch_size; a failed request gets
@@ -183,6 +191,57 @@ def error_json(ident, stage: str, message: str) -> dict:
     return {"id": ident, "ok": False, "stage": stage, "error": message}
 
 
+class DeckError(Exception):
+    """A deck request that fails before it reaches the device."""
+
+    def __init__(self, stage: str, message: str):
+        super().__init__(message)
+        self.stage = stage
+
+
+def flat_from_deck(text: str):
+    """.inp text -> (FlatModel, pending error message or None), through
+    svx_inp_parse and svx_resolve; raises DeckError("parse" | "solve")."""
+    lib = abi.load()
+    raw = text.encode()
+    h = C.c_void_p()
+    err = abi.SvxError()
+    st = lib.svx_inp_parse(raw, len(raw), C.byref(h), C.byref(err))
+    if st == abi.SVX_PARSE_ERROR:
+        raise DeckError("parse", f"line {int(err.elem_index)}: {err.message.decode()}")
+    if st != abi.SVX_OK:
+        raise DeckError("parse", err.message.decode() or f"deck rejected ({st})")
+    res = C.c_void_p()
+    try:
+        st = lib.svx_resolve(lib.svx_inp_model(h), C.byref(res), C.byref(err))
+        if st != abi.SVX_OK:
+            raise DeckError("solve", solve_error_message(st, err.message.decode()))
+        try:
+            d = lib.svx_resolved_flat(res).contents
+            nn, ne, nf = int(d.n_nodes), int(d.n_elem), int(d.n_fixed)
+            ndof = int(d.ndof)
+
+            def arr(p, n, dt):
+                return np.ctypeslib.as_array(p, shape=(n,)).astype(dt) if n else \
+                    np.zeros(0, dt)
+            conn_ptr = arr(d.conn_ptr, ne + 1, np.int64)
+            flat = FlatModel(
+                xyz=arr(d.xyz, 3 * nn, np.float64).reshape(nn, 3), kind=arr(d.kind, ne, np.uint8),
+                conn_ptr=conn_ptr, conn=arr(d.conn, int(conn_ptr[-1]), np.int32),
+                youngs=arr(d.youngs, ne, np.float64), poisson=arr(d.poisson, ne, np.float64),
+                thickness=float(d.thickness), ndof=ndof,
+                fixed_row=arr(d.fixed_row, nf, np.int64), f=arr(d.f, nn * ndof, np.float64),
+                node_id=arr(d.node_id, nn, np.uint32), elem_id=arr(d.elem_id, ne, np.uint32),
+                no_material=arr(d.no_material, ne, np.uint8) if d.no_material else None)
+            pst = lib.svx_resolved_pending(res, C.byref(err))
+            pending = solve_error_message(pst, err.message.decode()) if pst else None
+        finally:
+            lib.svx_resolved_free(res)
+    finally:
+        lib.svx_inp_free(h)
+    return flat, pending
+
+
 def result_json(ident, r: dict) -> dict:
     if r["status"] != abi.SVX_OK:
         return error_json(ident, "solve", solve_error_message(
@@ -212,6 +271,7 @@ def serve_json(inp, out, server: Server) -> int:
     ``out``; returns the process exit code (0)."""
     lock = threading.Lock()
     ids = {}
+    late_errors = {}
     pending = [0]
     eof = threading.Event()
 
@@ -230,8 +290,12 @@ def serve_json(inp, out, server: Server) -> int:
                 continue
             with lock:
                 ident = ids.pop(r["tag"], None)
+                late = late_errors.pop(r["tag"], None)
                 pending[0] -= 1
-            emit(result_json(ident, r))
+            if late is not None and r["status"] == abi.SVX_OK:
+                emit(error_json(ident, "solve", late))
+            else:
+                emit(result_json(ident, r))
 
     t = threading.Thread(target=drain, daemon=True)
     t.start()
@@ -240,21 +304,31 @@ def serve_json(inp, out, server: Server) -> int:
         line = line.strip()
         if not line:
             continue
+        late = None
         try:
             req = json.loads(line)
             ident = req.get("id")
-            flat = flat_from_json(req["model"])
+            if "deck" in req:
+                flat, late = flat_from_deck(req["deck"])
+            else:
+                flat = flat_from_json(req["model"])
+        except DeckError as e:
+            emit(error_json(ident, e.stage, str(e)))
+            continue
         except Exception as e:  # malformed request: answer and keep serving
             emit(error_json(None, "parse", f"bad request: {e}"))
             continue
         tag += 1
         with lock:
             ids[tag] = ident
+            if late is not None:
+                late_errors[tag] = late
             pending[0] += 1
         st, msg = server.submit(flat, tag)
         if st != abi.SVX_OK:
             with lock:
                 ids.pop(tag, None)
+                late_errors.pop(tag, None)
                 pending[0] -= 1
             emit(error_json(ident, "solve", solve_error_message(st, msg)))
     eof.set()

@@ -128,3 +128,65 @@ def test_sharding_is_a_balanced_partition():
         loads = [sum(estimated_work(n_dof[i]) for i in s) for s in shards]
         assert max(loads) <= 1.05 * (sum(loads) / world) + max(estimated_work(n) for n in n_dof)
         assert shards == shard_instances(n_dof, world)  # deterministic
+
+
+def small_deck(cload_node=10, bcs=True, bad_line=None):
+    """A 4x1 CPS4 strip of my own: nodes 1-10 row-major, clamped at x = 0."""
+    lines = ["*HEADING", " strip"]
+    lines.append("*NODE")
+    for j in range(2):
+        for i in range(5):
+            lines.append(f"{j * 5 + i + 1}, {0.25 * i}, {0.1 * j}")
+    if bad_line is not None:
+        lines[bad_line - 1] = "3, x.y, 0.0"
+    lines.append("*ELEMENT, TYPE=CPS4, ELSET=ALL")
+    for i in range(4):
+        lines.append(f"{i + 1}, {i + 1}, {i + 2}, {i + 7}, {i + 6}")
+    lines += ["*MATERIAL, NAME=STEEL", "*ELASTIC", "210e9, 0.3",
+              "*SOLID SECTION, ELSET=ALL, MATERIAL=STEEL", "0.01", "*STEP", "*STATIC"]
+    if bcs:
+        lines += ["*BOUNDARY", "1, 1, 2", "6, 1, 2"]
+    lines += ["*CLOAD", f"{cload_node}, 2, -100.0", "*END STEP"]
+    return "\n".join(lines) + "\n"
+
+
+def run_lines(lines):
+    out = io.StringIO()
+    assert serve_json(io.StringIO("\n".join(lines) + "\n"), out, FakeServer()) == 0
+    return [json.loads(l) for l in out.getvalue().splitlines()]
+
+
+def test_deck_requests_are_read_resolved_and_solved():
+    from oracle import oracle
+    from solvix_b200.inp import parse_inp
+    from solvix_b200.serve import flat_from_deck
+    flat, late = flat_from_deck(small_deck())
+    assert late is None and flat.ndof == 2 and flat.n_elem == 4
+    want, _ = oracle.resolve(parse_inp(small_deck())[0])
+    for name in ("xyz", "kind", "conn_ptr", "conn", "youngs", "poisson", "fixed_row", "f"):
+        assert np.array_equal(getattr(flat, name), getattr(want, name)), name
+    out = run_lines([json.dumps({"id": "a", "deck": small_deck()})])
+    assert out == [dict(out[0], id="a", ok=True)] and out[0]["iterations"] == 10
+
+
+def test_deck_errors_follow_the_reference_stages_and_order():
+    out = run_lines([json.dumps({"id": 1, "deck": small_deck(bad_line=5)}),
+                     json.dumps({"id": 2, "deck": small_deck(bcs=False)}),
+                     json.dumps({"id": "x", "deck": small_deck(cload_node=99)})])
+    by_id = {o["id"]: o for o in out}
+    assert by_id[1] == {"id": 1, "ok": False, "stage": "parse",
+                        "error": "line 5: malformed coordinate 'x.y'"}
+    assert by_id[2] == {"id": 2, "ok": False, "stage": "solve", "error": "no constraints"}
+    # the CLOAD error is raised after the element loop: reported once the
+    # solve found no failing element
+    assert by_id["x"] == {"id": "x", "ok": False, "stage": "solve",
+                          "error": "invalid model: load on unknown node 99"}
+    # ... and an element failure wins over it (the fake server fails the
+    # third submitted request, tag 3)
+    out = run_lines([json.dumps({"id": "g1", "deck": small_deck()}),
+                     json.dumps({"id": "g2", "deck": small_deck()}),
+                     json.dumps({"id": "y", "deck": small_deck(cload_node=99)})])
+    by_id = {o["id"]: o for o in out}
+    assert by_id["g1"]["ok"] and by_id["g2"]["ok"]
+    assert by_id["y"]["ok"] is False and by_id["y"]["stage"] == "solve"
+    assert by_id["y"]["error"].startswith("invalid model: element 2")
