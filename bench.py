@@ -13,10 +13,18 @@ of 1e-10 and von Mises / reaction recovery.
   (svx_solve_flat) from pinned host buffers: the model's H2D copy and the
   D2H read of u, displacements, von Mises and reactions are inside the
   timed region.
-* ``roofline`` - the SpMV kernel (spmv_dot) against the measured HBM copy
-  peak, from its algorithmic bytes and its live CUDA-event duration.
+* ``roofline`` - the dominant kernel (the persistent PCG kernel) against
+  the measured HBM copy peak, from its algorithmic bytes and its live
+  CUDA-event duration.
 * ``cpu_baseline`` - the oracle (the C++ restatement of the reference's
   Rust path) solving the same model on the host cores.
+* ``precision_c3``, ``batched_c4``, ``served_c5`` - the metric's own
+  comparisons, measured in the same single-GPU run after the plain line
+  (skipped with ``--plain-only`` and under torchrun): FP64 against mixed on
+  the 480x48x48 heterogeneous C3D8 model; the 4,096-plate mix batched in
+  FP64 and mixed against one-at-a-time FP64 solves; a reduced served stream
+  in mixed precision with p50/p95/p99 latency, the FP64 saturation beside
+  it, and the 4,096-plate mix through the server.
 
 ``--form direct`` times the direct path (RCM-ordered band LDL^T on the
 device, the reference's Method::Ldlt) on the mesh of the reference's own
@@ -56,20 +64,35 @@ def parse_args():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default=None,
                     help="plain, batched and served forms: fp64 (default) or the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="plain form: skip the precision / batched / served blocks that the "
+                         "default single-GPU line carries beside the plain solve")
     ap.add_argument("--form",
-                    choices=["plain", "batched", "precision", "served", "thermal", "direct"],
+                    choices=["plain", "batched", "precision", "served", "thermal", "direct",
+                             "kernels"],
                     default="plain",
                     help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
                          "2D plates in one launch; precision: FP64 vs mixed on the "
                          "480x48x48 heterogeneous C3D8 model; served: Poisson request "
                          "stream through the continuous-batching server; thermal: steady "
                          "conduction in a 480x48x48 C3D8 block; direct: the band LDL^T "
-                         "direct path")
+                         "direct path; kernels: device times of single kernels on one "
+                         "workload (the command the profiles are captured with)")
     ap.add_argument("--direct-workload", choices=["hex40", "c2"], default="hex40",
                     help="direct form: the 40x4x4 hex cantilever of the reference's LDL^T "
                          "test (default) or the 160x16x16 C3D8 cantilever")
     ap.add_argument("--requests", type=int, default=20000,
                     help="served form: requests per rate point")
+    ap.add_argument("--workload", choices=sorted(KERNEL_WORKLOADS), default="c3d8_160",
+                    help="kernels form: the model")
+    ap.add_argument("--kernel-mode", choices=["iteration", "solve", "batch", "batch-3d",
+                                              "direct"], default="iteration",
+                    help="kernels form: the iteration kernels back to back (iteration), one "
+                         "FP64 solve (solve), one batched solve of --batch-count plates or "
+                         "C3D8 cantilevers of the served stream (batch, batch-3d), the direct "
+                         "path (direct)")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--reps", type=int, default=20, help="kernels form: launches per kernel")
     ap.add_argument("--rates", type=str, default="",
                     help="served form: comma-separated arrival rates (requests/s); default "
                          "fractions of the measured saturation throughput")
@@ -290,7 +313,7 @@ def run_ours(args, rank, world, local_rank):
     # roofline of the dominant kernel, the persistent PCG kernel: its
     # algorithmic bytes per launch (CHUNK iterations) over its average
     # launch duration, from the PCG device time of the timed steps
-    from solvix_b200.kernel_timer import pcg_iteration_bytes, spmv_node_bytes
+    from solvix_b200.roofline import pcg_iteration_bytes, spmv_node_bytes
     # iterations per persistent launch (persistent_chunk in svx_pcg.cu)
     chunk = 64 if nnz > 100_000_000 else (256 if nnz > 10_000_000 else 1024)
     it_total = float(np.sum(iters))
@@ -461,7 +484,7 @@ def run_batched(args, rank, world, local_rank):
     import torch
 
     from solvix_b200 import Context, abi, workloads
-    from solvix_b200.kernel_timer import pcg_iteration_bytes
+    from solvix_b200.roofline import pcg_iteration_bytes
     from solvix_b200.sharding import shard_instances
 
     torch.cuda.set_device(local_rank)
@@ -598,7 +621,7 @@ def run_precision(args, rank, world, local_rank):
                 np.linalg.norm(res["fp64"]["u"]))
     peak, peak_kind = measured_peaks()
     nnz = op.nnz
-    from solvix_b200.kernel_timer import spmv_node_bytes
+    from solvix_b200.roofline import spmv_node_bytes
     spmv_bytes = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
     fp32_bytes = spmv_bytes - 4 * nnz
     f64 = res["fp64"]
@@ -707,7 +730,7 @@ def run_served(args, rank, world, local_rank):
     import torch
 
     from solvix_b200 import Context, abi, workloads
-    from solvix_b200.kernel_timer import pcg_iteration_bytes
+    from solvix_b200.roofline import pcg_iteration_bytes
     from solvix_b200.serve import Server
 
     torch.cuda.set_device(local_rank)
@@ -855,6 +878,267 @@ def run_served(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------
+# The metric's own comparisons (mixed / batched / served against FP64), run
+# after the plain line in the default single-GPU bench and reported beside it.
+# ---------------------------------------------------------------------------
+def _rel(a, b):
+    import numpy as np
+    return float(np.linalg.norm(a - b) / max(float(np.linalg.norm(b)), 1e-300))
+
+
+def _device_timed(stream, fn):
+    """fn() between two CUDA events on the library's stream; (result, ms)."""
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def precision_block(local_rank):
+    """The 480x48x48 heterogeneous C3D8 cantilever: one FP64 and one mixed
+    solve (reassembly + PCG + stress) of the same device-resident operator,
+    each timed with CUDA events on the library's stream; the mixed form's
+    iteration split and its displacement error against the FP64 solve (the
+    oracle itself cannot solve this size: hours and ~20 GB of triplets)."""
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, abi, workloads
+    from solvix_b200.model import NotConverged
+
+    flat = workloads.heterogeneous_c3d8(480, 48, 48, seed=3)
+    n = flat.n_dof
+    with Context(local_rank) as ctx:
+        stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
+        op = ctx.assemble(flat)
+        try:
+            for prec in (abi.SVX_FP64, abi.SVX_MIXED):  # graphs, pools, first launches
+                try:
+                    op.solve_device(precision=prec, max_iter=64, want_stress=False)
+                except NotConverged:
+                    pass
+            clocks = ClockSampler(local_rank)
+            clocks.start()
+            res = {}
+            for name, prec in (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED)):
+                def one():
+                    op.reassemble()
+                    return op.solve_device(precision=prec, max_iter=200000, want_stress=True)
+                (it, r, ms_s, _ms_st, ms_a), ms = _device_timed(stream, one)
+                fp32_it = op.last_fp32_iterations
+                disp = op.stress()[3]
+                res[name] = {"iterations": it, "fp32_iterations": fp32_it, "ms": ms,
+                             "pcg_ms": ms_s, "residual": r,
+                             "u": np.asarray(disp).reshape(-1, 3)[:, :flat.ndof].ravel()}
+            clk = clocks.stop()
+            kms = op.time_kernels(reps=10)
+            nnz = op.nnz
+        finally:
+            op.free()
+    from solvix_b200.roofline import spmv_node_bytes
+    spmv64 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
+    spmv32 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes, value_bytes=4)
+    peak, peak_kind = measured_peaks()
+    f64, mx = res["fp64"], res["mixed"]
+    row = lambda d: {"iterations": d["iterations"], "ms_per_solve": d["ms"],
+                     "pcg_ms": d["pcg_ms"], "solves_per_s": 1000.0 / d["ms"],
+                     "dof_iter_per_s": n * d["iterations"] / (d["ms"] / 1000.0),
+                     "residual": d["residual"]}
+    out = {
+        "workload": PRECISION_NAME, "n_dof": n, "nnz": nnz,
+        "fp64": row(f64),
+        "mixed": dict(row(mx), fp32_iterations=mx["fp32_iterations"],
+                      fp32_share=mx["fp32_iterations"] / max(1, mx["iterations"]),
+                      rel_err_vs_fp64=_rel(mx["u"], f64["u"])),
+        "ratio_mixed_over_fp64": f64["ms"] / mx["ms"],
+        "spmv_fp64": {"ms": float(kms[0]), "gbs": spmv64 / kms[0] / 1e6,
+                      "frac": spmv64 / kms[0] / 1e6 / peak},
+        "spmv_fp32": {"ms": float(kms[3]), "gbs": spmv32 / kms[3] / 1e6,
+                      "frac": spmv32 / kms[3] / 1e6 / peak},
+        "peak_gbs": peak, "peak_source": peak_kind,
+        "timing": "CUDA events on the library stream around reassembly + PCG + stress of one "
+                  "solve per precision, after a 64-iteration warm-up of each; K (2.3 GB FP64) "
+                  "is larger than L2",
+        "clocks": clk,
+    }
+    return out
+
+
+def _serve_summary(results, wall, reqs):
+    import numpy as np
+
+    from solvix_b200.roofline import pcg_iteration_bytes
+    lat = np.array([r["t_done_ms"] - r["t_submit_ms"] for r in results.values()])
+    ok = [r for r in results.values() if r["status"] == 0]
+    dof_it = float(sum(reqs[r["tag"]].n_dof * r["iterations"] for r in results.values()))
+    alg = float(sum(r["iterations"] * pcg_iteration_bytes(
+        reqs[r["tag"]].n_dof, r["nnz"], reqs[r["tag"]].ndof, reqs[r["tag"]].n_nodes)
+        for r in ok))
+    return {"requests": len(results), "failed": len(results) - len(ok),
+            "solves_per_s": len(ok) / wall, "dof_iter_per_s": dof_it / wall,
+            "algorithmic_gbs": alg / wall / 1e9,
+            "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+            "p99_ms": float(np.percentile(lat, 99)),
+            "mean_batch": float(np.mean([r["batch_size"] for r in results.values()])),
+            "wall_s": wall}
+
+
+def _served_saturation(local_rank, prec, reqs):
+    """Every request submitted at once to a fresh server (after a warm-up of
+    the first 256); returns (server, summary)."""
+    import numpy as np
+
+    from solvix_b200.serve import Server
+    srv = Server(local_rank, precision=prec)
+    warm = reqs[:min(len(reqs), 256)]
+    _serve_run(srv, warm, 0.0, np.zeros(len(warm)))
+    res, wall = _serve_run(srv, reqs, 0.0, np.zeros(len(reqs)))
+    return srv, _serve_summary(res, wall, reqs)
+
+
+def batched_block(local_rank):
+    """The 4,096-plate mix through svx_batch_solve in FP64 and mixed, against
+    the one-at-a-time plain FP64 GPU path (svx_solve_flat) on a sample."""
+    import numpy as np
+    import torch
+
+    from solvix_b200 import Context, abi, workloads
+
+    torch.cuda.set_device(local_rank)
+    flats = workloads.plate_batch(4096, seed=4)
+    total_dof = int(sum(f.n_dof for f in flats))
+    out = {"workload": BATCH_NAME, "models": len(flats), "total_dof": total_dof}
+    us = {}
+    with Context(local_rank) as ctx:
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        for name, prec in (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED)):
+            ctx.solve_batch(flats, precision=prec)  # warm-up (autotune, pools)
+            best = None
+            for _ in range(2):
+                t0 = time.perf_counter()
+                res, st = ctx.solve_batch(flats, precision=prec)
+                wall = time.perf_counter() - t0
+                dev_ms = st["ms_assemble"] + st["ms_solve"] + st["ms_stress"]
+                if best is None or dev_ms < best[1]:
+                    best = (wall, dev_ms, st, res)
+            wall, dev_ms, st, res = best
+            us[name] = [r["u"] for r in res]
+            its = np.array([r["iterations"] for r in res])
+            out[name] = {
+                "solves_per_s_device": len(flats) / (dev_ms / 1000.0),
+                "solves_per_s_e2e": len(flats) / wall,
+                "dof_iter_per_s_device": float(sum(f.n_dof * int(r["iterations"])
+                                                   for f, r in zip(flats, res))) /
+                (dev_ms / 1000.0),
+                "ms_device": dev_ms, "ms_pcg": st["ms_solve"], "wall_s": wall,
+                "iterations_mean": float(its.mean()), "not_converged": int(st["not_converged"]),
+                "fp32_iterations": int(st["fp32_iterations"])}
+        rng = np.random.default_rng(0)
+        idx = [int(k) for k in rng.choice(len(flats), 64, replace=False)]
+        per, dev_one = one_at_a_time(ctx, [flats[k] for k in idx])
+        clk = clocks.stop()
+    out["one_at_a_time"] = {"solves_per_s": 1.0 / per, "device_ms_per_solve": dev_one,
+                            "sample": "64 models of the mix through svx_solve_flat (FP64), one "
+                                      "after another, wall clock, faster of two passes"}
+    for name in ("fp64", "mixed"):
+        out[name]["ratio_device_vs_one_at_a_time"] = out[name]["solves_per_s_device"] * per
+        out[name]["ratio_e2e_vs_one_at_a_time"] = out[name]["solves_per_s_e2e"] * per
+    errs = [_rel(a, b) for a, b in zip(us["mixed"], us["fp64"])]
+    out["mixed"]["rel_err_vs_fp64"] = {"max": max(errs), "median": float(np.median(errs))}
+    out["timing"] = ("device = the call's CUDA-event times (assembly + batched PCG + von "
+                     "Mises), e2e = wall clock of the svx_batch_solve call from host arrays; "
+                     "best of 2 after a warm-up")
+    out["clocks"] = clk
+    return out, per
+
+
+def served_block(local_rank, c4_one_at_a_time_s=None, count=2000):
+    """A reduced C5 stream (the first `count` requests: 70% plates, 30% C3D8
+    cantilevers) served in mixed precision as C5 specifies, at saturation
+    and as a Poisson stream at half the saturation rate (p50/p95/p99), the
+    FP64 saturation beside it, against one-at-a-time FP64 solves of a
+    sample; then the 4,096-plate mix through the same server."""
+    import numpy as np
+
+    from solvix_b200 import Context, abi, workloads
+    from solvix_b200.serve import Server
+
+    stream = workloads.request_stream(count, 1.0, seed=5)
+    reqs = [m for _, m in stream]
+    base_t = np.array([t for t, _ in stream])
+    out = {"workload": SERVED_NAME.replace("2 lanes", f"2 lanes; first {count} requests"),
+           "requests": count}
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    srv, sat = _served_saturation(local_rank, abi.SVX_MIXED, reqs)
+    rate = round(0.5 * sat["solves_per_s"], 1)
+    res, wall = _serve_run(srv, reqs, 1.0 / rate, base_t)
+    poisson = _serve_summary(res, wall, reqs)
+    poisson["rate_per_s"] = rate
+    srv.close()
+    srv64, sat64 = _served_saturation(local_rank, abi.SVX_FP64, reqs)
+    srv64.close()
+    # error of the served mixed results against one-at-a-time FP64 solves
+    rng = np.random.default_rng(1)
+    idx = [int(i) for i in rng.choice(len(reqs), 48, replace=False)]
+    with Server(local_rank, lanes=1, precision=abi.SVX_MIXED) as one:
+        for k in idx:
+            one.submit(reqs[k], k)
+        served_u = {}
+        while len(served_u) < len(idx):
+            r = one.poll(200)
+            if r is not None:
+                served_u[r["tag"]] = r["u"]
+    with Context(local_rank) as ctx:
+        errs = [_rel(served_u[k], ctx.solve_flat(reqs[k]).u) for k in idx]
+        per, dev_one = one_at_a_time(ctx, [reqs[k] for k in idx])
+    out["mixed_saturation"] = sat
+    out["mixed_poisson"] = poisson
+    out["fp64_saturation"] = sat64
+    out["latency_ms"] = {"p50": poisson["p50_ms"], "p95": poisson["p95_ms"],
+                         "p99": poisson["p99_ms"], "at_rate_per_s": rate,
+                         "precision": "mixed"}
+    out["one_at_a_time"] = {"solves_per_s": 1.0 / per, "device_ms_per_solve": dev_one,
+                            "sample": "48 requests through svx_solve_flat (FP64), one after "
+                                      "another, wall clock, faster of two passes"}
+    out["ratio_mixed_vs_one_at_a_time"] = sat["solves_per_s"] * per
+    out["ratio_fp64_vs_one_at_a_time"] = sat64["solves_per_s"] * per
+    out["mixed_rel_err_vs_fp64"] = {"max": max(errs), "median": float(np.median(errs)),
+                                    "sample": len(errs)}
+    # the 4,096-plate mix through the same server (the batched form's mix)
+    plates = workloads.plate_batch(4096, seed=4)
+    c4 = {}
+    for name, prec in (("mixed", abi.SVX_MIXED), ("fp64", abi.SVX_FP64)):
+        s, row = _served_saturation(local_rank, prec, plates)
+        s.close()
+        if c4_one_at_a_time_s:
+            row["ratio_vs_one_at_a_time"] = row["solves_per_s"] * c4_one_at_a_time_s
+        c4[name] = row
+    out["plates4096_saturation"] = c4
+    out["clocks"] = clocks.stop()
+    out["timing"] = ("wall clock from the first submit to the last result on the host; "
+                     "latency from each submit to its result")
+    return out
+
+
+def metric_forms(local_rank):
+    """precision_c3, batched_c4 and served_c5 blocks of the default line."""
+    blocks = {}
+    t0 = time.perf_counter()
+    blocks["precision_c3"] = precision_block(local_rank)
+    blocks["batched_c4"], per_c4 = batched_block(local_rank)
+    blocks["served_c5"] = served_block(local_rank, c4_one_at_a_time_s=per_c4)
+    blocks["metric_forms_wall_s"] = time.perf_counter() - t0
+    return blocks
+
+
 THERMAL_NAME = ("steady conduction in a C3D8 block 480x48x48 over 2.0x0.2x0.2 m (1,154,881 "
                 "nodes = DOF, 30,297,025 nnz), k=45, uniform source 1e5, T=20 on x=0 and T=80 "
                 "on x=L; relative residual 1e-10")
@@ -895,7 +1179,7 @@ def run_thermal(args, rank, world, local_rank):
 
     from oracle import oracle
     from solvix_b200 import Context
-    from solvix_b200.kernel_timer import pcg_iteration_bytes
+    from solvix_b200.roofline import pcg_iteration_bytes
 
     torch.cuda.set_device(local_rank)
     nx, ny, nz = 480, 48, 48
@@ -1112,6 +1396,92 @@ def run_direct(args, rank, world, local_rank):
     return line
 
 
+KERNEL_WORKLOADS = {
+    "c3d8_160": ("C3D8 cantilever 160x16x16 (C2)",
+                 lambda w: w.cantilever_c3d8(160, 16, 16)),
+    "c3d8_480": ("heterogeneous C3D8 cantilever 480x48x48 (C3)",
+                 lambda w: w.heterogeneous_c3d8(480, 48, 48)),
+    "c3d8_240": ("heterogeneous C3D8 cantilever 240x24x24",
+                 lambda w: w.heterogeneous_c3d8(240, 24, 24)),
+    "hetero_160": ("heterogeneous C3D8 cantilever 160x16x16",
+                   lambda w: w.heterogeneous_c3d8(160, 16, 16)),
+    "cps4_200": ("CPS4 cantilever 200x20 (C1)", lambda w: w.cantilever_cps4(200, 20)),
+    "c3d8_40x4x4": ("C3D8 cantilever 40x4x4",
+                    lambda w: w.cantilever_c3d8(40, 4, 4, lx=2.0, ly=0.1, lz=0.1)),
+}
+
+
+def run_kernels(args, local_rank):
+    """--form kernels: device times of single kernels on one workload, small
+    and self-contained so that ncu can capture one kernel of it.
+
+    * iteration: the FP64 node-block SpMV + p.Kp, the u/r update, the p
+      update and the FP32 difference-form SpMV, each over --reps
+      back-to-back launches (CUDA events);
+    * solve: one full FP64 solve (the persistent kernel below 50M nonzeros);
+    * batch / batch-3d: one batched solve of the first --batch-count plates
+      of the 4,096-plate mix / C3D8 cantilevers of the served stream;
+    * direct: the direct path twice, the second run's device time."""
+    from solvix_b200 import Context, abi, workloads
+    from solvix_b200.roofline import pcg_iteration_bytes, spmv_node_bytes
+
+    out = {"form": "kernels", "mode": args.kernel_mode}
+    prec = abi.SVX_MIXED if args.precision == "mixed" else abi.SVX_FP64
+    with Context(local_rank) as ctx:
+        if args.kernel_mode in ("batch", "batch-3d"):
+            if args.kernel_mode == "batch":
+                flats = workloads.plate_batch(4096, seed=4)[:args.batch_count]
+            else:
+                stream = workloads.request_stream(max(64, 4 * args.batch_count), 1.0, seed=5)
+                flats = [m for _, m in stream if m.ndof == 3][:args.batch_count]
+            res, st = ctx.solve_batch(flats, precision=prec)
+            b = sum(r["iterations"] * pcg_iteration_bytes(f.n_dof, r["nnz"], f.ndof, f.n_nodes)
+                    for f, r in zip(flats, res))
+            out.update({"models": len(flats), "total_dof": int(st["total_dof"]),
+                        "iterations": int(sum(r["iterations"] for r in res)),
+                        "pcg_ms": st["ms_solve"], "threads_per_cta": st["threads_per_cta"],
+                        "lanes_per_node": st["lanes_per_node"],
+                        "cluster_members": st["cluster_members"], "algorithmic_bytes": b,
+                        "gbs": b / (st["ms_solve"] * 1e-3) / 1e9})
+            return out
+        name, make = KERNEL_WORKLOADS[args.workload]
+        flat = make(workloads)
+        out["workload"] = name
+        if args.kernel_mode == "direct":
+            for _ in range(2):
+                sol = ctx.solve_flat(flat, want_stress=False, method=abi.SVX_METHOD_LDLT)
+            n, bw = flat.n_dof, sol.factor_bandwidth
+            out.update({"n": n, "bandwidth": bw, "direct_ms": sol.ms_factor,
+                        "residual": sol.final_residual,
+                        "band_gflops": n * bw * bw / (sol.ms_factor * 1e-3) / 1e9})
+            return out
+        op = ctx.assemble(flat)
+        try:
+            n, nnz = op.n, op.nnz
+            out.update({"n": n, "nnz": nnz})
+            if args.kernel_mode == "solve":
+                it, res, ms_solve, _, _ = op.solve_device(precision=prec, want_stress=False,
+                                                          max_iter=200000)
+                b = pcg_iteration_bytes(n, nnz, flat.ndof, flat.n_nodes)
+                out.update({"iterations": it, "residual": res, "pcg_ms": ms_solve,
+                            "fp32_iterations": op.last_fp32_iterations,
+                            "us_per_iteration": 1000.0 * ms_solve / max(1, it),
+                            "bytes_per_iteration": b,
+                            "gbs": b * it / (ms_solve * 1e-3) / 1e9})
+            else:
+                ms = op.time_kernels(reps=args.reps)
+                b64 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
+                b32 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes, value_bytes=4)
+                out.update({"reps": args.reps, "spmv_ms": ms[0], "update_ms": ms[1],
+                            "p_update_ms": ms[2], "spmv_fp32_ms": ms[3],
+                            "spmv_bytes": b64, "spmv_gbs": b64 / (ms[0] * 1e-3) / 1e9,
+                            "spmv_fp32_bytes": b32,
+                            "spmv_fp32_gbs": b32 / (ms[3] * 1e-3) / 1e9})
+        finally:
+            op.free()
+    return out
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1139,8 +1509,12 @@ def main():
             line = run_thermal(args, rank, world, local_rank) if rank == 0 else None
         elif args.form == "direct":
             line = run_direct(args, rank, world, local_rank) if rank == 0 else None
+        elif args.form == "kernels":
+            line = run_kernels(args, local_rank) if rank == 0 else None
         else:
             line = run_ours(args, rank, world, local_rank)
+            if world == 1 and not args.plain_only:
+                line.update(metric_forms(local_rank))
     finally:
         if world > 1:
             import torch

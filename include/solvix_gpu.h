@@ -567,26 +567,35 @@ int svx_diag_barrier_timeout(int device, long long spins, int* returned_ok, int*
  * an application that manages all device memory through its own arena, or
  * a latency-bounded loop that cannot absorb the implicit synchronisation of
  * cudaMalloc / cudaFree.  This entry point has no counterpart in the
- * reference; it runs the same kernels, launch geometry and stopping rule as
- * svx_op_solve (FP64).
+ * reference.  It runs the FP64 Jacobi-PCG recurrence and stopping rule of
+ * svx_op_solve (||r|| / ||f|| <= tol checked after each r update, the same
+ * iteration count semantics) on a row-CSR SpMV with its own launch
+ * geometry, not on svx_op_solve's node-block kernels, so its reduction
+ * order, and with it the last bits of u and the iteration count, can differ
+ * from svx_op_solve's on the same system.
  *
  * Every pointer but `iterations` / `residual` (host) is a device pointer of
  * the current device: row_ptr [n + 1] and col_idx [nnz] (int32, sorted
  * columns, the diagonal present), vals [nnz], f [n], u [n] (output).  tol is
- * the relative residual tolerance; max_iter <= 0 means max(1000, 10 n).
- * stream is a cudaStream_t (NULL = the legacy default stream); the call
- * returns after the solve has finished on it.
+ * the relative residual tolerance (>= 0); max_iter <= 0 means
+ * max(1000, 10 n).  stream is a cudaStream_t (NULL = the legacy default
+ * stream); the call returns after the solve has finished on it.
  *
  * Nothing is allocated: the work vectors (4 x SVX_NOALLOC_MAX_DOF doubles,
  * about 8 MB) live in one static device array that every GPU loading this
  * library holds until the process exits.  All calls on a device share that
- * array and it keeps the previous call's contents, so calls whose work
- * overlaps on the GPU (other threads, other streams) race; serialise them.
- * The first call on each device looks up the array's device address, so
- * make that first call before any stream capture.
+ * array and it keeps the previous call's contents (each call clears what
+ * must start at zero), so calls whose work overlaps on the GPU (other
+ * threads, other streams) race; serialise them.  The first call on each
+ * device looks up the array's device address and keeps it, so make that
+ * first call before any stream capture; a cudaDeviceReset of that device
+ * afterwards leaves the kept address stale, so do not call this entry point
+ * on a device again after resetting it in the same process.
  *
- * Returns SVX_OK, SVX_NOT_CONVERGED (iterations / residual filled),
- * SVX_BAD_ARGUMENT (null pointer, n <= 0 or n > SVX_NOALLOC_MAX_DOF) or
+ * Returns SVX_OK; SVX_NOT_CONVERGED when max_iter is reached or the
+ * recurrence breaks down (p.Kp <= 0 or NaN), with iterations / residual
+ * filled and u holding the last iterate; SVX_BAD_ARGUMENT (null pointer,
+ * n <= 0, n > SVX_NOALLOC_MAX_DOF, tol negative or NaN) before any work; or
  * SVX_CUDA_ERROR. */
 int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const int32_t* col_idx,
                           const double* vals, const double* f, double tol, int64_t max_iter,

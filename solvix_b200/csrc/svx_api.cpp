@@ -862,6 +862,11 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
             const long long v = std::strtoll(e, &end, 10);
             if (end != e && v >= 0) ctx->shared_adj_max = v;
         }
+        if (const char* e = std::getenv("SVX_GRAPH_MIN_NNZ")) {
+            char* end = nullptr;
+            const long long v = std::strtoll(e, &end, 10);
+            if (end != e && v >= 0) ctx->graph_min_nnz = v;
+        }
         // the main stream (uploads, assembly, stress, plain solves) has the
         // highest priority; the long batched PCG kernels run on the lowest,
         // so a served lane's assembly gets SMs while another lane's batch

@@ -176,6 +176,11 @@ struct svx_ctx {
     // (bytes; 0 keeps it in global memory); SVX_SHARED_ADJ_MAX in the
     // environment at svx_ctx_create overrides the build's default
     long long shared_adj_max = -1;
+    // systems with more nonzeros than this iterate with the standalone
+    // kernels in a CUDA graph instead of the persistent kernel (-1: the
+    // build's default); SVX_GRAPH_MIN_NNZ in the environment at
+    // svx_ctx_create overrides it
+    long long graph_min_nnz = -1;
 };
 
 namespace svx {

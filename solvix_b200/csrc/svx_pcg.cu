@@ -1687,20 +1687,6 @@ unsigned grid_vec(const svx_ctx* ctx, int64_t n) {
     return unsigned(std::max<int64_t>(1, std::min(need, cap)));
 }
 
-template <class V>
-void launch_spmv_dot(int G, unsigned grid, cudaStream_t st, int64_t n, const svx_op* op,
-                     const V* vals, const V* p, V* q, double* partials, PcgScalars* s) {
-    const int32_t* rp = op->pat.row_ptr.p;
-    const int32_t* ci = op->pat.col_idx.p;
-    switch (G) {
-        case 2: spmv_dot_kernel<2, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
-        case 4: spmv_dot_kernel<4, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
-        case 8: spmv_dot_kernel<8, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
-        case 16: spmv_dot_kernel<16, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
-        default: spmv_dot_kernel<32, V><<<grid, BLOCK, 0, st>>>(n, rp, ci, vals, p, q, partials, s); break;
-    }
-}
-
 // Lanes per node for the node-block kernels: the smallest of 8 / 16 / 32
 // that covers the largest node degree (27 for interior C3D8 nodes).
 int pick_node_group(int max_deg) {
@@ -1927,6 +1913,11 @@ struct PinnedScalars {
 // absence of launch gaps wins.
 constexpr int64_t GRAPH_MIN_NNZ = 50000000;
 
+bool use_graph_form(const svx_ctx* ctx, const svx_op* op) {
+    const int64_t threshold = ctx->graph_min_nnz >= 0 ? ctx->graph_min_nnz : GRAPH_MIN_NNZ;
+    return op->pat.nnz > threshold;
+}
+
 int persistent_chunk(int64_t nnz) {
     if (nnz > 100000000) return 64;
     if (nnz > 10000000) return 256;
@@ -2042,7 +2033,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
-    const bool graph = op->pat.nnz > GRAPH_MIN_NNZ;
+    const bool graph = use_graph_form(ctx, op);
     if (!graph) {
         p2.alloc(ctx->pool, n + 1);
         SVX_CUDA(cudaMemsetAsync(p2.p, 0, (n + 1) * sizeof(double), st));
@@ -2141,7 +2132,7 @@ reliable_resume_kernel(int64_t n, const double* __restrict__ r64, V* __restrict_
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps) {
     if (check_every <= 0) check_every = auto_check_every(op->n, op->pat.nnz);
-    const bool graph = op->pat.nnz > GRAPH_MIN_NNZ;
+    const bool graph = use_graph_form(ctx, op);
     const double delta = (inner_tol > 0.01 && inner_tol < 1.0) ? inner_tol : 0.1;
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
@@ -2396,6 +2387,7 @@ extern "C" int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const in
     using namespace svx;
     if (n <= 0 || !row_ptr || !col_idx || !vals || !f || !u) return SVX_BAD_ARGUMENT;
     if (n > NOALLOC_MAX_N) return SVX_BAD_ARGUMENT;  // beyond the static scratch
+    if (!(tol >= 0.0)) return SVX_BAD_ARGUMENT;      // negative or NaN
     int device = 0, sms = 0;
     double* scratch = nullptr;
     if (noalloc_setup(&device, &scratch, &sms) != cudaSuccess) {
@@ -2420,20 +2412,24 @@ extern "C" int svx_pcg_solve_noalloc(int64_t n, const int32_t* row_ptr, const in
     }
     const int G = pick_group(double(nnz) / double(n));
     const int64_t per_block = BLOCK / G;
-    const unsigned grid_r =
-        unsigned(std::max<int64_t>(1, std::min<int64_t>((n + per_block - 1) / per_block,
-                                                        int64_t(sms) * 8)));
-    const unsigned grid_v = unsigned(
-        std::max<int64_t>(1, std::min<int64_t>((n + BLOCK - 1) / BLOCK, int64_t(sms) * 8)));
-    if (2 * int64_t(std::max(grid_r, grid_v)) + 2 > NOALLOC_PARTIALS) return SVX_BAD_ARGUMENT;
+    // the block partials hold two values per block of the widest grid; the
+    // grids stop at that (a device with more SMs only gets fewer blocks)
+    const int64_t grid_cap =
+        std::min<int64_t>(int64_t(sms) * 8, (NOALLOC_PARTIALS - 2) / 2);
+    const unsigned grid_r = unsigned(std::max<int64_t>(
+        1, std::min<int64_t>((n + per_block - 1) / per_block, grid_cap)));
+    const unsigned grid_v =
+        unsigned(std::max<int64_t>(1, std::min<int64_t>((n + BLOCK - 1) / BLOCK, grid_cap)));
     if (max_iter <= 0) max_iter = std::max<int64_t>(1000, 10 * n);
     const int check_every = auto_check_every(n, nnz);
 
-    // the scalars must start from a clean state every call
+    // the scalars must start from a clean state every call; rr_stop < 0
+    // disables the reliable-update stop, as in the allocating FP64 solve
     PcgScalars init{};
     init.tol = tol;
     init.max_iter = max_iter;
     init.status = PCG_RUNNING;
+    init.rr_stop = -1.0;
     PcgScalars h{};
     cudaError_t e = cudaMemcpyAsync(s, &init, sizeof(init), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {

@@ -1,7 +1,11 @@
 """Generate the golden fixtures under tests/golden/ from the reference's decks.
 
-Run once in a container that has the reference checkout (the path is given
-on the command line, default /root/reference); the GPU box never runs this.
+Run once in a checkout that has the reference beside it, giving the
+reference's root directory as the only argument:
+
+    python tests/golden/make_golden.py <reference-root>
+
+The GPU box never runs this.
 
 For each example deck it writes ``<name>.json`` holding the model exactly as
 the reference's parser would build it for these decks (node ids and
@@ -127,7 +131,7 @@ def read_deck(text: str) -> dict:
     }
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str) -> None:
     for name, gold in GOLDEN.items():
         with open(os.path.join(ref_root, gold["deck"])) as fh:
             model = read_deck(fh.read())
@@ -139,4 +143,6 @@ def main(ref_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference-root>")
+    main(sys.argv[1])
