@@ -131,6 +131,17 @@ typedef struct svx_model_desc {
     const uint32_t* cload_node_ids;
     const int64_t* cload_dofs;       /* 1-based */
     const double* cload_values;
+
+    /* Model::density (kg/m^3) for gravity loads; the reference's Model
+     * default is 7850, so a caller building a model by hand sets it. */
+    double density;
+    int64_t n_dloads;                /* DistributedLoad{element_id, face, magnitude} */
+    const uint32_t* dload_elem_ids;
+    const int64_t* dload_faces;      /* 1-based plane edge (P1..P4) */
+    const double* dload_values;      /* pressure, positive into the element */
+    int32_t has_gravity;             /* the load state's gravity is Some((g, dir)) */
+    double gravity_magnitude;        /* g */
+    double gravity_dir[3];           /* dir (not normalised; plane models use x, y) */
 } svx_model_desc_t;
 
 /* ------------------------------------------------------------------ */
@@ -236,11 +247,14 @@ int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len);
 /* ---- a1: id / material / load resolution (host, O(N)) -------------- */
 /* Replaces Mesh::node_index (lib.rs:106-108), Model::material_for_element
  * (lib.rs:357-367), validate (lib.rs:406-436), ndof_per_node
- * (lib.rs:725-752), the CLOAD loop of assemble_with (assembly.rs:365-380)
- * and constrained_dofs (solver.rs:15-41).  Errors the reference raises
- * before assembly are returned here; errors it raises after the element
- * loop (CLOAD, BC) are kept pending inside the resolved model and reported
- * by svx_solve_resolved only when no element fails first. */
+ * (lib.rs:725-752), the load vector of assemble_with: CLOADs
+ * (assembly.rs:365-380), edge pressure (edge_pressure_forces,
+ * assembly.rs:382, :393-452) and gravity (gravity_forces, assembly.rs:383,
+ * :458-539), and constrained_dofs (solver.rs:15-41).  Errors the reference
+ * raises before assembly are returned here; errors it raises after the
+ * element loop (CLOAD, DLOAD, gravity, BC, in that order) are kept pending
+ * inside the resolved model and reported by svx_solve_resolved only when no
+ * element fails first. */
 int svx_resolve(const svx_model_desc_t* desc, svx_resolved_t** out, svx_error_t* err);
 /* Borrowed view of the resolved flat model (valid until svx_resolved_free). */
 const svx_flat_model_t* svx_resolved_flat(const svx_resolved_t* res);
@@ -351,10 +365,11 @@ int svx_solve_thermal_flat(svx_ctx_t* ctx, const svx_thermal_model_t* model,
 /* ---- .inp reader (linear-static decks) ------------------------------ */
 /* The reference's parse_inp (crates/solvix-io/src/parser.rs:87-1370) for the
  * keywords of linear-static decks (*HEADING, *NODE, *ELEMENT, *NSET, *ELSET
- * [GENERATE], *MATERIAL, *ELASTIC, *SOLID SECTION, *STEP, *STATIC,
- * *BOUNDARY, *CLOAD, *END STEP; unknown keywords are warned and skipped
- * like the reference does), producing the model svx_resolve consumes with
- * the BCs and loads of Model::load_state (lib.rs:388-403).  Returns SVX_OK,
+ * [GENERATE], *MATERIAL, *ELASTIC, *DENSITY, *SOLID SECTION, *STEP,
+ * *STATIC, *BOUNDARY, *CLOAD, *DLOAD [P1..P4, GRAV], *END STEP; unknown
+ * keywords are warned and skipped like the reference does), producing the
+ * model svx_resolve consumes with the BCs and loads of Model::load_state
+ * (lib.rs:388-403).  Returns SVX_OK,
  * SVX_PARSE_ERROR (err->elem_index = the 1-based line, err->message the
  * reference's ParseError message) or SVX_UNSUPPORTED (a keyword the
  * reference reads with another meaning, or *STEP, NLGEOM=YES: parse that

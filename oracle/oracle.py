@@ -11,6 +11,8 @@ host-side model handling in plain Python:
 * ``Mesh::node_index``             lib.rs:106-108 (first node with the id)
 * ``Model::material_for_element``  lib.rs:357-367
 * CLOAD loop of ``assemble_with``  crates/solvix-core/src/assembly.rs:365-380
+* ``edge_pressure_forces``         assembly.rs:382, :393-452
+* ``gravity_forces``               assembly.rs:383, :458-539 (plane kinds)
 * ``constrained_dofs``             crates/solvix-core/src/solver.rs:15-41
 
 Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
@@ -19,6 +21,7 @@ use this module; the product never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 import sys
@@ -139,12 +142,95 @@ def ndof_per_node(kinds) -> int:
     return 3 if solid else 2
 
 
+_KIND_DEBUG = {ElemKind.Cps3: "Cps3", ElemKind.Cps4: "Cps4", ElemKind.Cps8: "Cps8",
+               ElemKind.Cpe4: "Cpe4", ElemKind.Cpe8: "Cpe8", ElemKind.C3d8: "C3d8",
+               ElemKind.C3d4: "C3d4", ElemKind.B31: "B31"}
+
+
+def _edge_pressure(model, dloads, first_index, ndof, f):
+    """edge_pressure_forces (assembly.rs:393-452): pressure * thickness *
+    edge length, half to each end node, along the inward normal."""
+    mesh = model.mesh
+    ids = mesh.elem_ids.tolist()
+    for dl in dloads:
+        try:
+            e = ids.index(int(dl.element_id))
+        except ValueError:
+            return Pending(InvalidModel(f"distributed load on unknown element {dl.element_id}"))
+        kind = ElemKind(int(mesh.elem_kinds[e]))
+        if kind == ElemKind.Cps3:
+            max_face = 3
+        elif kind in (ElemKind.Cps4, ElemKind.Cpe4):
+            max_face = 4
+        else:
+            return Pending(InvalidModel(
+                f"edge pressure on element {dl.element_id} ({_KIND_DEBUG[kind]}) unsupported "
+                "(linear quad/tri edges only)"))
+        if dl.face == 0 or dl.face > max_face:
+            return Pending(InvalidModel(
+                f"element {dl.element_id} ({_KIND_DEBUG[kind]}) has no face {dl.face}"))
+        a = int(mesh.conn_ptr[e])
+        nn = int(mesh.conn_ptr[e + 1]) - a
+        ia = first_index[int(mesh.conn[a + dl.face - 1])]
+        ib = first_index[int(mesh.conn[a + dl.face % nn])]
+        pa = (float(mesh.coords[ia][0]), float(mesh.coords[ia][1]))
+        pb = (float(mesh.coords[ib][0]), float(mesh.coords[ib][1]))
+        d = (pb[0] - pa[0], pb[1] - pa[1])
+        length = math.sqrt(d[0] * d[0] + d[1] * d[1])
+        if length == 0.0:
+            return Pending(InvalidModel(f"zero-length pressure edge on element {dl.element_id}"))
+        n_in = (-d[1] / length, d[0] / length)
+        fmag = float(dl.magnitude) * float(model.thickness) * length / 2.0
+        for i in (ia, ib):
+            f[i * ndof] += fmag * n_in[0]
+            f[i * ndof + 1] += fmag * n_in[1]
+    return None
+
+
+def _gravity(model, gravity, first_index, ndof, f):
+    """gravity_forces (assembly.rs:458-539) for CPS3 (thirds) and CPS4 /
+    CPE4 (quarters); solids are rejected; the kinds the device path does
+    not assemble (CPS8, CPE8, B31) are left out, their element error wins."""
+    if gravity is None:
+        return None
+    g, direction = float(gravity[0]), gravity[1]
+    dir2 = (float(direction[0]), float(direction[1]))
+    if dir2 == (0.0, 0.0):
+        return Pending(InvalidModel("gravity direction has no in-plane component"))
+    mesh = model.mesh
+    rho, t = float(model.density), float(model.thickness)
+    for e in range(mesh.n_elements):
+        kind = ElemKind(int(mesh.elem_kinds[e]))
+        a, b = int(mesh.conn_ptr[e]), int(mesh.conn_ptr[e + 1])
+        idx = [first_index[int(nid)] for nid in mesh.conn[a:b].tolist()]
+        p = [(float(mesh.coords[i][0]), float(mesh.coords[i][1])) for i in idx]
+        if kind == ElemKind.Cps3:
+            cross = (p[1][0] - p[0][0]) * (p[2][1] - p[0][1]) - \
+                (p[1][1] - p[0][1]) * (p[2][0] - p[0][0])
+            per = [rho * t * abs(cross) / 2.0 * g / 3.0] * 3
+        elif kind in (ElemKind.Cps4, ElemKind.Cpe4):
+            shoelace = 0.0
+            for k in range(4):
+                pa, pb = p[k], p[(k + 1) % 4]
+                shoelace += pa[0] * pb[1] - pb[0] * pa[1]
+            per = [rho * t * abs(shoelace) / 2.0 * g / 4.0] * 4
+        elif kind in (ElemKind.C3d8, ElemKind.C3d4):
+            return Pending(InvalidModel(
+                "gravity on solid elements unsupported (plane and beam only)"))
+        else:
+            continue
+        for i, w in zip(idx, per):
+            f[i * ndof] += w * dir2[0]
+            f[i * ndof + 1] += w * dir2[1]
+    return None
+
+
 def resolve(model: Model):
     """Reference-shaped model -> (FlatModel, pending error or None).
 
     Raises the SolveError the reference raises before assembly.
     """
-    bcs, cloads, _dl, _g = model.load_state()
+    bcs, cloads, dloads, gravity = model.load_state()
     mesh = model.mesh
     if len(bcs) == 0:
         raise NoConstraints("no constraints")
@@ -210,6 +296,10 @@ def resolve(model: Model):
             pending = Pending(InvalidModel(f"load on unknown node {cl.node_id}"))
             break
         f[idx * ndof + cl.dof - 1] += cl.value
+    if pending is None:
+        pending = _edge_pressure(model, dloads, first_index, ndof, f)
+    if pending is None:
+        pending = _gravity(model, gravity, first_index, ndof, f)
     rows = []
     if pending is None:
         # constrained_dofs (solver.rs:15-41)

@@ -6,15 +6,15 @@ recovery run as hand-written sm_100a CUDA kernels in ``libsolvix_b200.so``,
 reached through the C ABI declared in ``include/solvix_gpu.h``.  This package
 mirrors solvix-core's data model and ``solve`` entry points on top of it.
 """
-from .model import (BoundaryCondition, ConcentratedLoad, DeviceError, ElemKind, Element,
-                    ElementSet, EmptyMesh, InvalidModel, Material, Mesh, Method, Model, Node,
+from .model import (BoundaryCondition, ConcentratedLoad, DeviceError, DistributedLoad,
+                    ElemKind, Element, ElementSet, EmptyMesh, InvalidModel, Material, Mesh, Method, Model, Node,
                     NoConstraints, NotConverged, Reaction, SolveError, Solution, Step)
 from .marshal import FlatModel
 from .core import Context, Operator, default_context, solve, solve_with_method
 from . import abi
 
 __all__ = [
-    "BoundaryCondition", "ConcentratedLoad", "DeviceError", "ElemKind", "Element", "ElementSet",
+    "BoundaryCondition", "ConcentratedLoad", "DeviceError", "DistributedLoad", "ElemKind", "Element", "ElementSet",
     "EmptyMesh", "InvalidModel", "Material", "Mesh", "Method", "Model", "Node", "NoConstraints",
     "NotConverged", "Reaction", "SolveError", "Solution", "Step", "FlatModel", "Context",
     "Operator", "default_context", "solve", "solve_with_method", "abi",

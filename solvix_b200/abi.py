@@ -94,6 +94,14 @@ class SvxModelDesc(C.Structure):
         ("cload_node_ids", c_uint32_p),
         ("cload_dofs", c_int64_p),
         ("cload_values", c_double_p),
+        ("density", C.c_double),
+        ("n_dloads", C.c_int64),
+        ("dload_elem_ids", c_uint32_p),
+        ("dload_faces", c_int64_p),
+        ("dload_values", c_double_p),
+        ("has_gravity", C.c_int32),
+        ("gravity_magnitude", C.c_double),
+        ("gravity_dir", C.c_double * 3),
     ]
 
 

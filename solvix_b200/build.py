@@ -32,7 +32,10 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # units whose arithmetic must round like the reference (no fused multiply-add)
 NO_FMA = {"svx_element.cu"}
 CXX = os.environ.get("CXX", "g++")
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CSRC}",
+# host arithmetic that restates the reference's (load vectors) must round
+# operation by operation: Rust never fuses a*b+c
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
+             f"-I{INCLUDE}", f"-I{CSRC}",
              f"-I{os.path.join(CUDA_HOME, 'include')}"]
 
 

@@ -168,10 +168,6 @@ class Context:
                     inner_tol: float = 1e-5, method: int = abi.SVX_METHOD_AUTO) -> Solution:
         """The reference-shaped path: resolve ids / sets on the host (C++),
         then assemble, solve and recover stresses on the device."""
-        _bcs, _cl, dloads, gravity = model.load_state()
-        if dloads or gravity:
-            raise InvalidModel("distributed loads and gravity are outside the linear-static "
-                               "GPU path (concentrated loads only)")
         desc, keep = model_desc(model)
         res = C.c_void_p()
         err = abi.SvxError()

@@ -867,6 +867,12 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
             const long long v = std::strtoll(e, &end, 10);
             if (end != e && v >= 0) ctx->graph_min_nnz = v;
         }
+        if (const char* e = std::getenv("SVX_PCG_SMEM")) ctx->pcg_smem = (e[0] != '0');
+        if (const char* e = std::getenv("SVX_PCG_ALG")) ctx->pcg_alg = (e[0] == '0') ? 0 : 1;
+        if (const char* e = std::getenv("SVX_PCG_UNROLL")) {
+            const long v = std::strtol(e, nullptr, 10);
+            if (v == 1 || v == 2 || v == 4) ctx->pcg_unroll = int(v);
+        }
         // the main stream (uploads, assembly, stress, plain solves) has the
         // highest priority; the long batched PCG kernels run on the lowest,
         // so a served lane's assembly gets SMs while another lane's batch

@@ -230,9 +230,22 @@ struct Cload {
     int64_t dof;
     double value;
 };
+struct Dload {
+    uint32_t elem;
+    int64_t face;
+    double magnitude;
+};
+
+struct Gravity {
+    double g;
+    double dir[3];
+};
+
 struct StepAcc {
     std::vector<Bc> bcs;
     std::vector<Cload> cloads;
+    std::vector<Dload> dloads;
+    std::optional<Gravity> gravity;
 };
 
 // parser.rs:176-185: the element types it knows, with their node counts
@@ -250,12 +263,11 @@ const KindInfo KINDS[] = {{"CPS4", SVX_CPS4, 4, "Cps4"}, {"CPS3", SVX_CPS3, 3, "
 
 // Keywords the reference gives a meaning outside the linear-static path.
 bool outside_subset(const std::string& k) {
-    static const char* names[] = {"density",     "plastic",      "conductivity",
-                                  "expansion",   "beam section", "surface",
-                                  "surface interaction", "friction", "contact pair",
-                                  "dload",       "temperature",  "dflux",
-                                  "cflux",       "heat transfer", "dynamic",
-                                  "damping"};
+    static const char* names[] = {"plastic",      "conductivity", "expansion",
+                                  "beam section", "surface",      "surface interaction",
+                                  "friction",     "contact pair", "temperature",
+                                  "dflux",        "cflux",        "heat transfer",
+                                  "dynamic",      "damping"};
     for (const char* n : names)
         if (k == n) return true;
     return false;
@@ -276,6 +288,7 @@ struct svx_inp {
     std::vector<std::vector<uint32_t>> elset_ids;
     std::vector<std::pair<std::string, std::string>> assign;
     double thickness = 1.0;
+    double density = 7850.0;  // Model::default (lib.rs:310-317)
     StepAcc state;  // Model::load_state
     int32_t n_steps = 0;
     std::vector<std::string> warnings;
@@ -284,8 +297,9 @@ struct svx_inp {
     std::vector<int64_t> elset_ptr;
     std::vector<uint32_t> elset_flat;
     std::vector<int64_t> bc_node_ptr, bc_dof_ptr, bc_dofs, cl_dofs;
-    std::vector<uint32_t> bc_nodes, cl_nodes;
-    std::vector<double> cl_values;
+    std::vector<uint32_t> bc_nodes, cl_nodes, dl_elems;
+    std::vector<double> cl_values, dl_values;
+    std::vector<int64_t> dl_faces;
     svx_model_desc_t desc{};
 
     void parse(std::string_view text);
@@ -296,8 +310,10 @@ void svx_inp::parse(std::string_view text) {
     const std::vector<Item> items = tokenize(text);
     std::unordered_map<std::string, std::vector<uint32_t>> nsets;
     std::unordered_map<std::string, size_t> elset_index;
-    std::unordered_map<uint32_t, char> node_seen, elem_seen;
+    std::unordered_map<uint32_t, char> node_seen;
+    std::unordered_map<uint32_t, int> elem_kind;  // element id -> kind
     std::optional<std::string> pending_material, cur_material;
+    bool density_seen = false;
     StepAcc model_data;
     std::vector<StepAcc> steps_done;
     std::optional<StepAcc> cur;
@@ -433,7 +449,7 @@ void svx_inp::parse(std::string_view text) {
                 std::vector<uint32_t> c;
                 for (size_t q = 1; q < g.size(); ++q)
                     c.push_back(num_u<uint32_t>(g[q], first, "node id"));
-                if (!elem_seen.emplace(id, 1).second)
+                if (!elem_kind.emplace(id, k->kind).second)
                     throw ParseFail{first, "duplicate element id " + std::to_string(id)};
                 if (setname) upsert_elset(*setname, &id, 1);
                 elem_ids.push_back(id);
@@ -514,6 +530,111 @@ void svx_inp::parse(std::string_view text) {
                 } else {
                     warn(L(d.line) +
                          "extra *ELASTIC row ignored (temperature dependence is v0.2)");
+                }
+            }
+        } else if (name == "density") {  // parser.rs:332-365
+            ++j;
+            bool first_row = true;
+            for (; j < items.size() && !items[j].kw; ++j) {
+                const Item& d = items[j];
+                const auto f = fields(d.text);
+                if (first_row) {
+                    if (!cur_material) {
+                        warn(L(d.line) + "*DENSITY outside *MATERIAL — ignored");
+                    } else if (f.empty()) {
+                        throw ParseFail{d.line, "*DENSITY expects a density value"};
+                    } else {
+                        const double v = num_f(f[0], d.line, "density");
+                        if (density_seen && density != v)
+                            warn(L(d.line) + "*DENSITY overwrites an earlier value "
+                                             "(per-material density is v0.4)");
+                        density = v;
+                        density_seen = true;
+                        if (f.size() > 1)
+                            warn(L(d.line) + "extra *DENSITY fields ignored (temperature "
+                                             "dependence is v0.2)");
+                    }
+                    first_row = false;
+                } else {
+                    warn(L(d.line) +
+                         "extra *DENSITY row ignored (temperature dependence is v0.2)");
+                }
+            }
+        } else if (name == "dload") {  // parser.rs:846-950
+            const bool op_new = op_is_new(kw);
+            if (!cur) {
+                warn(L(kw.line) +
+                     "*DLOAD outside *STEP — ignored (distributed loads live in steps)");
+                ++j;
+                skip_data();
+                continue;
+            }
+            if (op_new) {
+                cur->dloads.clear();
+                cur->gravity.reset();
+            }
+            ++j;
+            for (; j < items.size() && !items[j].kw; ++j) {
+                const Item& d = items[j];
+                const auto f = fields(d.text);
+                if (!f.empty() && lower(f[0]) == "grav") {
+                    if (f.size() < 3 || f.size() > 5)
+                        throw ParseFail{d.line, "*DLOAD GRAV expects GRAV, magnitude, dir1[, "
+                                                "dir2][, dir3]; got " +
+                                                    std::to_string(f.size()) + " field(s)"};
+                    Gravity gr{};
+                    gr.g = num_f(f[1], d.line, "gravity magnitude");
+                    gr.dir[0] = num_f(f[2], d.line, "gravity direction");
+                    gr.dir[1] = f.size() > 3 ? num_f(f[3], d.line, "gravity direction") : 0.0;
+                    gr.dir[2] = f.size() > 4 ? num_f(f[4], d.line, "gravity direction") : 0.0;
+                    cur->gravity = gr;
+                    continue;
+                }
+                if (f.size() != 3)
+                    throw ParseFail{d.line,
+                                    "*DLOAD expects element/elset, P1..P4, magnitude; got " +
+                                        std::to_string(f.size()) + " field(s)"};
+                const std::string ltype = upper(f[1]);
+                std::optional<uint64_t> face;
+                if (!ltype.empty() && ltype[0] == 'P')
+                    face = parse_unsigned<uint64_t>(std::string_view(ltype).substr(1));
+                if (!face || *face < 1 || *face > 4) {
+                    warn(L(d.line) + "*DLOAD type '" + ltype +
+                         "' unsupported (v0.3: P1|P2|P3|P4, GRAV) — line ignored");
+                    continue;
+                }
+                const double magnitude = num_f(f[2], d.line, "pressure magnitude");
+                // parser.rs:1450-1457: an element set first, then a bare id
+                std::vector<uint32_t> ids;
+                const auto es = elset_index.find(upper(f[0]));
+                if (es != elset_index.end()) {
+                    ids = elset_ids[es->second];
+                } else if (const auto id = parse_unsigned<uint32_t>(f[0])) {
+                    ids.push_back(*id);
+                } else {
+                    warn(L(d.line) + "*DLOAD target '" + std::string(f[0]) +
+                         "' is not a known element or ELSET — line ignored");
+                    continue;
+                }
+                for (const uint32_t id : ids) {
+                    const auto ek = elem_kind.find(id);
+                    if (ek == elem_kind.end()) {
+                        warn(L(d.line) + "*DLOAD on unknown element " + std::to_string(id) +
+                             " — ignored");
+                        continue;
+                    }
+                    const int kind = ek->second;
+                    const uint64_t faces =
+                        kind == SVX_CPS3 ? 3 : ((kind == SVX_CPS4 || kind == SVX_CPE4) ? 4 : 0);
+                    if (*face > faces) {
+                        std::string kn;
+                        for (const auto& ki : KINDS)
+                            if (ki.kind == kind) kn = lower(ki.type);
+                        warn(L(d.line) + "element " + std::to_string(id) + " (" + kn +
+                             ") has no face " + std::to_string(*face) + " — ignored");
+                        continue;
+                    }
+                    cur->dloads.push_back(Dload{id, int64_t(*face), magnitude});
                 }
             }
         } else if (name == "solid section") {  // parser.rs:537-584
@@ -680,6 +801,11 @@ void svx_inp::finish() {
         cl_dofs.push_back(c.dof);
         cl_values.push_back(c.value);
     }
+    for (const auto& dl : state.dloads) {
+        dl_elems.push_back(dl.elem);
+        dl_faces.push_back(dl.face);
+        dl_values.push_back(dl.magnitude);
+    }
     svx_model_desc_t& d = desc;
     d.n_nodes = int64_t(node_ids.size());
     d.node_ids = node_ids.data();
@@ -710,6 +836,16 @@ void svx_inp::finish() {
     d.cload_node_ids = cl_nodes.data();
     d.cload_dofs = cl_dofs.data();
     d.cload_values = cl_values.data();
+    d.density = density;
+    d.n_dloads = int64_t(dl_elems.size());
+    d.dload_elem_ids = dl_elems.data();
+    d.dload_faces = dl_faces.data();
+    d.dload_values = dl_values.data();
+    d.has_gravity = state.gravity ? 1 : 0;
+    if (state.gravity) {
+        d.gravity_magnitude = state.gravity->g;
+        for (int k = 0; k < 3; ++k) d.gravity_dir[k] = state.gravity->dir[k];
+    }
 }
 
 namespace {

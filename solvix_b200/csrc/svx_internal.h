@@ -181,6 +181,17 @@ struct svx_ctx {
     // build's default); SVX_GRAPH_MIN_NNZ in the environment at
     // svx_ctx_create overrides it
     long long graph_min_nnz = -1;
+    // plain FP64 solves below the graph threshold run the shared-memory
+    // persistent kernel (1) or the register-vector one (0); SVX_PCG_SMEM in
+    // the environment at svx_ctx_create overrides it
+    int pcg_smem = 1;
+    // the shared-memory kernel's form (-1: by size; 1 = two grid barriers an
+    // iteration, neighbours forming p from z and the previous p; 0 = three,
+    // p stored); SVX_PCG_ALG in the environment at svx_ctx_create sets it
+    int pcg_alg = -1;
+    // its nodes per warp step with all loads in flight (0: 4);
+    // SVX_PCG_UNROLL sets it
+    int pcg_unroll = 0;
 };
 
 namespace svx {

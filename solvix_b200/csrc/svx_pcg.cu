@@ -616,7 +616,7 @@ constexpr long long SHARED_ADJ_MAX = SVX_SHARED_ADJ_MAX;
 // One node's rows given its d column node indices (cols: global memory,
 // read through the read-only path, or shared memory when SCOLS) and its
 // row block v.
-template <int ND, int G, class M, class V, bool SCOLS>
+template <int ND, int G, class M, class V, bool SCOLS, int UNROLL = 2>
 __device__ __forceinline__ void node_rows_cg_at(const int32_t* cols, int d,
                                                 const M* __restrict__ v, const V* x, int64_t i,
                                                 int gl, double* acc) {
@@ -634,7 +634,7 @@ __device__ __forceinline__ void node_rows_cg_at(const int32_t* cols, int d,
 #pragma unroll
         for (int db = 0; db < ND; ++db) xi[db] = double(__ldcg(x + i * ND + db));
     }
-#pragma unroll 2
+#pragma unroll UNROLL
     for (int k = gl; k < d; k += G) {
         const int32_t j = SCOLS ? cols[k] : __ldg(cols + k);
         const int64_t c = int64_t(j) * ND;
@@ -736,12 +736,13 @@ struct SharedAdj {
     const int32_t* cols;
 };
 
-__device__ __forceinline__ SharedAdj load_shared_adj(const int64_t* __restrict__ adj_ptr,
-                                                     const int32_t* __restrict__ adj,
-                                                     const int64_t* __restrict__ node_base,
-                                                     int64_t nb0, int64_t nb1, int nodes_cap) {
-    extern __shared__ __align__(16) unsigned char svx_dyn_smem[];
-    int64_t* vb = reinterpret_cast<int64_t*>(svx_dyn_smem);
+__device__ __forceinline__ SharedAdj load_shared_adj_at(unsigned char* base,
+                                                        const int64_t* __restrict__ adj_ptr,
+                                                        const int32_t* __restrict__ adj,
+                                                        const int64_t* __restrict__ node_base,
+                                                        int64_t nb0, int64_t nb1,
+                                                        int nodes_cap) {
+    int64_t* vb = reinterpret_cast<int64_t*>(base);
     int32_t* ap = reinterpret_cast<int32_t*>(vb + nodes_cap);
     int32_t* cl = ap + nodes_cap + 1;
     const int nloc = int(nb1 - nb0);
@@ -753,6 +754,14 @@ __device__ __forceinline__ SharedAdj load_shared_adj(const int64_t* __restrict__
     for (int64_t t = threadIdx.x; t < cnt; t += blockDim.x) cl[t] = adj[a_start + t];
     __syncthreads();
     return SharedAdj{vb, ap, cl};
+}
+
+__device__ __forceinline__ SharedAdj load_shared_adj(const int64_t* __restrict__ adj_ptr,
+                                                     const int32_t* __restrict__ adj,
+                                                     const int64_t* __restrict__ node_base,
+                                                     int64_t nb0, int64_t nb1, int nodes_cap) {
+    extern __shared__ __align__(16) unsigned char svx_dyn_smem[];
+    return load_shared_adj_at(svx_dyn_smem, adj_ptr, adj, node_base, nb0, nb1, nodes_cap);
 }
 
 size_t shared_adj_bytes(int64_t nodes_cap, int max_deg) {
@@ -1085,6 +1094,342 @@ pcg_persistent2_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         s->rz = rz;
         s->beta = beta;
     }
+}
+
+// ------------------------------------------------------------ shared-memory persistent PCG
+// The plain FP64 solve below GRAPH_MIN_NNZ (pcg_fp64).
+// A block owns the nodes [n_nodes*b/B, n_nodes*(b+1)/B) and their rows for a
+// whole launch.  Its adjacency (row-block offsets, column prefix, column
+// node indices) and its rows of u, r, p, q, z and 1/K_ii live in dynamic
+// shared memory across the launch; what neighbouring blocks gather goes to
+// global memory every iteration, u, r and p at the end of the launch.  Each
+// warp computes q = K p for a contiguous run of the block's nodes (G lanes
+// per node, partial sums combined by shuffles within the lane group) and
+// writes the node's rows of q to shared memory; the vector updates run over
+// the block's rows, one thread per row.  The recurrence is solver.rs:82-149
+// exactly (q = K p, alpha = r.z / p.q, u += alpha p, r -= alpha q, z = r /
+// K_ii, beta = r.z' / r.z, p = z + beta p), so the iterates round like the
+// reference's but for the order of the dot-product sums.  Two forms:
+//  * ALG 0: p is stored for the neighbours after its update, so an
+//    iteration has three grid barriers (p stored; p.q; r.r and r.z);
+//  * ALG 1: the SpMV forms each gathered p_j = z_j + beta p_prev_j itself
+//    from z (stored with the r update) and the previous p (a second buffer,
+//    alternating between iterations), so the barrier after the p update
+//    goes away: two grid barriers, two gathered vectors.  Every block forms
+//    p_j with the same fused multiply-add, so a row's p is bitwise the same
+//    in its owner and in every neighbour.
+// Reductions are in a fixed order (warp shuffles, shared memory, then every
+// block sums the block partials in index order), so repeated runs are
+// bitwise identical.
+
+// Sums a, b over the block; every thread gets the totals.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    __syncthreads();
+    if (lane == 0) {
+        sh[w] = a;
+        sh[32 + w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        double ta = lane < nw ? sh[lane] : 0.0;
+        double tb = lane < nw ? sh[32 + lane] : 0.0;
+        ta = warp_sum(ta);
+        tb = warp_sum(tb);
+        if (lane == 0) {
+            sh[0] = ta;
+            sh[32] = tb;
+        }
+    }
+    __syncthreads();
+    a = sh[0];
+    b = sh[32];
+}
+
+// Dynamic shared memory of pcg_smem_kernel for `nodes_cap` nodes of `nd`
+// dofs and at most max_deg neighbours: six vectors of nodes_cap * nd
+// doubles, then the adjacency in load_shared_adj's layout.
+size_t smem_pcg_bytes(int64_t nodes_cap, int nd, int max_deg) {
+    return size_t(nodes_cap) * size_t(nd) * 8 * 6 + shared_adj_bytes(nodes_cap, max_deg);
+}
+
+// One node's rows for the two-barrier form: x_j = z_j + beta * pprev_j.
+template <int ND, int G>
+__device__ __forceinline__ void node_rows_zp(const int32_t* cols, int d, const double* v,
+                                             const double* z, const double* pprev, double beta,
+                                             int64_t i, int gl, double* acc) {
+    if (d == 0) {
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da)
+                acc[da] = v[da] * __fma_rn(beta, __ldcg(pprev + i * ND + da),
+                                           __ldcg(z + i * ND + da));
+        return;
+    }
+    const int rowlen = ND * d;
+    for (int k = gl; k < d; k += G) {
+        const int64_t c = int64_t(cols[k]) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db)
+            xv[db] = __fma_rn(beta, __ldcg(pprev + c + db), __ldcg(z + c + db));
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                acc[da] += __ldg(v + da * rowlen + k * ND + db) * xv[db];
+    }
+}
+
+// The gathered value of column c: p_c itself (ALG 0) or z_c + beta pprev_c
+// formed with one fused multiply-add (ALG 1).
+template <int ALG>
+__device__ __forceinline__ double gathered(const double* x, const double* z, const double* pprev,
+                                           double beta, int64_t c) {
+    if constexpr (ALG == 0) return __ldcg(x + c);
+    return __fma_rn(beta, __ldcg(pprev + c), __ldcg(z + c));
+}
+
+// One node's rows, lane gl of its G-lane group taking neighbour blocks gl,
+// gl + G, ...  The first block is loaded under a predicate rather than a
+// branch, so that the U nodes of a warp step issue all their loads before
+// their first multiply-add; nodes with more than G neighbour blocks (none
+// in a C3D8 or CPS4 mesh at G = 32 / 16) loop over the rest.
+template <int ND, int G, int ALG>
+__device__ __forceinline__ void node_rows_pred(bool valid, const int32_t* cols, int d,
+                                               const double* v, const double* x,
+                                               const double* z, const double* pprev,
+                                               double beta, int64_t i, int gl, double* acc) {
+    const int rowlen = ND * d;
+    const bool act = valid && gl < d;
+    const int64_t c0 = int64_t(act ? cols[gl] : 0) * ND;
+    double xv[ND];
+#pragma unroll
+    for (int db = 0; db < ND; ++db) xv[db] = act ? gathered<ALG>(x, z, pprev, beta, c0 + db) : 0.0;
+#pragma unroll
+    for (int da = 0; da < ND; ++da)
+#pragma unroll
+        for (int db = 0; db < ND; ++db)
+            acc[da] += (act ? __ldg(v + da * rowlen + gl * ND + db) : 0.0) * xv[db];
+    if (valid && d > G) {
+        for (int k = gl + G; k < d; k += G) {
+            const int64_t c = int64_t(cols[k]) * ND;
+#pragma unroll
+            for (int db = 0; db < ND; ++db) xv[db] = gathered<ALG>(x, z, pprev, beta, c + db);
+#pragma unroll
+            for (int da = 0; da < ND; ++da)
+#pragma unroll
+                for (int db = 0; db < ND; ++db)
+                    acc[da] += __ldg(v + da * rowlen + k * ND + db) * xv[db];
+        }
+    }
+    if (valid && d == 0 && gl == 0)  // an unreferenced node: rows of length 1
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+            acc[da] = v[da] * gathered<ALG>(x, z, pprev, beta, i * ND + da);
+}
+
+template <int ND, int G, int PB, int BPS, int ALG, int U>
+__global__ void __launch_bounds__(PB, BPS)
+pcg_smem_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                const int32_t* __restrict__ adj, const int64_t* __restrict__ node_base,
+                const double* __restrict__ vals, const double* __restrict__ inv_diag,
+                double* u_g, double* r_g, double* p_g, double* p2_g, double* z_g,
+                double* part, PcgScalars* s, GridBarrier* gb, int chunk, int nodes_cap,
+                int first) {
+    extern __shared__ __align__(16) unsigned char svx_dyn_smem[];
+    __shared__ double sh[64];
+    // block-uniform values kept out of registers: ||f||, tol, the last
+    // iterate's ||r|| / ||f|| and r.r (thread 0 keeps them), max_iter
+    __shared__ double s_c[4];
+    __shared__ long long s_max_iter;
+    constexpr int NPS = 32 / G;  // nodes per warp step
+    constexpr int W = PB / 32;
+    const unsigned int B = gridDim.x;
+    unsigned int bar_target = 0;
+    volatile PcgScalars* vs = s;
+    if (vs->status != PCG_RUNNING) return;
+    // nodes and rows fit in int32 (the CSR indices are int32)
+    const int nb0 = int(n_nodes * int64_t(blockIdx.x) / B);
+    const int nb1 = int(n_nodes * int64_t(blockIdx.x + 1) / B);
+    const int nloc = nb1 - nb0, rows = nloc * ND, row0 = nb0 * ND;
+    const int rcap = nodes_cap * ND;
+    double* u_s = reinterpret_cast<double*>(svx_dyn_smem);
+    double* r_s = u_s + rcap;
+    double* p_s = r_s + rcap;
+    double* q_s = p_s + rcap;
+    double* z_s = q_s + rcap;
+    double* d_s = z_s + rcap;
+    const SharedAdj sa = load_shared_adj_at(reinterpret_cast<unsigned char*>(d_s + rcap),
+                                            adj_ptr, adj, node_base, nb0, nb1, nodes_cap);
+    if (threadIdx.x == 0) {
+        s_c[0] = vs->bnorm;
+        s_c[1] = vs->tol;
+        s_c[2] = vs->res;
+        s_c[3] = vs->rr;
+        s_max_iter = vs->max_iter;
+    }
+    long long it = vs->it;
+    double rz = vs->rz, beta = vs->beta;
+    // ALG 1 alternates the previous-p buffers: iteration it reads p_{it-1}
+    // from buf(it) and writes p_it to buf(it + 1)
+    auto buf = [&](long long k) -> double* { return (k & 1) ? p2_g : p_g; };
+    for (int t = threadIdx.x; t < rows; t += PB) {
+        const int row = row0 + t;
+        const double di = inv_diag[row];
+        const double ri = r_g[row];
+        d_s[t] = di;
+        r_s[t] = ri;
+        z_s[t] = ri * di;
+        u_s[t] = u_g[row];
+        // the first launch starts from p = z (the init kernel's p); later
+        // launches from the stored direction
+        p_s[t] = ALG == 1 ? (first ? 0.0 : buf(it)[row]) : p_g[row];
+    }
+    if (ALG == 1 && first) beta = 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wn0 = nb0 + nloc * warp / W, wn1 = nb0 + nloc * (warp + 1) / W;
+    const int gl = lane & (G - 1), grp = lane / G;
+    const bool writer = (blockIdx.x == 0 && threadIdx.x == 0);
+    __syncthreads();
+    if (ALG == 1 && first) {
+        // neighbours gather z and the previous p (zero): store z, barrier
+        for (int t = threadIdx.x; t < rows; t += PB) {
+            z_g[row0 + t] = z_s[t];
+            p_g[row0 + t] = 0.0;
+        }
+        if (!grid_sync(gb, B, bar_target)) return;
+    }
+
+    // sum over the grid of the block partials (a, b) written at `part`
+    auto grid_totals = [&](double a, double b, double& ta, double& tb) -> bool {
+        block_sum2(a, b, sh);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = a;
+            part[2 * blockIdx.x + 1] = b;
+        }
+        if (!grid_sync(gb, B, bar_target)) return false;
+        double x = 0.0, y = 0.0;
+        for (int k = threadIdx.x; k < int(B); k += PB) {
+            x += __ldcg(part + 2 * k);
+            y += __ldcg(part + 2 * k + 1);
+        }
+        block_sum2(x, y, sh);
+        ta = x;
+        tb = y;
+        return true;
+    };
+    auto finish = [&](int status) {
+        for (int t = threadIdx.x; t < rows; t += PB) {
+            const int row = row0 + t;
+            u_g[row] = u_s[t];
+            r_g[row] = r_s[t];
+            if (ALG == 0) p_g[row] = p_s[t];
+        }
+        if (writer) {
+            s->it = it;
+            s->res = s_c[2];
+            s->rr = s_c[3];
+            s->rz = rz;
+            s->beta = beta;
+            __threadfence();
+            if (status != PCG_RUNNING) s->status = status;
+        }
+    };
+
+    for (int c = 0; c < chunk; ++c) {
+        // q = K p on the block's nodes, p.q on its rows
+        const double* pprev = buf(it);
+        double* pnext = buf(it + 1);
+        if (ALG == 0) {
+            for (int t = threadIdx.x; t < rows; t += PB) p_g[row0 + t] = p_s[t];
+            if (!grid_sync(gb, B, bar_target)) return;
+        } else {
+            for (int t = threadIdx.x; t < rows; t += PB) {
+                const double pi = __fma_rn(beta, p_s[t], z_s[t]);
+                p_s[t] = pi;
+                pnext[row0 + t] = pi;
+            }
+        }
+        // U steps of the warp's nodes at a time, all their loads in flight
+        const int steps = (wn1 - wn0 + NPS - 1) / NPS;
+        for (int k = 0; k < steps; k += U) {
+            double acc[U][ND];
+#pragma unroll
+            for (int uu = 0; uu < U; ++uu) {
+                const int i = wn0 + (k + uu) * NPS + grp;
+                const bool valid = i < wn1;
+                const int li = valid ? i - nb0 : 0;
+                const int a0 = sa.aptr[li];
+                const int d = valid ? sa.aptr[li + 1] - a0 : 0;
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[uu][da] = 0.0;
+                const int64_t vb = valid ? sa.vbase[li] : 0;
+                node_rows_pred<ND, G, ALG>(valid, sa.cols + a0, d, vals + vb, p_g, z_g, pprev,
+                                           beta, i, gl, acc[uu]);
+            }
+#pragma unroll
+            for (int uu = 0; uu < U; ++uu)
+#pragma unroll
+                for (int da = 0; da < ND; ++da) acc[uu][da] = group_sum<G>(acc[uu][da]);
+#pragma unroll
+            for (int uu = 0; uu < U; ++uu) {
+                const int i = wn0 + (k + uu) * NPS + grp;
+                if (i < wn1 && gl < ND) {
+                    double qi = acc[uu][0];
+#pragma unroll
+                    for (int da = 1; da < ND; ++da)
+                        if (gl == da) qi = acc[uu][da];
+                    q_s[(i - nb0) * ND + gl] = qi;
+                }
+            }
+        }
+        __syncthreads();
+        double pq = 0.0, zero = 0.0;
+        for (int t = threadIdx.x; t < rows; t += PB) pq += p_s[t] * q_s[t];
+        double pap, unused;
+        if (!grid_totals(pq, zero, pap, unused)) return;
+        if (!(pap > 0.0)) {  // p.Kp <= 0 or NaN: breakdown
+            it += 1;
+            if (writer) s->pap = pap;
+            finish(PCG_BREAKDOWN);
+            return;
+        }
+        const double alpha = rz / pap;
+        // u += alpha p, r -= alpha q, z = r / K_ii; r.r, r.z
+        double lrr = 0.0, lrz = 0.0;
+        for (int t = threadIdx.x; t < rows; t += PB) {
+            u_s[t] += alpha * p_s[t];
+            const double ri = r_s[t] - alpha * q_s[t];
+            const double zi = ri * d_s[t];
+            r_s[t] = ri;
+            z_s[t] = zi;
+            if (ALG == 1) z_g[row0 + t] = zi;
+            lrr += ri * ri;
+            lrz += ri * zi;
+        }
+        double rr, rz_new;
+        if (!grid_totals(lrr, lrz, rr, rz_new)) return;
+        it += 1;
+        const double res = sqrt(rr) / s_c[0];
+        if (threadIdx.x == 0) {
+            s_c[2] = res;
+            s_c[3] = rr;
+        }
+        if (res <= s_c[1] || it >= s_max_iter) {
+            if (ALG == 1) beta = rz_new / rz;  // the next p of a resumed solve
+            rz = rz_new;
+            finish(res <= s_c[1] ? PCG_CONVERGED : PCG_MAXITER);
+            return;
+        }
+        beta = rz_new / rz;
+        rz = rz_new;
+        if (ALG == 0)
+            for (int t = threadIdx.x; t < rows; t += PB) p_s[t] = z_s[t] + beta * p_s[t];
+    }
+    finish(PCG_RUNNING);
 }
 
 
@@ -1849,6 +2194,119 @@ struct PcgRun {
         return status;
     }
 
+    // Shared-memory persistent form (pcg_smem_kernel, plain FP64 only):
+    // cooperative launches of up to `chunk` iterations each until the
+    // device status leaves RUNNING.  Returns -1 without launching when a
+    // block's rows and adjacency do not fit its shared memory (the caller
+    // then runs the register-vector persistent kernel).
+    int iterate_smem(int chunk) {
+        if constexpr (!(std::is_same<M, double>::value && std::is_same<V, double>::value &&
+                        std::is_same<U, double>::value)) {
+            (void)chunk;
+            return -1;
+        } else {
+            cudaStream_t st = ctx->stream;
+            const int ND = op->ndof;
+            const bool narrow = op->pat.max_deg <= 8;
+            const int G = ND == 3 ? (narrow ? 8 : 32) : (narrow ? 8 : 16);
+            int coop = 0;
+            SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+            if (!coop) return -1;
+            // one block of 512 threads per SM: fewer arrivals per grid barrier
+            // measured faster than 1,024-thread or two-block shapes.  The
+            // two-barrier form (ALG 1) gathers two vectors per neighbour
+            // value: it wins for 2D and small 3D systems (the C1 cantilever
+            // 7.56 -> 6.24 us an iteration) and loses at the 160x16x16 C3D8
+            // size (25.7 -> 28.6 us); SVX_PCG_ALG and SVX_PCG_UNROLL
+            // override the choice for measurements.
+            constexpr int PB = 512;
+            const unsigned int B = unsigned(ctx->sm_count);
+            const int nodes_cap = int((op->n_nodes + B - 1) / B);
+            const int alg =
+                ctx->pcg_alg >= 0 ? ctx->pcg_alg : ((ND <= 2 || nodes_cap <= 64) ? 1 : 0);
+            const int unroll = ctx->pcg_unroll > 0 ? ctx->pcg_unroll : 4;
+            auto kernel_for = [&]() -> void* {
+#define SVX_SMEM_PICK(ND_, G_)                                                           \
+    if (ND == ND_ && G == G_) {                                                          \
+        if (alg == 0) {                                                                  \
+            if (unroll == 1) return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 0, 1>;        \
+            if (unroll == 2) return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 0, 2>;        \
+            return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 0, 4>;                         \
+        }                                                                                \
+        if (unroll == 1) return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 1, 1>;            \
+        if (unroll == 2) return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 1, 2>;            \
+        return (void*)pcg_smem_kernel<ND_, G_, PB, 1, 1, 4>;                             \
+    }
+                SVX_SMEM_PICK(3, 32)
+                SVX_SMEM_PICK(3, 8)
+                SVX_SMEM_PICK(2, 16)
+                SVX_SMEM_PICK(2, 8)
+                SVX_SMEM_PICK(1, 16)
+                SVX_SMEM_PICK(1, 8)
+#undef SVX_SMEM_PICK
+                return nullptr;
+            };
+            int max_smem = 0;
+            SVX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                            ctx->device));
+            const size_t smem = smem_pcg_bytes(nodes_cap, ND, op->pat.max_deg);
+            if (smem > size_t(max_smem)) return -1;
+            void* fn = kernel_for();
+            if (!fn) return -1;
+            SVX_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(smem)));
+            int bps = 0;
+            SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, PB, smem));
+            if (bps < 1) return -1;
+            const int pb = PB;
+            if (!fn) return -1;
+            DBuf<double> part, z;
+            DBuf<GridBarrier> gb;
+            part.alloc(ctx->pool, 2 * size_t(B) + 2);
+            z.alloc(ctx->pool, n + 1);
+            gb.alloc(ctx->pool, 1);
+            SVX_CUDA(cudaMemsetAsync(gb.p, 0, sizeof(GridBarrier), st));
+            int64_t n_nodes = op->n_nodes;
+            const int64_t* a_ptr = op->pat.adj_ptr.p;
+            const int32_t* a_idx = op->pat.adj.p;
+            const int64_t* nbase = op->pat.node_base.p;
+            GridBarrier* gbp = gb.p;
+            double* pp = part.p;
+            double* zp = z.p;
+            int first = 1;
+            if (!p2) return -1;
+            void* args[] = {&n_nodes, (void*)&a_ptr, (void*)&a_idx, (void*)&nbase,
+                            (void*)&vals, (void*)&inv_diag, (void*)&u, (void*)&r, (void*)&p,
+                            (void*)&p2, (void*)&zp, (void*)&pp, (void*)&s, (void*)&gbp,
+                            (void*)&chunk, (void*)&nodes_cap, (void*)&first};
+            SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+            SVX_CUDA(cudaStreamSynchronize(st));
+            const long long launches_max = h_s->max_iter / chunk + 2;
+            GridBarrier hgb{};
+            int status = h_s->status;
+            for (long long launch = 0; status == PCG_RUNNING; ++launch) {
+                if (launch >= launches_max)
+                    throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                    "PCG status did not leave RUNNING within max_iter"};
+                SVX_CUDA(cudaMemsetAsync(&gbp->count, 0, sizeof(unsigned int), st));
+                SVX_CUDA(cudaLaunchCooperativeKernel(fn, dim3(B), dim3(pb), args, smem, st));
+                g_launches.fetch_add(1, std::memory_order_relaxed);
+                first = 0;
+                SVX_CUDA(cudaMemcpyAsync(h_s, s, sizeof(PcgScalars), cudaMemcpyDeviceToHost,
+                                         st));
+                SVX_CUDA(cudaMemcpyAsync(&hgb, gbp, sizeof(GridBarrier), cudaMemcpyDeviceToHost,
+                                         st));
+                SVX_CUDA(cudaStreamSynchronize(st));
+                if (hgb.error)
+                    throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                                    "persistent PCG: a grid barrier wait ran out (blocks not "
+                                    "co-resident)"};
+                status = h_s->status;
+            }
+            return status;
+        }
+    }
+
     // Runs until the device status leaves RUNNING; returns the status.
     int iterate(int check_every) {
         cudaStream_t st = ctx->stream;
@@ -2075,7 +2533,9 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
     if (status == PCG_RUNNING) {
         // the graph form starts from the init kernel's p = z0 too: a
         // persistent launch that cannot start leaves p untouched
-        status = graph ? -1 : run.iterate_persistent(persistent_chunk(op->pat.nnz));
+        status = -1;
+        if (!graph && ctx->pcg_smem) status = run.iterate_smem(persistent_chunk(op->pat.nnz));
+        if (!graph && status < 0) status = run.iterate_persistent(persistent_chunk(op->pat.nnz));
         if (status < 0) status = run.iterate(check_every);
     }
     SVX_CUDA(cudaEventRecord(ctx->ev[1], st));

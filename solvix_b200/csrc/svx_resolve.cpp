@@ -10,11 +10,15 @@
 //   Model::material_for_element   lib.rs:357-367 (first assignment whose
 //                                 first-named elset holds the id decides)
 //   CLOAD loop of assemble_with   crates/solvix-core/src/assembly.rs:365-380
+//   edge_pressure_forces          assembly.rs:382, :393-452 (*DLOAD Pn)
+//   gravity_forces                assembly.rs:383, :458-539 (*DLOAD GRAV)
 //   constrained_dofs              crates/solvix-core/src/solver.rs:15-41
 // The reference's lookups are linear scans (O(N^2) over a mesh); the
-// results here are identical.  CLOAD and BC errors are raised by the
-// reference only after the element loop, so they are kept pending and
-// reported by svx_solve_resolved when no element fails first.
+// results here are identical.  CLOAD, DLOAD, gravity and BC errors are
+// raised by the reference only after the element loop (in that order), so
+// they are kept pending and reported by svx_solve_resolved when no element
+// fails first.  The load vector is summed in the reference's order with
+// its operation order (CLOADs, then pressures, then gravity per element).
 
 #include <cmath>
 #include <cstring>
@@ -63,10 +67,128 @@ void set_err(svx_error_t* err, int code, const std::string& msg) {
     std::snprintf(err->message, sizeof(err->message), "%s", msg.c_str());
 }
 
+// ElemKind's Debug names, as the reference's "{:?}" prints them.
+const char* kind_debug(int kind) {
+    static const char* names[8] = {"Cps3", "Cps4", "Cps8", "Cpe4", "Cpe8", "C3d8", "C3d4", "B31"};
+    return (kind >= 0 && kind < 8) ? names[kind] : "?";
+}
+
+void pend(svx_resolved* r, const std::string& msg) {
+    r->pending_code = SVX_INVALID_MODEL;
+    r->pending_msg = msg;
+}
+
+// edge_pressure_forces (assembly.rs:393-452): the total pressure *
+// thickness * edge length splits half and half over the edge's two end
+// nodes, along the inward normal of a counter-clockwise element.
+void edge_pressure(const svx_model_desc_t* d,
+                   const std::unordered_map<uint32_t, int32_t>& node_index, int ndof,
+                   svx_resolved* r) {
+    if (d->n_dloads <= 0) return;
+    std::unordered_map<uint32_t, int64_t> first_elem;  // the first element with an id
+    first_elem.reserve(size_t(d->n_elems) * 2);
+    for (int64_t e = 0; e < d->n_elems; ++e) first_elem.emplace(d->elem_ids[e], e);
+    for (int64_t k = 0; k < d->n_dloads; ++k) {
+        const uint32_t id = d->dload_elem_ids[k];
+        const auto it = first_elem.find(id);
+        if (it == first_elem.end()) {
+            pend(r, "distributed load on unknown element " + std::to_string(id));
+            return;
+        }
+        const int64_t e = it->second;
+        const int kind = d->elem_kinds[e];
+        int max_face = 0;
+        if (kind == SVX_CPS3) max_face = 3;
+        else if (kind == SVX_CPS4 || kind == SVX_CPE4) max_face = 4;
+        else {
+            pend(r, "edge pressure on element " + std::to_string(id) + " (" + kind_debug(kind) +
+                        ") unsupported (linear quad/tri edges only)");
+            return;
+        }
+        const int64_t face = d->dload_faces[k];
+        if (face <= 0 || face > max_face) {
+            pend(r, "element " + std::to_string(id) + " (" + kind_debug(kind) +
+                        ") has no face " + std::to_string(face));
+            return;
+        }
+        const int64_t c0 = d->elem_conn_ptr[e];
+        const int64_t nn = d->elem_conn_ptr[e + 1] - c0;
+        const int32_t ia = node_index.at(d->elem_conn[c0 + face - 1]);
+        const int32_t ib = node_index.at(d->elem_conn[c0 + face % nn]);
+        const double pax = d->node_coords[3 * int64_t(ia)], pay = d->node_coords[3 * int64_t(ia) + 1];
+        const double pbx = d->node_coords[3 * int64_t(ib)], pby = d->node_coords[3 * int64_t(ib) + 1];
+        const double dx = pbx - pax, dy = pby - pay;
+        const double len = std::sqrt(dx * dx + dy * dy);
+        if (len == 0.0) {
+            pend(r, "zero-length pressure edge on element " + std::to_string(id));
+            return;
+        }
+        const double nx = -dy / len, ny = dx / len;
+        const double fmag = d->dload_values[k] * d->thickness * len / 2.0;
+        for (const int32_t i : {ia, ib}) {
+            r->f[size_t(int64_t(i) * ndof)] += fmag * nx;
+            r->f[size_t(int64_t(i) * ndof + 1)] += fmag * ny;
+        }
+    }
+}
+
+// gravity_forces (assembly.rs:458-539) for the element kinds this path
+// assembles: rho * t * area * g lumped in equal thirds (CPS3) or quarters
+// (CPS4, CPE4) along the in-plane direction; solid elements are rejected
+// with the reference's text.  Kinds the element loop rejects anyway
+// (CPS8, CPE8, B31) add nothing here: their element error comes first.
+void gravity(const svx_model_desc_t* d, const std::unordered_map<uint32_t, int32_t>& node_index,
+             int ndof, svx_resolved* r) {
+    if (!d->has_gravity) return;
+    const double g = d->gravity_magnitude;
+    const double dir0 = d->gravity_dir[0], dir1 = d->gravity_dir[1];
+    if (dir0 == 0.0 && dir1 == 0.0) {
+        pend(r, "gravity direction has no in-plane component");
+        return;
+    }
+    for (int64_t e = 0; e < d->n_elems; ++e) {
+        const int kind = d->elem_kinds[e];
+        const int64_t c0 = d->elem_conn_ptr[e];
+        int32_t idx[4];
+        double px[4], py[4];
+        int nn = 0;
+        double per = 0.0;
+        if (kind == SVX_CPS3 || kind == SVX_CPS4 || kind == SVX_CPE4) {
+            nn = kind == SVX_CPS3 ? 3 : 4;
+            for (int q = 0; q < nn; ++q) {
+                idx[q] = node_index.at(d->elem_conn[c0 + q]);
+                px[q] = d->node_coords[3 * int64_t(idx[q])];
+                py[q] = d->node_coords[3 * int64_t(idx[q]) + 1];
+            }
+            if (nn == 3) {
+                const double cross =
+                    (px[1] - px[0]) * (py[2] - py[0]) - (py[1] - py[0]) * (px[2] - px[0]);
+                per = d->density * d->thickness * std::fabs(cross) / 2.0 * g / 3.0;
+            } else {
+                double shoelace = 0.0;
+                for (int q = 0; q < 4; ++q) {
+                    const int b = (q + 1) % 4;
+                    shoelace += px[q] * py[b] - px[b] * py[q];
+                }
+                per = d->density * d->thickness * std::fabs(shoelace) / 2.0 * g / 4.0;
+            }
+        } else if (kind == SVX_C3D8 || kind == SVX_C3D4) {
+            pend(r, "gravity on solid elements unsupported (plane and beam only)");
+            return;
+        } else {
+            continue;
+        }
+        for (int q = 0; q < nn; ++q) {
+            r->f[size_t(int64_t(idx[q]) * ndof)] += per * dir0;
+            r->f[size_t(int64_t(idx[q]) * ndof + 1)] += per * dir1;
+        }
+    }
+}
+
 svx_resolved* resolve(const svx_model_desc_t* d) {
     if (!d) throw Fail{SVX_BAD_ARGUMENT, "null model"};
     if (d->n_nodes < 0 || d->n_elems < 0 || d->n_materials < 0 || d->n_elsets < 0 ||
-        d->n_assignments < 0 || d->n_bcs < 0 || d->n_cloads < 0)
+        d->n_assignments < 0 || d->n_bcs < 0 || d->n_cloads < 0 || d->n_dloads < 0)
         throw Fail{SVX_BAD_ARGUMENT, "negative size"};
     // lib.rs:597-599: a free body is NoConstraints before anything else
     if (d->n_bcs == 0) throw Fail{SVX_NO_CONSTRAINTS, "no constraints"};
@@ -160,6 +282,8 @@ svx_resolved* resolve(const svx_model_desc_t* d) {
         }
         r->f[size_t(int64_t(it->second) * ndof + dof - 1)] += d->cload_values[c];
     }
+    if (r->pending_code == SVX_OK) edge_pressure(d, node_index, ndof, r.get());
+    if (r->pending_code == SVX_OK) gravity(d, node_index, ndof, r.get());
     // constrained_dofs (solver.rs:15-41)
     if (r->pending_code == SVX_OK) {
         for (int32_t b = 0; b < d->n_bcs && r->pending_code == SVX_OK; ++b) {

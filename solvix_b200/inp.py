@@ -11,8 +11,8 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from .model import (BoundaryCondition, ConcentratedLoad, ElemKind, Element, ElementSet,
-                    Material, Mesh, Model, Node)
+from .model import (BoundaryCondition, ConcentratedLoad, DistributedLoad, ElemKind, Element,
+                    ElementSet, Material, Mesh, Model, Node, Step)
 
 
 class ParseError(Exception):
@@ -72,9 +72,18 @@ def parse_inp(text: str):
                for b in range(int(d.n_bcs))]
         cloads = [ConcentratedLoad(int(d.cload_node_ids[k]), int(d.cload_dofs[k]),
                                    float(d.cload_values[k])) for k in range(int(d.n_cloads))]
-        model = Model(mesh=Mesh(nodes, elems), thickness=float(d.thickness), materials=mats,
-                      elsets=sets, mat_assignments=assign, boundary_conditions=bcs,
-                      cloads=cloads)
+        dloads = [DistributedLoad(int(d.dload_elem_ids[k]), int(d.dload_faces[k]),
+                                  float(d.dload_values[k])) for k in range(int(d.n_dloads))]
+        gravity = ((float(d.gravity_magnitude), tuple(float(v) for v in d.gravity_dir))
+                   if d.has_gravity else None)
+        model = Model(mesh=Mesh(nodes, elems), thickness=float(d.thickness),
+                      density=float(d.density), materials=mats, elsets=sets,
+                      mat_assignments=assign, boundary_conditions=bcs, cloads=cloads)
+        if dloads or gravity is not None:
+            # distributed loads and gravity live in steps (Model::load_state
+            # reads them only from the last step)
+            model.steps = [Step(boundary_conditions=bcs, cloads=cloads, dloads=dloads,
+                                gravity=gravity)]
         warnings = [lib.svx_inp_warning(h, i).decode()
                     for i in range(lib.svx_inp_warning_count(h))]
         steps = int(lib.svx_inp_step_count(h))

@@ -145,7 +145,7 @@ def model_desc(model: Model):
 
     Returns ``(desc, keepalive)``.
     """
-    bcs, cloads, _dloads, _gravity = model.load_state()
+    bcs, cloads, dloads, gravity = model.load_state()
     mesh = model.mesh
     keep = []
 
@@ -228,6 +228,22 @@ def model_desc(model: Model):
     d.cload_node_ids = abi.ptr(cn, C.c_uint32)
     d.cload_dofs = abi.ptr(cd, C.c_int64)
     d.cload_values = abi.ptr(cv, C.c_double)
+
+    d.density = float(model.density)
+    d.n_dloads = len(dloads)
+    de = np.array([x.element_id for x in dloads] or [0], dtype=np.uint32)
+    df = np.array([x.face for x in dloads] or [0], dtype=np.int64)
+    dv = np.array([x.magnitude for x in dloads] or [0.0], dtype=np.float64)
+    keep += [de, df, dv]
+    d.dload_elem_ids = abi.ptr(de, C.c_uint32)
+    d.dload_faces = abi.ptr(df, C.c_int64)
+    d.dload_values = abi.ptr(dv, C.c_double)
+    d.has_gravity = 1 if gravity is not None else 0
+    if gravity is not None:
+        g, direction = gravity
+        d.gravity_magnitude = float(g)
+        for k in range(3):
+            d.gravity_dir[k] = float(direction[k])
     return d, keep
 
 

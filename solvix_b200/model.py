@@ -138,6 +138,17 @@ class ConcentratedLoad:
 
 
 @dataclass
+class DistributedLoad:
+    """Edge pressure on a plane element (lib.rs:150-158): `face` is the
+    1-based Abaqus edge (P1..P4 on CPS4, P1..P3 on CPS3), edge n joining
+    local nodes n and n+1; positive magnitude acts into the element."""
+
+    element_id: int
+    face: int
+    magnitude: float
+
+
+@dataclass
 class Step:
     """One analysis step's accumulated state (lib.rs:309-330)."""
 
@@ -154,6 +165,7 @@ class Model:
 
     mesh: Mesh = field(default_factory=Mesh)
     thickness: float = 1.0
+    density: float = 7850.0
     materials: list = field(default_factory=list)
     elsets: list = field(default_factory=list)
     mat_assignments: list = field(default_factory=list)

@@ -12,10 +12,11 @@ import pytest
 from oracle import oracle
 from solvix_b200 import abi
 from solvix_b200.marshal import FlatModel, model_desc
-from solvix_b200.model import (BoundaryCondition, ConcentratedLoad, ElemKind, Element,
-                               ElementSet, InvalidModel, Material, Mesh, Model, Node,
-                               NoConstraints, SolveError)
-from svx_cases import cantilever_deck, hex_mesh, load_golden, patch_deck, quad_mesh, steel_model
+from solvix_b200.model import (BoundaryCondition, ConcentratedLoad, DistributedLoad, ElemKind,
+                               Element, ElementSet, InvalidModel, Material, Mesh, Model, Node,
+                               NoConstraints, SolveError, Step)
+from svx_cases import (cantilever_deck, hex_cantilever, hex_mesh, load_golden, patch_deck,
+                       quad_mesh, steel_model)
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -57,8 +58,10 @@ def test_no_device_is_a_loud_error():
     assert buf.value
 
 
-def product_resolve(model):
-    """svx_resolve -> (FlatModel, pending status, pending message)."""
+def product_resolve(model, pending=None):
+    """svx_resolve -> (FlatModel, status, message); the error raised after
+    the element loop, if any, goes into the `pending` list as
+    (code, message)."""
     lib = abi.load()
     desc, keep = model_desc(model)
     res = C.c_void_p()
@@ -68,6 +71,11 @@ def product_resolve(model):
         return None, st, err.message.decode()
     try:
         flat = FlatModel.from_struct(lib.svx_resolved_flat(res).contents)
+        if pending is not None:
+            perr = abi.SvxError()
+            code = lib.svx_resolved_pending(res, C.byref(perr))
+            if code != abi.SVX_OK:
+                pending.append((code, perr.message.decode()))
     finally:
         lib.svx_resolved_free(res)
     return flat, st, ""
@@ -211,10 +219,142 @@ def bc_bad_dof():
     return m
 
 
+def _pressure_model(kind_mix=True):
+    """A jittered 4 x 2 plate (thickness 0.02, density 2700) whose last quad
+    is split into two CPS3, with edge pressures on every kind of face and a
+    slanted gravity in its one step."""
+    mesh = quad_mesh(4, 2, 2.0, 1.0)
+    rng = np.random.default_rng(12)
+    nodes = [Node(n.id, (n.coords[0] + rng.uniform(-0.05, 0.05),
+                         n.coords[1] + rng.uniform(-0.05, 0.05), 0.0)) for n in mesh.nodes]
+    elems = list(mesh.elements)
+    if kind_mix:
+        last = elems.pop()
+        a, b, c, d = last.connectivity
+        elems += [Element(last.id, ElemKind.Cps3, [a, b, c]),
+                  Element(last.id + 1, ElemKind.Cps3, [a, c, d])]
+    m = steel_model(Mesh(nodes, elems), thickness=0.02)
+    m.density = 2700.0
+    bcs = [BoundaryCondition([1, 6, 11], [1, 2])]
+    m.steps = [Step(boundary_conditions=bcs, cloads=[ConcentratedLoad(15, 2, -300.0)],
+                    dloads=[DistributedLoad(4, 2, 2.5e5), DistributedLoad(1, 1, -1.0e5),
+                            DistributedLoad(8, 3, 7.0e4), DistributedLoad(9, 1, 3.3e4),
+                            DistributedLoad(4, 2, 1.5e4)],
+                    gravity=(9.81, (0.3, -1.0, 0.7)))]
+    return m
+
+
+def test_pressure_and_gravity_load_vector_bit_exact():
+    """edge_pressure_forces and gravity_forces (assembly.rs:382-539) after
+    the CLOADs, in the reference's order and operation order: the load
+    vector is bit-identical to the oracle's, and its resultant is the
+    pressures' and the weight's."""
+    m = _pressure_model()
+    fp, st, _ = product_resolve(m)
+    fo, pending, _ = oracle_resolve(m)
+    assert st == abi.SVX_OK and pending is None
+    assert_same_flat(fp, fo)
+    assert np.array_equal(fp.fixed_row, fo.fixed_row)
+    # the weight: rho * t * area * g along the in-plane direction
+    xy = np.array([n.coords[:2] for n in m.mesh.nodes])
+    area = 0.0
+    for e in m.mesh.elements:
+        p = xy[[i - 1 for i in e.connectivity]]
+        area += 0.5 * abs(np.dot(p[:, 0], np.roll(p[:, 1], -1)) -
+                          np.dot(np.roll(p[:, 0], -1), p[:, 1]))
+    weight = 2700.0 * 0.02 * area * 9.81
+    no_grav = _pressure_model()
+    no_grav.steps[0].gravity = None
+    fg, _, _ = product_resolve(no_grav)
+    diff = (fp.f - fg.f).reshape(-1, 2).sum(axis=0)
+    assert np.allclose(diff, [0.3 * weight, -1.0 * weight], rtol=1e-12)
+
+
+@_case
+def dload_unknown_element():
+    m = _pressure_model()
+    m.steps[0].dloads.append(DistributedLoad(99, 1, 1.0))
+    return m
+
+
+@_case
+def dload_no_face():
+    m = _pressure_model()
+    m.steps[0].dloads.append(DistributedLoad(8, 4, 1.0))  # a CPS3 has edges 1..3
+    return m
+
+
+@_case
+def dload_face_zero():
+    m = _pressure_model()
+    m.steps[0].dloads.insert(0, DistributedLoad(2, 0, 1.0))
+    return m
+
+
+@_case
+def dload_zero_length_edge():
+    m = _pressure_model(kind_mix=False)
+    first = m.mesh.elements[0]
+    a, b, c, _d = first.connectivity
+    m.mesh = Mesh(m.mesh.nodes, [Element(first.id, ElemKind.Cps4, [a, b, c, c])] +
+                  list(m.mesh.elements[1:]))
+    m.steps[0].dloads = [DistributedLoad(first.id, 3, 5.0)]
+    return m
+
+
+@_case
+def dload_on_a_solid():
+    m = hex_cantilever(2, 1, 1)
+    m.steps = [Step(boundary_conditions=m.boundary_conditions, cloads=m.cloads,
+                    dloads=[DistributedLoad(1, 1, 1.0)])]
+    return m
+
+
+@_case
+def gravity_out_of_plane():
+    m = _pressure_model()
+    m.steps[0].gravity = (9.81, (0.0, 0.0, -1.0))
+    return m
+
+
+@_case
+def gravity_on_a_solid():
+    m = hex_cantilever(2, 1, 1)
+    m.steps = [Step(boundary_conditions=m.boundary_conditions, cloads=m.cloads,
+                    gravity=(9.81, (0.0, -1.0, 0.0)))]
+    return m
+
+
+@_case
+def cload_error_before_dload_error():
+    m = _pressure_model()
+    m.steps[0].cloads.append(ConcentratedLoad(777, 1, 1.0))
+    m.steps[0].dloads.append(DistributedLoad(99, 1, 1.0))
+    return m
+
+
+@_case
+def dload_error_before_gravity_and_bc_errors():
+    m = _pressure_model()
+    m.steps[0].dloads.append(DistributedLoad(8, 4, 1.0))
+    m.steps[0].gravity = (9.81, (0.0, 0.0, 1.0))
+    m.steps[0].boundary_conditions.append(BoundaryCondition([888], [1]))
+    return m
+
+
+@_case
+def gravity_error_before_bc_error():
+    m = _pressure_model()
+    m.steps[0].gravity = (9.81, (0.0, 0.0, 1.0))
+    m.steps[0].boundary_conditions.append(BoundaryCondition([888], [1]))
+    return m
+
+
 @pytest.mark.parametrize("case", ERROR_CASES, ids=[f.__name__ for f in ERROR_CASES])
 def test_resolve_errors_match_oracle(case):
     model = case()
-    fp, st, msg = product_resolve(model)
+    pend = []
+    fp, st, msg = product_resolve(model, pend)
     fo, ost, omsg = oracle_resolve(model)
     if fo is None:  # raised before assembly
         assert st == ost and msg == omsg
@@ -222,8 +362,10 @@ def test_resolve_errors_match_oracle(case):
         assert st == abi.SVX_OK
         if ost is None:
             assert_same_flat(fp, fo)
+            assert pend == []
     if fo is not None and ost is not None:
-        # pending error: the oracle raises it after assembly
+        # pending error, raised by the reference after the element loop
+        assert pend == [(abi.SVX_INVALID_MODEL, str(ost.err))]
         with pytest.raises(InvalidModel) as ei:
             oracle.solve(model)
         assert str(ei.value) == str(ost.err)

@@ -80,12 +80,21 @@ def test_full_deck_parses_all_keywords():
     assert w[0].startswith("line 33: ")
 
 
+def test_full_deck_with_its_dload_block_outside_the_step():
+    # parser.rs:1554-1617 with its *DLOAD block, which sits before *STEP:
+    # skipped with a warning, then the prescribed-displacement warning
+    m, w, steps = parse_inp(DECK.format(dload="*DLOAD\nALLSIDES, P, 1.0\n"))
+    assert len(w) == 2 and steps == 1
+    assert w[0] == ("line 29: *DLOAD outside *STEP — ignored (distributed loads live in "
+                    "steps)")
+    assert "nonzero prescribed displacement" in w[1]
+    assert m.load_state()[2] == [] and m.load_state()[3] is None
+
+
 def test_keywords_outside_the_reader_send_the_deck_to_the_reference_parser():
-    with pytest.raises(UnsupportedDeck, match=r"line 29: \*DLOAD"):
-        parse_inp(DECK.format(dload="*DLOAD\nALLSIDES, P, 1.0\n"))
     with pytest.raises(UnsupportedDeck, match="NLGEOM"):
         parse_inp("*NODE\n1,0,0\n*STEP, NLGEOM=YES\n*STATIC\n*END STEP\n")
-    for kw in ("DENSITY", "DYNAMIC", "TEMPERATURE", "CONTACT PAIR", "BEAM SECTION"):
+    for kw in ("PLASTIC", "DYNAMIC", "TEMPERATURE", "CONTACT PAIR", "BEAM SECTION"):
         with pytest.raises(UnsupportedDeck):
             parse_inp(f"*NODE\n1,0,0\n*{kw}\n1.0\n")
 
@@ -184,6 +193,80 @@ def plate_deck(pre, steps):
             "4, 5, 6, 9, 8\n*NSET, NSET=BASE\n1, 2, 3\n*MATERIAL, NAME=STEEL\n"
             "*ELASTIC\n210.0E9, 0.3\n" + pre +
             "*SOLID SECTION, ELSET=ALL, MATERIAL=STEEL\n0.01\n" + steps)
+
+
+def test_dload_edges_grav_and_density_parse():
+    # parser.rs:1858-1898
+    m, w, steps = parse_inp(plate_deck("*DENSITY\n7850.,\n", (
+        "*STEP, NAME=PRESS\n*STATIC\n*DLOAD\nALL, P1, 1.5e6\n3, P3, 2.5e5\n"
+        "GRAV, 9.81, 0.0, -1.0\n*BOUNDARY\nBASE, 1, 2\n*END STEP\n")))
+    assert w == [] and steps == 1
+    assert m.density == 7850.0
+    bcs, _cl, dloads, gravity = m.load_state()
+    assert len(dloads) == 5  # ALL expands to the 4 quads, then element 3
+    assert [(d.element_id, d.face, d.magnitude) for d in dloads] == \
+        [(1, 1, 1.5e6), (2, 1, 1.5e6), (3, 1, 1.5e6), (4, 1, 1.5e6), (3, 3, 2.5e5)]
+    assert gravity == (9.81, (0.0, -1.0, 0.0))
+    assert [(b.node_ids, b.dofs) for b in bcs] == [([1, 2, 3], [1, 2])]
+
+
+def test_dload_unsupported_types_and_targets_warn():
+    # parser.rs:1900-1919
+    m, w, _ = parse_inp(plate_deck("", (
+        "*STEP\n*STATIC\n*DLOAD\nNOSUCHSET, P1, 1.0\nALL, P5, 2.0\nALL, TRVEC, 3.0\n"
+        "3, P4, 4.0\nALL, P3, 5.0\n*BOUNDARY\nBASE, 1, 2\n*END STEP\n")))
+    assert w == [
+        "line 26: *DLOAD target 'NOSUCHSET' is not a known element or ELSET — line ignored",
+        "line 27: *DLOAD type 'P5' unsupported (v0.3: P1|P2|P3|P4, GRAV) — line ignored",
+        "line 28: *DLOAD type 'TRVEC' unsupported (v0.3: P1|P2|P3|P4, GRAV) — line ignored",
+    ]
+    assert len(m.load_state()[2]) == 5
+
+
+def test_density_after_elastic_and_overwrite_warning():
+    # parser.rs:1921-1931
+    m, w, _ = parse_inp(plate_deck("*DENSITY\n2500.,\n", (
+        "*STEP\n*STATIC\n*BOUNDARY\nBASE, 1, 2\n*CLOAD\n9, 2, -1.0\n*END STEP\n")))
+    assert w == [] and m.density == 2500.0
+    assert [(x.name, x.youngs_modulus) for x in m.materials] == [("STEEL", 210.0e9)]
+
+
+def test_density_and_dload_warnings_errors_and_op_new():
+    """parser.rs:332-365 and :846-950: the density default, its overwrite,
+    extra-field, extra-row and outside-material warnings; GRAV and Pn field
+    counts; a face beyond the element's edges and an unknown element warn;
+    *DLOAD, OP=NEW clears the pressures and gravity the step inherited."""
+    m, w, _ = parse_inp(plate_deck("", "*STEP\n*STATIC\n*BOUNDARY\nBASE, 1, 2\n*END STEP\n"))
+    assert w == [] and m.density == 7850.0
+    deck = ("*NODE\n1, 0, 0\n2, 1, 0\n3, 0, 1\n*DENSITY\n1.0\n"
+            "*ELEMENT, TYPE=CPS3, ELSET=T\n7, 1, 2, 3\n*MATERIAL, NAME=M\n*ELASTIC\n1e9, 0.3\n"
+            "*DENSITY\n2000., 20.\n3000.\n*DENSITY\n2500.\n"
+            "*SOLID SECTION, ELSET=T, MATERIAL=M\n*STEP\n*STATIC\n"
+            "*DLOAD\nT, P4, 5.0\n8, P1, 1.0\nT, P2, 6.0\nGRAV, 9.8, 1.0\n*BOUNDARY\n1, 1, 2\n"
+            "*END STEP\n*STEP\n*STATIC\n*DLOAD\nT, P1, 2.0\n*END STEP\n"
+            "*STEP\n*STATIC\n*DLOAD, OP=NEW\nT, P3, 3.0\n*END STEP\n")
+    m, w, steps = parse_inp(deck)
+    assert w == [
+        "line 6: *DENSITY outside *MATERIAL — ignored",
+        "line 13: extra *DENSITY fields ignored (temperature dependence is v0.2)",
+        "line 14: extra *DENSITY row ignored (temperature dependence is v0.2)",
+        "line 16: *DENSITY overwrites an earlier value (per-material density is v0.4)",
+        "line 21: element 7 (cps3) has no face 4 — ignored",
+        "line 22: *DLOAD on unknown element 8 — ignored",
+    ]
+    assert m.density == 2500.0 and steps == 3
+    _b, _c, dloads, gravity = m.load_state()
+    assert [(d.element_id, d.face, d.magnitude) for d in dloads] == [(7, 3, 3.0)]
+    assert gravity is None
+    for bad, text in (("GRAV, 9.8\n", "*DLOAD GRAV expects GRAV, magnitude, dir1[, dir2][, "
+                                      "dir3]; got 2 field(s)"),
+                      ("GRAV, 9.8, 1, 2, 3, 4\n", "got 6 field(s)"),
+                      ("T, P1\n", "*DLOAD expects element/elset, P1..P4, magnitude; got 2 "
+                                  "field(s)"),
+                      ("T, P1, x\n", "malformed pressure magnitude 'x'")):
+        with pytest.raises(ParseError) as ei:
+            parse_inp(plate_deck("", "*STEP\n*STATIC\n*DLOAD\n" + bad))
+        assert text in str(ei.value)
 
 
 def two_step_deck(op_new):

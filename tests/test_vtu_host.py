@@ -168,3 +168,142 @@ def test_f64_text_matches_rust_display_on_random_bit_patterns(tmp_path):
     want = [vtu_oracle.rust_f64(v) for v in disp.ravel()]
     assert got == want
     assert all(float(t) == v or (v == 0.0) for t, v in zip(got, disp.ravel()))
+
+
+# ---- the reference's own fixtures and literal expectations (vtu.rs:382-738)
+def _ref_quad_tri():
+    """vtu.rs:382-430: a unit square as one CPS4 (1 2 3 4) and one CPS3
+    (2 4 3), with its solution."""
+    xyz = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [1.0, 1.0, 0.0], [0.0, 1.0, 0.0]])
+    kind = np.array([1, 0], dtype=np.uint8)
+    cp = np.array([0, 4, 7], dtype=np.int64)
+    conn = np.array([0, 1, 2, 3, 1, 3, 2], dtype=np.int32)
+    disp = np.array([[0.1, 0.2, 0.0], [0.0, -0.5, 0.0], [-0.3, 0.0, 0.5], [0.0, 0.0, 0.0]])
+    vm = np.array([42.5, 7.25])
+    return xyz, kind, cp, conn, disp, vm
+
+
+def test_reference_fixture_is_well_formed_and_round_trips(tmp_path):
+    # vtu.rs:382-451 (vtu_is_well_formed_and_round_trips)
+    xyz, kind, cp, conn, disp, vm = _ref_quad_tri()
+    path = tmp_path / "r.vtu"
+    write_vtu(path, xyz, kind, cp, conn, disp, vm)
+    xml = path.read_text()
+    for literal in ('type="UnstructuredGrid"', 'byte_format="ascii"', 'NumberOfPoints="4"',
+                    'NumberOfCells="2"', "0 1 2 3 1 3 2", "4 7", "9 5", 'Name="Displacement"',
+                    "0.1 0.2 0", "-0.3 0 0.5", 'Name="VonMises"', "42.5", "7.25"):
+        assert literal in xml, literal
+    assert xml.rstrip().endswith("</VTKFile>")
+
+
+def test_reference_fixture_extra_point_data_arrays(tmp_path):
+    # vtu.rs:453-513 (vtu_extra_point_data_arrays): one B31 on two nodes,
+    # an empty solution, two extra PointData arrays read back; with no extra
+    # arrays the file is byte-identical to the stock writer's
+    xyz = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    kind = np.array([7], dtype=np.uint8)
+    cp = np.array([0, 2], dtype=np.int64)
+    conn = np.array([0, 1], dtype=np.int32)
+    empty = np.zeros((0, 3))
+    path = tmp_path / "x.vtu"
+    arrays = [("Mode1", [0.25, 1.0]), ("Temperature", [100.0, 0.5])]
+    write_vtu(path, xyz, kind, cp, conn, empty, np.zeros(0),
+              extra=[(n, np.array(v)) for n, v in arrays])
+    xml = path.read_text()
+    for name, values in arrays:
+        after = xml.split(f'Name="{name}"')[1]
+        body = after[:after.index("</DataArray>")]
+        nums = []
+        for line in body.splitlines():
+            try:
+                nums.append(float(line.strip()))
+            except ValueError:
+                pass
+        assert nums == values, name
+    plain, stock = tmp_path / "p.vtu", tmp_path / "s.vtu"
+    write_vtu(plain, xyz, kind, cp, conn, empty, np.zeros(0), extra=[])
+    write_vtu(stock, xyz, kind, cp, conn, empty, np.zeros(0))
+    assert plain.read_bytes() == stock.read_bytes()
+
+
+def test_reference_fixture_types_for_new_kinds(tmp_path):
+    # vtu.rs:515-558 (vtu_types_for_new_kinds): CPS8, CPE8 -> 23, CPE4 -> 9,
+    # B31 -> 3 on nodes x = 1..11
+    xyz = np.array([[float(i), 0.0, 0.0] for i in range(1, 12)])
+    kind = np.array([2, 4, 3, 7], dtype=np.uint8)
+    cp = np.array([0, 8, 16, 20, 22], dtype=np.int64)
+    conn = np.array(list(range(8)) + list(range(8)) + [0, 1, 2, 3] + [8, 9], dtype=np.int32)
+    path = tmp_path / "k.vtu"
+    write_vtu(path, xyz, kind, cp, conn, np.zeros((0, 3)), np.zeros(0))
+    assert "23 23 9 3" in path.read_text()
+
+
+def test_reference_fixture_binary_round_trips_exact_appended_values(tmp_path):
+    # vtu.rs:560-673 (binary_vtu_round_trips_exact_appended_values): its bit
+    # patterns, the extremes of f64 and signed zeros; nodes 10 20 30 40,
+    # CPS4 (20 40 10 30) and CPS3 (20 30 40)
+    bits = lambda b: struct.unpack("<d", struct.pack("<Q", b))[0]  # noqa: E731
+    coordinate, displacement, stress = bits(0x3FF3C0D6E2F4B0D1), bits(0x3FDD555555555555), \
+        bits(0x404ACCCCCCCCCCCC)
+    tiny, big = 2.2250738585072014e-308, 1.7976931348623157e308
+    xyz = np.array([[tiny, -0.0, coordinate], [big, coordinate, 0.0],
+                    [-coordinate, tiny, -0.0], [0.0, -coordinate, big]])
+    kind = np.array([1, 0], dtype=np.uint8)
+    cp = np.array([0, 4, 7], dtype=np.int64)
+    conn = np.array([1, 3, 0, 2, 1, 2, 3], dtype=np.int32)
+    disp = np.array([[displacement, big, -tiny], [-0.0, coordinate, -displacement],
+                     [tiny, -coordinate, 0.0], [-big, displacement, coordinate]])
+    vm = np.array([stress, -stress])
+    path = tmp_path / "e.vtu"
+    write_vtu(path, xyz, kind, cp, conn, disp, vm, binary=True)
+    data = path.read_bytes()
+    marker = b'<AppendedData encoding="raw">_'
+    start = data.index(marker) + len(marker)
+    xml = data[:start].decode()
+    assert ('<VTKFile type="UnstructuredGrid" version="0.1" byte_order="LittleEndian">'
+            in xml)
+    assert '<Piece NumberOfPoints="4" NumberOfCells="2">' in xml
+
+    def block(name_or_section):
+        section, name = name_or_section
+        s = xml[xml.index(f"<{section}>"):xml.index(f"</{section}>")]
+        arrays = re.findall(r"<DataArray[^>]*/>", s)
+        arr = next(a for a in arrays if name is None or f'Name="{name}"' in a)
+        assert 'format="appended"' in arr
+        at = start + int(re.search(r'offset="(\d+)"', arr).group(1))
+        (n,) = struct.unpack("<i", data[at:at + 4])
+        return data[at + 4:at + 4 + n]
+
+    def same_bits(raw, expected):
+        got = np.frombuffer(raw, dtype="<f8")
+        return np.array_equal(got.view(np.int64), np.asarray(expected).view(np.int64))
+
+    pts = block(("Points", None))
+    assert len(pts) == 4 * 3 * 8 and same_bits(pts, xyz.ravel())
+    assert list(np.frombuffer(block(("Cells", "connectivity")), "<i8")) == [1, 3, 0, 2, 1, 2, 3]
+    assert list(np.frombuffer(block(("Cells", "offsets")), "<i8")) == [4, 7]
+    assert list(np.frombuffer(block(("Cells", "types")), "<i8")) == [9, 5]
+    d = block(("PointData", "Displacement"))
+    assert len(d) == 4 * 3 * 8 and same_bits(d, disp.ravel())
+    v = block(("CellData", "VonMises"))
+    assert len(v) == 2 * 8 and list(np.frombuffer(v, "<f8")) == [stress, -stress]
+
+
+def test_reference_fixture_binary_smaller_than_ascii(tmp_path):
+    # vtu.rs:675-737 (binary_vtu_is_smaller_than_ascii_for_a_large_mesh):
+    # 300 nodes on a line of B31 elements with its values
+    bits = lambda b: struct.unpack("<d", struct.pack("<Q", b))[0]  # noqa: E731
+    coordinate, displacement, stress = bits(0x3FF3C0D6E2F4B0D1), bits(0x3FDD555555555555), \
+        bits(0x404ACCCCCCCCCCCC)
+    ids = np.arange(1, 301, dtype=np.float64)
+    xyz = np.stack([ids * coordinate, -ids * coordinate, coordinate / ids], axis=1)
+    kind = np.full(299, 7, dtype=np.uint8)
+    cp = np.arange(0, 600, 2, dtype=np.int64)
+    conn = np.stack([np.arange(299), np.arange(1, 300)], axis=1).ravel().astype(np.int32)
+    disp = np.stack([np.full(300, displacement), np.full(300, -displacement),
+                     displacement / ids], axis=1)
+    vm = stress * np.arange(1, 300, dtype=np.float64)
+    a, b = tmp_path / "a.vtu", tmp_path / "b.vtu"
+    write_vtu(a, xyz, kind, cp, conn, disp, vm)
+    write_vtu(b, xyz, kind, cp, conn, disp, vm, binary=True)
+    assert os.path.getsize(b) < os.path.getsize(a)
