@@ -901,11 +901,14 @@ def _device_timed(stream, fn):
 
 
 def precision_block(local_rank):
-    """The 480x48x48 heterogeneous C3D8 cantilever: one FP64 and one mixed
-    solve (reassembly + PCG + stress) of the same device-resident operator,
-    each timed with CUDA events on the library's stream; the mixed form's
-    iteration split and its displacement error against the FP64 solve (the
-    oracle itself cannot solve this size: hours and ~20 GB of triplets)."""
+    """The 480x48x48 heterogeneous C3D8 cantilever: one FP64, one mixed and
+    one defect-correction solve (reassembly + PCG + stress) of the same
+    device-resident operator, each timed with CUDA events on the library's
+    stream; the FP32 forms' iteration splits and their displacement errors
+    against the FP64 solve (the oracle itself cannot solve this size: hours
+    and ~20 GB of triplets).  The defect-correction form (SVX_MIXED_DEFECT)
+    is the textbook one: an FP32 inner PCG (FP32 K, vectors and Jacobi;
+    FP64 dots) to 1e-5 inside FP64 defect correction."""
     import numpy as np
     import torch
 
@@ -918,7 +921,9 @@ def precision_block(local_rank):
         stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
         op = ctx.assemble(flat)
         try:
-            for prec in (abi.SVX_FP64, abi.SVX_MIXED):  # graphs, pools, first launches
+            forms = (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED),
+                     ("defect", abi.SVX_MIXED_DEFECT))
+            for _, prec in forms:  # graphs, pools, first launches
                 try:
                     op.solve_device(precision=prec, max_iter=64, want_stress=False)
                 except NotConverged:
@@ -926,15 +931,16 @@ def precision_block(local_rank):
             clocks = ClockSampler(local_rank)
             clocks.start()
             res = {}
-            for name, prec in (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED)):
+            for name, prec in forms:
                 def one():
                     op.reassemble()
                     return op.solve_device(precision=prec, max_iter=200000, want_stress=True)
                 (it, r, ms_s, _ms_st, ms_a), ms = _device_timed(stream, one)
                 fp32_it = op.last_fp32_iterations
+                outer = op.last_outer_iterations
                 disp = op.stress()[3]
                 res[name] = {"iterations": it, "fp32_iterations": fp32_it, "ms": ms,
-                             "pcg_ms": ms_s, "residual": r,
+                             "pcg_ms": ms_s, "residual": r, "outer": outer,
                              "u": np.asarray(disp).reshape(-1, 3)[:, :flat.ndof].ravel()}
             clk = clocks.stop()
             kms = op.time_kernels(reps=10)
@@ -945,7 +951,7 @@ def precision_block(local_rank):
     spmv64 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
     spmv32 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes, value_bytes=4)
     peak, peak_kind = measured_peaks()
-    f64, mx = res["fp64"], res["mixed"]
+    f64, mx, dc = res["fp64"], res["mixed"], res["defect"]
     row = lambda d: {"iterations": d["iterations"], "ms_per_solve": d["ms"],
                      "pcg_ms": d["pcg_ms"], "solves_per_s": 1000.0 / d["ms"],
                      "dof_iter_per_s": n * d["iterations"] / (d["ms"] / 1000.0),
@@ -957,6 +963,11 @@ def precision_block(local_rank):
                       fp32_share=mx["fp32_iterations"] / max(1, mx["iterations"]),
                       rel_err_vs_fp64=_rel(mx["u"], f64["u"])),
         "ratio_mixed_over_fp64": f64["ms"] / mx["ms"],
+        "defect_correction": dict(row(dc), fp32_iterations=dc["fp32_iterations"],
+                                  fp64_iterations=dc["iterations"] - dc["fp32_iterations"],
+                                  corrections=dc["outer"], inner_tol=1e-5,
+                                  rel_err_vs_fp64=_rel(dc["u"], f64["u"])),
+        "ratio_defect_over_fp64": f64["ms"] / dc["ms"],
         "spmv_fp64": {"ms": float(kms[0]), "gbs": spmv64 / kms[0] / 1e6,
                       "frac": spmv64 / kms[0] / 1e6 / peak},
         "spmv_fp32": {"ms": float(kms[3]), "gbs": spmv32 / kms[3] / 1e6,
@@ -1132,9 +1143,25 @@ def metric_forms(local_rank):
     """precision_c3, batched_c4 and served_c5 blocks of the default line."""
     blocks = {}
     t0 = time.perf_counter()
-    blocks["precision_c3"] = precision_block(local_rank)
-    blocks["batched_c4"], per_c4 = batched_block(local_rank)
-    blocks["served_c5"] = served_block(local_rank, c4_one_at_a_time_s=per_c4)
+
+    def guarded(name, fn):
+        # a failing block is reported in the line, never loses the line
+        try:
+            return fn()
+        except Exception as e:  # noqa: BLE001
+            blocks[name] = {"error": f"{type(e).__name__}: {e}"}
+            return None
+
+    out = guarded("precision_c3", lambda: precision_block(local_rank))
+    if out is not None:
+        blocks["precision_c3"] = out
+    per_c4 = None
+    out = guarded("batched_c4", lambda: batched_block(local_rank))
+    if out is not None:
+        blocks["batched_c4"], per_c4 = out
+    out = guarded("served_c5", lambda: served_block(local_rank, c4_one_at_a_time_s=per_c4))
+    if out is not None:
+        blocks["served_c5"] = out
     blocks["metric_forms_wall_s"] = time.perf_counter() - t0
     return blocks
 

@@ -175,9 +175,18 @@ typedef struct svx_resolved svx_resolved_t;
 /* Precision forms of the PCG solve. */
 enum svx_precision {
     SVX_FP64 = 0,      /* FP64 K, FP64 PCG: the plain form */
-    SVX_MIXED = 1      /* FP32-stored K streamed by the PCG, FP64 vectors, u, dots and
-                          true residual (reliable-update defect correction, finishing
-                          with the FP64 operator once the FP32 one stops gaining) */
+    SVX_MIXED = 1,     /* one FP64 Jacobi-PCG (FP64 vectors, u and dots) whose operator
+                          is relaxed as it converges: FP64 K until ||r||/||f|| <=
+                          clamp(tol * 1e7, tol, 0.1), then the FP32-stored K on the same
+                          search directions for at most as many iterations again, then
+                          FP64 K; convergence is decided on the true FP64 residual, and
+                          CG restarts on FP64 K if that is short of tol */
+    SVX_MIXED_DEFECT = 2 /* single solves only: FP64 defect correction (u, r = f - K64 u
+                          and the correction's update in FP64) around an inner Jacobi-PCG
+                          whose K, vectors and preconditioner are FP32 and whose dots
+                          accumulate in FP64, each inner solve to inner_tol; after two
+                          corrections that cut ||r|| by less than 2x the inner solver is
+                          the FP64 PCG */
 };
 
 /* Linear solver selection (Method, lib.rs:523-534; dispatch lib.rs:664-686). */
@@ -193,9 +202,9 @@ typedef struct svx_solve_opts {
     double tol;            /* relative residual tolerance (reference: 1e-10) */
     int64_t max_iter;      /* <= 0: max(1000, 10 * ndof_total) like lib.rs:632 */
     int32_t precision;     /* enum svx_precision */
-    double inner_tol;      /* mixed: residual reduction of each FP32 segment between two
-                              FP64 true-residual updates; values outside (0.01, 1)
-                              select 0.1 */
+    double inner_tol;      /* SVX_MIXED_DEFECT: relative residual of each inner FP32
+                              solve; values outside (0, 1) select 1e-5.  Unused by the
+                              other forms */
     int32_t check_every;   /* iterations per graph launch between host checks (0: auto) */
     int32_t want_stress;   /* 1: compute von Mises + reactions */
     int32_t method;        /* enum svx_method (svx_default_opts: SVX_METHOD_PCG) */
@@ -293,6 +302,28 @@ int svx_op_spmv(svx_op_t* op, const double* x, double* y);
 /* Installs u (host, n_rows) as the operator's solution, e.g. to recover
  * stresses for a displacement field computed elsewhere. */
 int svx_op_set_solution(svx_op_t* op, const double* u);
+
+/* ---- consistent mass --------------------------------------------- */
+/* The consistent mass matrix of a flat model of density `density` (kg/m^3;
+ * plane elements take the model's thickness) assembled on the device: the
+ * element mass matrices of CPS3 (closed form rho t A / 12 x [2 1 1; 1 2 1;
+ * 1 1 2]), CPS4 / CPE4 (rho t det J N_i N_j under 2x2 Gauss) and C3D8
+ * (rho det J N_i N_j under 2x2x2 Gauss) on every dof pair (d, d), summed by
+ * the stiffness's fixed-order node-block assembly into the same CSR pattern
+ * (zero entries and every diagonal included), with no Dirichlet rows.
+ * Replaces assemble_mass (crates/solvix-core/src/modal.rs:203-271) with
+ * cps3_mass / cps4_mass / c3d8_mass (modal.rs:82-146); the values are
+ * bit-identical to summing the reference's triplets in element order.  The
+ * operator answers svx_op_dims, svx_op_get_csr (which = 0), svx_op_spmv
+ * (y = M x) and svx_op_reassemble; svx_op_solve, svx_op_stress and
+ * svx_op_get_vectors return SVX_BAD_ARGUMENT for it.  Errors: the first
+ * failing element in enumeration order with the reference's text
+ * ("element 7: degenerate (zero-area) triangle", "... non-positive Jacobian
+ * determinant at a Gauss point"); kinds outside the four are rejected as
+ * InvalidModel like the stiffness; a negative or non-finite density is
+ * SVX_BAD_ARGUMENT.  Material, load and constraint arrays are not read. */
+int svx_assemble_mass(svx_ctx_t* ctx, const svx_flat_model_t* model, double density,
+                      svx_op_t** out, svx_error_t* err);
 
 /* ---- K5-K7: PCG --------------------------------------------------- */
 /* Replaces solver::pcg (solver.rs:66-149) and jacobi_cond (lib.rs:634-644);

@@ -40,6 +40,7 @@ SVX_NOALLOC_MAX_DOF = 262144
 # enum svx_precision
 SVX_FP64 = 0
 SVX_MIXED = 1
+SVX_MIXED_DEFECT = 2
 SVX_METHOD_PCG = 0
 SVX_METHOD_LDLT = 1
 SVX_METHOD_AUTO = 2
@@ -306,6 +307,8 @@ SIGNATURES = {
     "svx_resolved_flat": (C.POINTER(SvxFlatModel), [_VP]),
     "svx_resolved_pending": (C.c_int, [_VP, C.POINTER(SvxError)]),
     "svx_resolved_free": (C.c_int, [_VP]),
+    "svx_assemble_mass": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.c_double, C.POINTER(_VP),
+                                    C.POINTER(SvxError)]),
     "svx_assemble": (C.c_int, [_VP, C.POINTER(SvxFlatModel), C.c_uint32, C.POINTER(_VP),
                                C.POINTER(SvxError)]),
     "svx_op_free": (C.c_int, [_VP]),

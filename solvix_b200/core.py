@@ -89,6 +89,21 @@ class Context:
         self._ops.add(op)
         return op
 
+    def assemble_mass(self, flat: FlatModel, density: float) -> "Operator":
+        """The consistent mass matrix of the flat model (svx_assemble_mass,
+        modal.rs:203-271) as an operator: ``csr()`` exports it and
+        ``spmv(x)`` returns M x."""
+        s = flat.as_struct()
+        h = C.c_void_p()
+        err = abi.SvxError()
+        st = self.lib.svx_assemble_mass(self.handle, C.byref(s), float(density), C.byref(h),
+                                        C.byref(err))
+        if st != abi.SVX_OK:
+            _raise(st, err)
+        op = Operator(self, h, flat)
+        self._ops.add(op)
+        return op
+
     def solve_thermal(self, tm: ThermalModel, tol: float = 1e-10, max_iter: int = 0,
                       check_every: int = 0):
         """Steady conduction on the device (svx_solve_thermal_flat, the
@@ -217,11 +232,13 @@ class _SolutionBuffers:
             reactions=reactions, iterations=int(s.iterations),
             final_residual=float(s.final_residual),
             solver_method="ldlt" if s.solver_method == abi.SVX_METHOD_LDLT else
-            "pcg" if precision == abi.SVX_FP64 else "pcg-mixed",
+            "pcg" if precision == abi.SVX_FP64 else
+            "pcg-mixed" if precision == abi.SVX_MIXED else "pcg-defect",
             cond_estimate=float(s.cond_estimate), u=self.u, reaction_values=self.react,
             outer_iterations=int(s.outer_iterations), ms_assemble=float(s.ms_assemble),
             ms_solve=float(s.ms_solve), ms_stress=float(s.ms_stress),
-            factor_bandwidth=int(s.factor_bandwidth), ms_factor=float(s.ms_factor))
+            factor_bandwidth=int(s.factor_bandwidth), ms_factor=float(s.ms_factor),
+            fp32_iterations=int(s.fp32_iterations))
 
     def solution(self, flat: FlatModel, precision) -> Solution:
         node_ids = flat.node_id if flat.node_id is not None else \
@@ -317,6 +334,7 @@ class Operator:
         if st != abi.SVX_OK:
             _raise(st, err)
         self.last_fp32_iterations = int(sol.fp32_iterations)
+        self.last_outer_iterations = int(sol.outer_iterations)
         return int(sol.iterations), float(sol.final_residual), float(sol.ms_solve), \
             float(sol.ms_stress), float(sol.ms_assemble)
 

@@ -356,9 +356,38 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
+// The consistent mass matrix from the operator's device-resident model:
+// element mass matrices, pattern, fixed-order assembly (no Dirichlet rows;
+// assemble_mass, modal.rs:203-271, has none).
+void mass_assemble(svx_ctx* ctx, svx_op* op) {
+    cudaStream_t st = ctx->stream;
+    SVX_CUDA(cudaEventRecord(ctx->ev[2], st));
+    DBuf<double> ke;
+    ke.alloc(ctx->pool, size_t(op->n_elem) * op->pat.ke_stride + 1);
+    const uint64_t g = integrate_mass(ctx, op, op->mass_rho, ke.p, op->pat.ke_stride);
+    if (g != ~uint64_t(0)) {
+        const int64_t g_fail = int64_t(g >> 8);
+        const int g_reason = int(g & 0xff);
+        throw ModelFail{SVX_INVALID_MODEL, g_reason, g_fail,
+                        "element " + std::to_string(op->h_elem_id[g_fail]) + ": " +
+                            reason_text(g_reason)};
+    }
+    if (!op->pat.row_ptr.p) build_pattern(ctx, op);
+    op->vals.alloc(ctx->pool, op->pat.nnz + 1);
+    assemble_values(ctx, op, ke.p, op->pat.ke_stride, op->vals.p);
+    ke.reset();
+    op->spmv_group = choose_spmv_group(op);
+    SVX_CUDA(cudaEventRecord(ctx->ev[3], st));
+    op->ms_assemble = elapsed_ms(ctx->ev[2], ctx->ev[3]);
+}
+
 // K1-K4 from the operator's device-resident model: element integration,
 // pattern, fixed-order assembly and Dirichlet.  Needs no host model.
 void device_assemble(svx_ctx* ctx, svx_op* op) {
+    if (op->mass_rho >= 0.0) {
+        mass_assemble(ctx, op);
+        return;
+    }
     cudaStream_t st = ctx->stream;
     SVX_CUDA(cudaEventRecord(ctx->ev[2], st));
     DBuf<double> ke;
@@ -381,6 +410,8 @@ void device_assemble(svx_ctx* ctx, svx_op* op) {
                                  cudaMemcpyDeviceToDevice, st));
     }
     op->vals32.reset();
+    op->vals32v.reset();
+    op->valsT.reset();
     apply_dirichlet(ctx, op);
     op->spmv_group = choose_spmv_group(op);
     SVX_CUDA(cudaEventRecord(ctx->ev[3], st));
@@ -477,6 +508,62 @@ svx_op* assemble_impl(svx_ctx* ctx, const svx_flat_model_t* m, uint32_t flags,
     return op.release();
 }
 
+// svx_assemble_mass: the model's geometry on the device and its consistent
+// mass matrix; no material, load or constraint data is read.
+svx_op* assemble_mass_impl(svx_ctx* ctx, const svx_flat_model_t* m, double rho) {
+    SVX_CUDA(cudaSetDevice(ctx->device));
+    check_flat(m);
+    if (!(rho >= 0.0) || std::isinf(rho))
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "density must be finite and >= 0"};
+    bool solid = false, plane = false, beam = false;
+    for (int64_t e = 0; e < m->n_elem; ++e) {
+        const int k = m->kind[e];
+        if (k == SVX_C3D8 || k == SVX_C3D4) solid = true;
+        else if (k == SVX_B31) beam = true;
+        else plane = true;
+    }
+    if (beam && (plane || solid))
+        throw ModelFail{SVX_INVALID_MODEL, 0, -1,
+                        "mixed beam and continuum elements (v1: B31-only models)"};
+    if (solid && plane) throw ModelFail{SVX_INVALID_MODEL, 0, -1, "mixed dimensionality"};
+    if (m->ndof != ((solid || beam) ? 3 : 2))
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "ndof does not match the element kinds"};
+    std::unique_ptr<svx_op> op(new svx_op());
+    op->ctx = ctx;
+    op->n_nodes = m->n_nodes;
+    op->n_elem = m->n_elem;
+    op->ndof = m->ndof;
+    op->n = m->n_nodes * m->ndof;
+    op->thickness = m->thickness;
+    op->mass_rho = rho;
+    cudaStream_t st = ctx->stream;
+    SVX_CUDA(cudaEventRecord(ctx->ev[6], st));
+    upload(ctx, op->xyz, m->xyz, size_t(3 * m->n_nodes));
+    upload(ctx, op->kind, m->kind, size_t(op->n_elem));
+    upload(ctx, op->conn_ptr, m->conn_ptr, size_t(op->n_elem + 1));
+    upload(ctx, op->conn, m->conn, size_t(op->n_elem > 0 ? m->conn_ptr[op->n_elem] : 0));
+    int max_nn = 0;
+    for (int64_t e = 0; e < op->n_elem; ++e) max_nn = std::max(max_nn, node_count(m->kind[e]));
+    op->pat.max_nn = std::max(max_nn, 1);
+    const int max_N = max_nn * m->ndof;
+    op->pat.ke_stride = std::max(1, max_N * max_N);
+    op->h_elem_id.resize(size_t(op->n_elem));
+    for (int64_t e = 0; e < op->n_elem; ++e) op->h_elem_id[e] = elem_id_of(m, e);
+    op->h_node_id.resize(size_t(m->n_nodes));
+    for (int64_t i = 0; i < m->n_nodes; ++i)
+        op->h_node_id[i] = m->node_id ? m->node_id[i] : uint32_t(i + 1);
+    mass_assemble(ctx, op.get());
+    SVX_CUDA(cudaEventRecord(ctx->ev[7], st));
+    op->ms_upload_assemble = elapsed_ms(ctx->ev[6], ctx->ev[7]);
+    return op.release();
+}
+
+void refuse_mass(const svx_op* op, const char* what) {
+    if (op->mass_rho >= 0.0)
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1,
+                        std::string("the operator holds a consistent mass matrix; ") + what};
+}
+
 void stress_to_device(svx_op* op) {
     svx_ctx* ctx = op->ctx;
     if (!op->vm_elem.p) op->vm_elem.alloc(ctx->pool, op->n_elem + 1);
@@ -513,6 +600,9 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
     long long max_iter = opts.max_iter > 0 ? opts.max_iter : default_max_iter(op->n);
     if (opts.method < SVX_METHOD_PCG || opts.method > SVX_METHOD_AUTO)
         throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "unknown solver method"};
+    if (opts.precision != SVX_FP64 && opts.precision != SVX_MIXED &&
+        opts.precision != SVX_MIXED_DEFECT)
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "unknown precision"};
     op->u.alloc(ctx->pool, op->n + 1);
     PcgResult r{PCG_CONVERGED, 0, 0.0, 0.0};
     long long outer = 0;
@@ -520,6 +610,9 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
         if (opts.precision == SVX_MIXED)
             r = pcg_mixed(ctx, op, opts.tol, max_iter, opts.inner_tol, opts.check_every,
                           op->u.p, &outer);
+        else if (opts.precision == SVX_MIXED_DEFECT)
+            r = pcg_defect_correction(ctx, op, opts.tol, max_iter, opts.inner_tol,
+                                      opts.check_every, op->u.p, &outer);
         else
             r = pcg_fp64(ctx, op, opts.tol, max_iter, opts.check_every, op->u.p);
     }
@@ -539,7 +632,7 @@ int solve_impl(svx_op* op, const svx_solve_opts_t* o, svx_solution_t* sol, svx_e
         sol->iterations = r.iterations;
         sol->outer_iterations = outer;
         sol->fp32_iterations =
-            (opts.precision == SVX_MIXED && !direct) ? op->mixed_sloppy_iters : 0;
+            (opts.precision != SVX_FP64 && !direct) ? op->mixed_sloppy_iters : 0;
         sol->final_residual = r.residual;
         sol->cond_estimate = direct ? dres.cond : op->cond_estimate;
         sol->solver_method = direct ? SVX_METHOD_LDLT : SVX_METHOD_PCG;
@@ -619,7 +712,8 @@ void run_batch(svx_ctx* ctx, int32_t count, const svx_flat_model_t* const* model
                std::vector<BatchModelOut>& out, BatchRun& run) {
     SVX_CUDA(cudaSetDevice(ctx->device));
     if (o.precision != SVX_FP64 && o.precision != SVX_MIXED)
-        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "unknown precision"};
+        throw ModelFail{SVX_BAD_ARGUMENT, 0, -1,
+                        "the batched and served forms run SVX_FP64 or SVX_MIXED"};
     out.assign(static_cast<size_t>(count), BatchModelOut{});
     run = BatchRun{};
     using clock = std::chrono::steady_clock;
@@ -869,6 +963,7 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         }
         if (const char* e = std::getenv("SVX_PCG_SMEM")) ctx->pcg_smem = (e[0] != '0');
         if (const char* e = std::getenv("SVX_PCG_ALG")) ctx->pcg_alg = (e[0] == '0') ? 0 : 1;
+        if (const char* e = std::getenv("SVX_PCG_STAGE")) ctx->pcg_stage = (e[0] != '0');
         if (const char* e = std::getenv("SVX_PCG_UNROLL")) {
             const long v = std::strtol(e, nullptr, 10);
             if (v == 1 || v == 2 || v == 4) ctx->pcg_unroll = int(v);
@@ -917,6 +1012,17 @@ int svx_last_error(const svx_ctx_t* ctx, char* buf, size_t len) {
     const std::string& s = ctx ? ctx->last_error : g_thread_error;
     std::snprintf(buf, len, "%s", s.c_str());
     return SVX_OK;
+}
+
+int svx_assemble_mass(svx_ctx_t* ctx, const svx_flat_model_t* model, double density,
+                      svx_op_t** out, svx_error_t* err) {
+    if (!ctx || !out) return SVX_BAD_ARGUMENT;
+    *out = nullptr;
+    return guarded(ctx, err, [&]() -> int {
+        *out = assemble_mass_impl(ctx, model, density);
+        clear_error(err);
+        return SVX_OK;
+    });
 }
 
 int svx_assemble(svx_ctx_t* ctx, const svx_flat_model_t* model, uint32_t flags, svx_op_t** out,
@@ -1004,6 +1110,7 @@ int svx_op_get_vectors(const svx_op_t* op, int which, double* f, double* inv_dia
     if (!op) return SVX_BAD_ARGUMENT;
     svx_ctx* ctx = op->ctx;
     return guarded(ctx, nullptr, [&]() -> int {
+        if (f || inv_diag) refuse_mass(op, "it has no load vector or Jacobi diagonal");
         SVX_CUDA(cudaSetDevice(ctx->device));
         cudaStream_t st = ctx->stream;
         if (f && op->n)
@@ -1053,13 +1160,17 @@ int svx_op_solve(svx_op_t* op, const svx_solve_opts_t* opts, svx_solution_t* sol
                  svx_error_t* err) {
     if (!op) return SVX_BAD_ARGUMENT;
     svx_ctx* ctx = op->ctx;
-    return guarded(ctx, err, [&]() -> int { return solve_impl(op, opts, sol, err); });
+    return guarded(ctx, err, [&]() -> int {
+        refuse_mass(op, "it is not solved");
+        return solve_impl(op, opts, sol, err);
+    });
 }
 
 int svx_op_stress(svx_op_t* op, svx_solution_t* sol) {
     if (!op || !sol) return SVX_BAD_ARGUMENT;
     svx_ctx* ctx = op->ctx;
     return guarded(ctx, nullptr, [&]() -> int {
+        refuse_mass(op, "it has no stresses");
         if (!op->has_solution)
             throw ModelFail{SVX_BAD_ARGUMENT, 0, -1, "operator has no solution yet"};
         SVX_CUDA(cudaSetDevice(ctx->device));

@@ -796,6 +796,138 @@ __global__ void conduction_kernel(int64_t n_elem, const uint8_t* __restrict__ ki
     fail(SVX_REASON_UNSUPPORTED_KIND);
 }
 
+// ---------------------------------------------------------------- consistent mass
+// Consistent mass matrices (modal.rs:82-146), one thread per element, into
+// the element's Ke slot (row-major (ND nn)^2) for the fixed-order assembly:
+// CPS3 closed form rho t |2A| / 24 x (2 on the diagonal, 1 off it);
+// CPS4 / CPE4 rho t detJ N_i N_j under 2x2 Gauss (xi outer); C3D8
+// rho detJ N_i N_j under 2x2x2 Gauss (xi, eta, zeta nested), each value on
+// every dof pair (d, d) of nodes i, j and zero elsewhere.  The Jacobians
+// are built as quad_b / hex_b build them (the conduction kernel's code), the
+// node-pair values summed over the Gauss points in the reference's order,
+// so the values are bit-identical to the oracle's.  Failures: a zero-area
+// triangle, det J <= 0 at a Gauss point, a kind outside CPS3 / CPS4 / CPE4
+// / C3D8.
+__global__ void mass_kernel(int64_t n_elem, int ndof, const uint8_t* __restrict__ kind,
+                            const int64_t* __restrict__ conn_ptr,
+                            const int32_t* __restrict__ conn, const double* __restrict__ xyz,
+                            double rho, double t, double* __restrict__ ke, int ke_stride,
+                            unsigned long long* first_fail) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= n_elem) return;
+    const int kd = kind[e];
+    const int64_t q0 = conn_ptr[e];
+    double* ke_e = ke + e * int64_t(ke_stride);
+    auto fail = [&](int reason) {
+        atomicMin(first_fail, (unsigned long long)(e << 8) | (unsigned long long)reason);
+    };
+    // writes the (nn ndof)^2 matrix whose dof pairs (d, d) of nodes i, j
+    // hold v[i * nn + j]
+    auto put = [&](const double* v, int nn) {
+        const int N = nn * ndof;
+        for (int a = 0; a < N; ++a)
+            for (int c = 0; c < N; ++c)
+                ke_e[a * N + c] = (a % ndof == c % ndof) ? v[(a / ndof) * nn + c / ndof] : 0.0;
+    };
+    if (kd == SVX_CPS3) {
+        double p[3][2];
+        for (int i = 0; i < 3; ++i) {
+            const int64_t nd = conn[q0 + i];
+            p[i][0] = xyz[nd * 3];
+            p[i][1] = xyz[nd * 3 + 1];
+        }
+        const double two_a = (p[1][0] - p[0][0]) * (p[2][1] - p[0][1]) -
+                             (p[2][0] - p[0][0]) * (p[1][1] - p[0][1]);
+        if (two_a == 0.0) {
+            fail(SVX_REASON_DEGENERATE_TRI);
+            return;
+        }
+        const double w = rho * t * fabs(two_a) / 24.0;
+        double v[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) v[i * 3 + j] = w * (i == j ? 2.0 : 1.0);
+        put(v, 3);
+        return;
+    }
+    const double g = 1.0 / sqrt(3.0);
+    if (kd == SVX_CPS4 || kd == SVX_CPE4) {
+        double x[8];
+        for (int i = 0; i < 4; ++i) {
+            const int64_t nd = conn[q0 + i];
+            x[2 * i] = xyz[nd * 3];
+            x[2 * i + 1] = xyz[nd * 3 + 1];
+        }
+        double v[16];
+        for (int i = 0; i < 16; ++i) v[i] = 0.0;
+        for (int a = 0; a < 2; ++a)
+            for (int bq = 0; bq < 2; ++bq) {
+                const double xi = a ? g : -g, eta = bq ? g : -g;
+                double dxi[4], deta[4], n[4];
+                for (int i = 0; i < 4; ++i) {
+                    const double xi_i = quadc(i, 0), eta_i = quadc(i, 1);
+                    dxi[i] = 0.25 * xi_i * (1.0 + eta * eta_i);
+                    deta[i] = 0.25 * eta_i * (1.0 + xi * xi_i);
+                    n[i] = 0.25 * (1.0 + xi * xi_i) * (1.0 + eta * eta_i);
+                }
+                double j00 = 0.0, j01 = 0.0, j10 = 0.0, j11 = 0.0;
+                for (int i = 0; i < 4; ++i) {
+                    j00 += dxi[i] * x[2 * i];
+                    j01 += dxi[i] * x[2 * i + 1];
+                    j10 += deta[i] * x[2 * i];
+                    j11 += deta[i] * x[2 * i + 1];
+                }
+                const double detj = j00 * j11 - j01 * j10;
+                if (detj <= 0.0) {
+                    fail(SVX_REASON_BAD_JACOBIAN);
+                    return;
+                }
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j) v[i * 4 + j] += rho * t * detj * n[i] * n[j];
+            }
+        put(v, 4);
+        return;
+    }
+    if (kd == SVX_C3D8) {
+        double x[24];
+        for (int i = 0; i < 8; ++i) {
+            const int64_t nd = conn[q0 + i];
+            for (int b = 0; b < 3; ++b) x[i * 3 + b] = xyz[nd * 3 + b];
+        }
+        double v[64];
+        for (int i = 0; i < 64; ++i) v[i] = 0.0;
+        for (int gp = 0; gp < 8; ++gp) {
+            const double xi = (gp & 4) ? g : -g, eta = (gp & 2) ? g : -g,
+                         zeta = (gp & 1) ? g : -g;
+            double dn[3][8], n[8];
+            for (int i = 0; i < 8; ++i) {
+                const double a = hexc(i, 0), b = hexc(i, 1), c = hexc(i, 2);
+                dn[0][i] = 0.125 * a * (1.0 + eta * b) * (1.0 + zeta * c);
+                dn[1][i] = 0.125 * b * (1.0 + xi * a) * (1.0 + zeta * c);
+                dn[2][i] = 0.125 * c * (1.0 + xi * a) * (1.0 + eta * b);
+                n[i] = 0.125 * (1.0 + xi * a) * (1.0 + eta * b) * (1.0 + zeta * c);
+            }
+            double J[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    double sum = 0.0;
+                    for (int i = 0; i < 8; ++i) sum += dn[a][i] * x[i * 3 + b];
+                    J[a * 3 + b] = sum;
+                }
+            const double detj = det3(J);
+            if (detj <= 0.0) {
+                fail(SVX_REASON_BAD_JACOBIAN);
+                return;
+            }
+            for (int i = 0; i < 8; ++i)
+                for (int j = 0; j < 8; ++j) v[i * 8 + j] += rho * detj * n[i] * n[j];
+        }
+        put(v, 8);
+        return;
+    }
+    fail(SVX_REASON_UNSUPPORTED_KIND);
+}
+
+
 // Element source loads summed per node over its incident (element, local)
 // slots in ascending element order: the reference's f[idx[i]] += fe[i] in
 // element enumeration order (heat.rs:207-212, 283-288).
@@ -923,6 +1055,22 @@ void recover_stress(svx_ctx* ctx, svx_op* op, const double* u, double* vm_elem, 
                                                                            op->ndof, u, disp3);
         SVX_LAUNCH_CHECK();
     }
+}
+
+uint64_t integrate_mass(svx_ctx* ctx, svx_op* op, double rho, double* ke, int ke_stride) {
+    DBuf<unsigned long long> fail;
+    fail.alloc(ctx->pool, 1);
+    SVX_CUDA(cudaMemsetAsync(fail.p, 0xff, sizeof(unsigned long long), ctx->stream));
+    if (op->n_elem > 0) {
+        mass_kernel<<<blocks_for(op->n_elem, 128), 128, 0, ctx->stream>>>(
+            op->n_elem, op->ndof, op->kind.p, op->conn_ptr.p, op->conn.p, op->xyz.p, rho,
+            op->thickness, ke, ke_stride, fail.p);
+        SVX_LAUNCH_CHECK();
+    }
+    unsigned long long h = 0;
+    SVX_CUDA(cudaMemcpyAsync(&h, fail.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+    return h;
 }
 
 uint64_t integrate_conduction(svx_ctx* ctx, svx_op* op, double conductivity, int has_source,

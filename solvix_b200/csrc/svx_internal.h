@@ -192,6 +192,9 @@ struct svx_ctx {
     // its nodes per warp step with all loads in flight (0: 4);
     // SVX_PCG_UNROLL sets it
     int pcg_unroll = 0;
+    // 1: the three-barrier form stages the gathered p window in shared
+    // memory; SVX_PCG_STAGE=0 gathers from L2 (measurements)
+    int pcg_stage = 1;
 };
 
 namespace svx {
@@ -267,7 +270,16 @@ struct svx_op {
     svx::Pattern pat;
     // assembled system
     svx::DBuf<double> vals;        // K after Dirichlet (the PCG operator)
+    // K again with each node's values ordered (da, db, neighbour slot), the
+    // slot fastest: the shared-memory PCG kernel's operand (ndof >= 2)
+    svx::DBuf<double> valsT;
     svx::DBuf<float> vals32;       // FP32 copy (mixed precision)
+    // the FP32 copy again with every node's rows 16-byte aligned and padded
+    // to whole float4s (3D operators, graph-form SpMV); base32v[i] is node
+    // i's first float, its rows are round_up(ndof * degree, 4) floats apart
+    svx::DBuf<float> vals32v;
+    svx::DBuf<int64_t> base32v;
+    int64_t n32v = 0;
     svx::DBuf<double> f;           // load vector after Dirichlet
     svx::DBuf<double> f_orig;      // load vector before Dirichlet
     svx::DBuf<double> inv_diag;
@@ -298,6 +310,9 @@ struct svx_op {
     // PCG tuning picked for this operator
     int spmv_group = 8;
     long long mixed_sloppy_iters = 0;  // FP32-operator iterations of the last mixed solve
+    // >= 0: the operator holds the consistent mass matrix of this density
+    // (svx_assemble_mass) instead of a stiffness
+    double mass_rho = -1.0;
     int spmv_block = 256;
 };
 
@@ -315,9 +330,17 @@ void assemble_values(svx_ctx* ctx, svx_op* op, const double* ke, int ke_stride, 
 void apply_dirichlet(svx_ctx* ctx, svx_op* op);
 // Inverse diagonal and condition estimate of op->vals alone (svx_assemble.cu).
 void jacobi_diagonal(svx_ctx* ctx, svx_op* op);
+// The graph form's FP32 difference-form SpMV with p.q, for FP64 (V =
+// double) or FP32 (V = float) vectors (svx_pcg.cu); at most `grid` blocks.
+template <class V>
+void launch_spmv_fp32(const svx_op* op, int G, unsigned grid, cudaStream_t st, const V* p, V* q,
+                      double* partials, PcgScalars* s);
 // Steady conduction (svx_element.cu): element conduction matrices into Ke
 // slots and source loads into fe ([n_elem * max_nn]); returns the first
 // failing element as (index << 8 | reason) or UINT64_MAX.
+// consistent mass matrices (modal.rs:82-146) into ke; the first failing
+// element as (index << 8 | reason), or all ones
+uint64_t integrate_mass(svx_ctx* ctx, svx_op* op, double rho, double* ke, int ke_stride);
 uint64_t integrate_conduction(svx_ctx* ctx, svx_op* op, double conductivity, int has_source,
                               double source, double* ke, int ke_stride, double* fe);
 // f = element source loads (node order of the slots) + plane-edge fluxes.
@@ -341,6 +364,9 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
                    double* u_dev);
 PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, double inner_tol,
                     int check_every, double* u_dev, long long* outer_steps);
+PcgResult pcg_defect_correction(svx_ctx* ctx, svx_op* op, double tol, long long max_iter,
+                                double inner_tol, int check_every, double* u_dev,
+                                long long* outer_steps);
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y);
 
 // Direct path (svx_ldlt.cu): LDL^T of op->vals in the reverse Cuthill-McKee
@@ -370,6 +396,7 @@ struct BatchStats {
 };
 // FP32 difference-form copy of the operator for the mixed forms (svx_pcg.cu).
 void build_fp32_operator(svx_ctx* ctx, svx_op* op);
+const double* transposed_values(svx_ctx* ctx, svx_op* op);
 void batch_pcg(svx_ctx* ctx, svx_op* op, int count, const std::vector<int64_t>& node_off,
                const std::vector<double>& tol, const std::vector<int64_t>& max_iter,
                std::vector<int64_t>& it, std::vector<double>& res, std::vector<int32_t>& status,

@@ -141,7 +141,8 @@ int64_t estimate_bytes(const svx_flat_model_t& m) {
     int64_t b = 0;
     b += ke * 8;                         // element matrices (freed after assembly)
     b += nnz * (8 + 4 + 4);              // K, its column indices, FP32 copy
-    b += n * 8 * 14 + m.n_fixed * 16;    // PCG and output vectors, constraints
+    b += n * 8 * 17 + m.n_fixed * 16;    // PCG, mixed-form rollback and output vectors,
+                                         // constraints
     b += m.n_nodes * (24 + 40) + m.n_elem * 64 + conn * (4 + 1 + 4 + 2 * 8);
     return b + 64 * 1024;
 }

@@ -208,6 +208,7 @@ class Solution:
     ms_stress: float = 0.0
     factor_bandwidth: int = 0   # direct path: half-bandwidth of K in the RCM order
     ms_factor: float = 0.0      # direct path: device time of factorization + solves
+    fp32_iterations: int = 0    # mixed forms: iterations on the FP32 operator
 
 
 class SolveError(Exception):

@@ -141,6 +141,19 @@ def test_heterogeneous_c3d8_graph_form_mixed_matches_oracle(graph_ctx, hetero_16
     assert sol.final_residual <= 1e-10
 
 
+def test_heterogeneous_c3d8_defect_correction_matches_oracle(graph_ctx, hetero_160):
+    """FP32 inner PCG (FP32 K, vectors, preconditioner; FP64 dots) to 1e-5
+    inside FP64 defect correction, on the graph form."""
+    flat, ref = hetero_160
+    sol = graph_ctx.solve_flat(flat, precision=abi.SVX_MIXED_DEFECT)
+    assert sol.solver_method == "pcg-defect"
+    assert sol.final_residual <= 1e-10
+    assert sol.outer_iterations >= 2
+    assert 0 < sol.fp32_iterations <= sol.iterations
+    assert rel(sol.u, ref.u) <= MIXED_TOL
+    assert vm_rel(sol.von_mises, ref.von_mises) <= 1e-7
+
+
 def test_heterogeneous_c3d8_persistent_form_matches_oracle(ctx, hetero_160):
     flat, ref = hetero_160
     sol = ctx.solve_flat(flat)
