@@ -195,6 +195,9 @@ struct svx_ctx {
     // 1: the three-barrier form stages the gathered p window in shared
     // memory; SVX_PCG_STAGE=0 gathers from L2 (measurements)
     int pcg_stage = 1;
+    // the FP32 operator's vectorised copy: 2 quads, 1 float4-padded rows,
+    // 0 none (the node-block kernel); SVX_FP32_LAYOUT (measurements)
+    int fp32_layout = 2;
 };
 
 namespace svx {
@@ -280,6 +283,14 @@ struct svx_op {
     svx::DBuf<float> vals32v;
     svx::DBuf<int64_t> base32v;
     int64_t n32v = 0;
+    // the FP32 copy in quads (3D operators, graph-form SpMV): node i's 9
+    // (da, db) rows over its neighbour slots, slot fastest, padded to a
+    // multiple of 4 slots, from baseq[i]; adjq its neighbours padded with
+    // the node itself, from baseq[i] / 9
+    svx::DBuf<float> vals32q;
+    svx::DBuf<int64_t> baseq;
+    svx::DBuf<int32_t> adjq;
+    int64_t n32q = 0;
     svx::DBuf<double> f;           // load vector after Dirichlet
     svx::DBuf<double> f_orig;      // load vector before Dirichlet
     svx::DBuf<double> inv_diag;

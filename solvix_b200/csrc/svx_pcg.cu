@@ -54,6 +54,11 @@ constexpr int NODE_BLOCKS_PER_SM = 5;
 #define SVX_SPMV32V_BPS 4
 #endif
 constexpr int SPMV32V_BLOCKS_PER_SM = SVX_SPMV32V_BPS;
+// ... and for the quad-layout FP32 SpMV (ND*ND float4 values a lane)
+#ifndef SVX_SPMV32Q_BPS
+#define SVX_SPMV32Q_BPS 3
+#endif
+constexpr int SPMV32Q_BLOCKS_PER_SM = SVX_SPMV32Q_BPS;
 // Resident threads per SM the batched kernels are compiled for: 1,024 (at
 // most 64 registers a thread) for 3D members, 1,536 for the lighter 2D ones,
 // to keep enough node gathers in flight.
@@ -727,6 +732,136 @@ spmv32v_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         __syncwarp();  // the staged values are rewritten for the next node
 #pragma unroll
         for (int ps = 0; ps < PASSES; ++ps) kv[ps] = kn[ps];
+    }
+    double bs = block_sum(dot, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+    if (last_block(&s->count_a)) {
+        double pap = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            s->count_a = 0;
+            s->pap = pap;
+            if (pap <= 0.0 || isnan(pap)) {
+                s->status = PCG_BREAKDOWN;
+                s->it = s->it + 1;
+                s->res = sqrt(s->rr) / s->bnorm;
+            } else {
+                s->alpha = s->rz / pap;
+            }
+        }
+    }
+}
+
+
+// ------------------------------------------------------------ quad FP32 operator
+// vals32 (node-block layout) -> vals32q: node i's ND*ND (da, db) rows over
+// its neighbour slots, slot fastest, each padded with zeros to dq =
+// round_up(d, 4) slots (4 for a node no element uses, whose own slot holds
+// its diagonal); adjq lists the node's neighbours padded with the node
+// itself.  baseq[i] is node i's first value; its neighbour list starts at
+// baseq[i] / (ND*ND).  Both are 16-byte aligned, so a lane reads four
+// slots of one (da, db) row, or four neighbour indices, in one load.
+template <int ND>
+__global__ void quad_fp32_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                                 const int32_t* __restrict__ adj,
+                                 const int64_t* __restrict__ node_base,
+                                 const int64_t* __restrict__ baseq,
+                                 const float* __restrict__ vals32, float* __restrict__ out,
+                                 int32_t* __restrict__ adjq) {
+    const int64_t t = int64_t(blockIdx.x) * BLOCK + threadIdx.x;
+    const int64_t i = t / (ND * ND);
+    if (i >= n_nodes) return;
+    const int e = int(t - i * (ND * ND)), da = e / ND, db = e - da * ND;
+    const int d = int(adj_ptr[i + 1] - adj_ptr[i]);
+    const int dq = d == 0 ? 4 : (d + 3) & ~3;
+    const int64_t q0 = baseq[i];
+    float* dst = out + q0 + int64_t(e) * dq;
+    if (d == 0) {
+        for (int k = 0; k < 4; ++k)
+            dst[k] = (k == 0 && da == db) ? vals32[node_base[i] + da] : 0.0f;
+    } else {
+        const float* src = vals32 + node_base[i] + int64_t(da) * ND * d + db;
+        for (int k = 0; k < dq; ++k) dst[k] = k < d ? src[int64_t(k) * ND] : 0.0f;
+    }
+    if (e == 0) {
+        int32_t* aq = adjq + q0 / (ND * ND);
+        for (int k = 0; k < dq; ++k) aq[k] = k < d ? adj[adj_ptr[i] + k] : int32_t(i);
+    }
+}
+
+// q = K32 p for the difference-form FP32 operator in the quad layout, and
+// the block partial of p.q (the last block forms pap and alpha, as
+// spmv_node_dot_kernel does).  Eight lanes per node, four nodes a warp:
+// lane g takes the neighbour slots 4g .. 4g+3 (one pass for up to 32
+// neighbour blocks), loads their four indices as one int4 and each of the
+// node's ND*ND rows as one float4, gathers the four neighbours' p, and
+// multiplies in FP64 with p_j - p_i (p_i for the node's own slot and the
+// padding, whose values are zero).  Per lane ND*ND 16-byte value loads are
+// in flight at once: four times the bytes of the node-block kernel's
+// scalar loads, which leave the FP32 operator latency-bound.
+template <int ND, class V>
+__global__ void __launch_bounds__(BLOCK, SPMV32Q_BLOCKS_PER_SM)
+spmv32q_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
+                        const int64_t* __restrict__ baseq, const int32_t* __restrict__ adjq,
+                        const float* __restrict__ vals32q, const V* __restrict__ p,
+                        V* __restrict__ q, double* __restrict__ partials,
+                        PcgScalars* __restrict__ s) {
+    constexpr int G = 8;
+    __shared__ double sh[32];
+    if (s->status != PCG_RUNNING) return;
+    const int gl = threadIdx.x & (G - 1);
+    const int64_t nodes_per_block = BLOCK / G;
+    double dot = 0.0;
+    for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
+         nb += int64_t(gridDim.x) * nodes_per_block) {
+        const int64_t i = nb + ((threadIdx.x & 31) / G);
+        double acc[ND];
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+        if (i < n_nodes) {
+            const int d = int(__ldg(adj_ptr + i + 1) - __ldg(adj_ptr + i));
+            const int dq4 = d == 0 ? 1 : (d + 3) >> 2;
+            const int64_t q0 = __ldg(baseq + i);
+            const float4* v4 = reinterpret_cast<const float4*>(vals32q + q0);
+            const int4* a4 = reinterpret_cast<const int4*>(adjq + q0 / (ND * ND));
+            double xi[ND];
+#pragma unroll
+            for (int db = 0; db < ND; ++db) xi[db] = double(__ldg(p + i * ND + db));
+            for (int c = gl; c < dq4; c += G) {
+                const int4 jj = __ldg(a4 + c);
+                float4 kv[ND * ND];
+#pragma unroll
+                for (int e = 0; e < ND * ND; ++e) kv[e] = __ldg(v4 + int64_t(e) * dq4 + c);
+                const int32_t js[4] = {jj.x, jj.y, jj.z, jj.w};
+                double xv[4][ND];
+#pragma unroll
+                for (int m = 0; m < 4; ++m)
+#pragma unroll
+                    for (int db = 0; db < ND; ++db) {
+                        const double x = double(__ldg(p + int64_t(js[m]) * ND + db));
+                        xv[m][db] = (js[m] != int32_t(i)) ? x - xi[db] : x;
+                    }
+#pragma unroll
+                for (int da = 0; da < ND; ++da)
+#pragma unroll
+                    for (int db = 0; db < ND; ++db) {
+                        const float4 k4 = kv[da * ND + db];
+                        acc[da] += double(k4.x) * xv[0][db];
+                        acc[da] += double(k4.y) * xv[1][db];
+                        acc[da] += double(k4.z) * xv[2][db];
+                        acc[da] += double(k4.w) * xv[3][db];
+                    }
+            }
+        }
+#pragma unroll
+        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+        if (i < n_nodes && gl == 0) {
+#pragma unroll
+            for (int da = 0; da < ND; ++da) {
+                const V qv = V(acc[da]);
+                q[i * ND + da] = qv;
+                dot += double(__ldg(p + i * ND + da)) * double(qv);
+            }
+        }
     }
     double bs = block_sum(dot, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = bs;
@@ -2399,7 +2534,7 @@ struct PcgRun {
 
     void enqueue_iteration(cudaStream_t st) {
         if constexpr (std::is_same<M, float>::value) {
-            if (vals == op->vals32.p && op->vals32v.p)
+            if (vals == op->vals32.p && (op->vals32v.p || op->vals32q.p))
                 launch_spmv_fp32(op, G, grid_r, st, p, q, partials, s);
             else
                 launch_spmv_node_dot<M, V>(op, G, grid_r, st, vals, p, q, partials, s);
@@ -2744,9 +2879,34 @@ void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
         compensated_fp32_kernel<2><<<grid, BLOCK, 0, ctx->stream>>>(
             op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->vals.p, op->vals32.p);
     SVX_LAUNCH_CHECK();
-    // the padded copy for the graph form's vectorised SpMV (3D, <= 32
-    // neighbour blocks a node); its row offsets depend only on the pattern
-    if (op->ndof != 3 || P.max_deg > 32 || op->n_nodes == 0) return;
+    // a vectorised copy for the graph form's FP32 SpMV (3D, <= 32 neighbour
+    // blocks a node); its offsets depend only on the pattern
+    if (op->ndof != 3 || P.max_deg > 32 || op->n_nodes == 0 || ctx->fp32_layout == 0) return;
+    if (ctx->fp32_layout == 2) {
+        if (!op->baseq.p) {
+            std::vector<int64_t> ap(size_t(op->n_nodes) + 1), base(size_t(op->n_nodes) + 1);
+            SVX_CUDA(cudaMemcpyAsync(ap.data(), P.adj_ptr.p, ap.size() * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+            SVX_CUDA(cudaStreamSynchronize(ctx->stream));
+            base[0] = 0;
+            for (int64_t i = 0; i < op->n_nodes; ++i) {
+                const int64_t d = ap[i + 1] - ap[i];
+                base[i + 1] = base[i] + 9 * (d == 0 ? 4 : (d + 3) & ~int64_t(3));
+            }
+            op->baseq.alloc(ctx->pool, base.size());
+            SVX_CUDA(cudaMemcpyAsync(op->baseq.p, base.data(), base.size() * sizeof(int64_t),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+            op->n32q = base.back();
+            op->adjq.alloc(ctx->pool, size_t(op->n32q / 9) + 4);
+        }
+        op->vals32q.alloc(ctx->pool, size_t(op->n32q) + 4);
+        const int64_t threads = op->n_nodes * 9;
+        quad_fp32_kernel<3><<<unsigned((threads + BLOCK - 1) / BLOCK), BLOCK, 0, ctx->stream>>>(
+            op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->baseq.p, op->vals32.p,
+            op->vals32q.p, op->adjq.p);
+        SVX_LAUNCH_CHECK();
+        return;
+    }
     if (!op->base32v.p) {
         std::vector<int64_t> ap(size_t(op->n_nodes) + 1), base(size_t(op->n_nodes) + 1);
         SVX_CUDA(cudaMemcpyAsync(ap.data(), P.adj_ptr.p, ap.size() * sizeof(int64_t),
@@ -2767,12 +2927,22 @@ void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
     SVX_LAUNCH_CHECK();
 }
 
-// The graph form's FP32 SpMV: the vectorised kernel on the padded copy when
-// it exists, the node-block kernel otherwise.
+// The graph form's FP32 SpMV: a vectorised kernel on its copy of the
+// operator when one exists, the node-block kernel otherwise.
 template <class V>
 void launch_spmv_fp32(const svx_op* op, int G, unsigned grid, cudaStream_t st, const V* p, V* q,
                       double* partials, PcgScalars* s) {
-    if (op->vals32v.p) {
+    if (op->vals32q.p) {
+        const Pattern& P = op->pat;
+        // one wave at this kernel's residency, never more blocks than the
+        // caller's partials hold
+        grid = unsigned(std::min<int64_t>(
+                {int64_t(grid), int64_t(op->ctx->sm_count) * SPMV32Q_BLOCKS_PER_SM,
+                 (op->n_nodes + BLOCK / 8 - 1) / (BLOCK / 8)}));
+        spmv32q_node_dot_kernel<3, V><<<grid, BLOCK, 0, st>>>(op->n_nodes, P.adj_ptr.p,
+                                                               op->baseq.p, op->adjq.p,
+                                                               op->vals32q.p, p, q, partials, s);
+    } else if (op->vals32v.p) {
         const Pattern& P = op->pat;
         // one wave at this kernel's residency, never more blocks than the
         // caller's partials hold
