@@ -935,7 +935,13 @@ def precision_block(local_rank):
                 def one():
                     op.reassemble()
                     return op.solve_device(precision=prec, max_iter=200000, want_stress=True)
-                (it, r, ms_s, _ms_st, ms_a), ms = _device_timed(stream, one)
+                try:
+                    (it, r, ms_s, _ms_st, ms_a), ms = _device_timed(stream, one)
+                except NotConverged as e:  # reported in the line, the other forms kept
+                    if name == "fp64":
+                        raise
+                    res[name] = {"error": f"NotConverged: {e}"}
+                    continue
                 fp32_it = op.last_fp32_iterations
                 outer = op.last_outer_iterations
                 disp = op.stress()[3]
@@ -952,6 +958,9 @@ def precision_block(local_rank):
     spmv32 = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes, value_bytes=4)
     peak, peak_kind = measured_peaks()
     f64, mx, dc = res["fp64"], res["mixed"], res["defect"]
+    def form(d, **extra):
+        return dict(row(d), **extra) if "error" not in d else d
+
     row = lambda d: {"iterations": d["iterations"], "ms_per_solve": d["ms"],
                      "pcg_ms": d["pcg_ms"], "solves_per_s": 1000.0 / d["ms"],
                      "dof_iter_per_s": n * d["iterations"] / (d["ms"] / 1000.0),
@@ -959,15 +968,16 @@ def precision_block(local_rank):
     out = {
         "workload": PRECISION_NAME, "n_dof": n, "nnz": nnz,
         "fp64": row(f64),
-        "mixed": dict(row(mx), fp32_iterations=mx["fp32_iterations"],
-                      fp32_share=mx["fp32_iterations"] / max(1, mx["iterations"]),
-                      rel_err_vs_fp64=_rel(mx["u"], f64["u"])),
-        "ratio_mixed_over_fp64": f64["ms"] / mx["ms"],
-        "defect_correction": dict(row(dc), fp32_iterations=dc["fp32_iterations"],
-                                  fp64_iterations=dc["iterations"] - dc["fp32_iterations"],
-                                  corrections=dc["outer"], inner_tol=1e-5,
-                                  rel_err_vs_fp64=_rel(dc["u"], f64["u"])),
-        "ratio_defect_over_fp64": f64["ms"] / dc["ms"],
+        "mixed": form(mx, fp32_iterations=mx.get("fp32_iterations"),
+                      fp32_share=mx.get("fp32_iterations", 0) / max(1, mx.get("iterations", 1)),
+                      rel_err_vs_fp64=_rel(mx["u"], f64["u"]) if "u" in mx else None),
+        "ratio_mixed_over_fp64": f64["ms"] / mx["ms"] if "ms" in mx else None,
+        "defect_correction": form(dc, fp32_iterations=dc.get("fp32_iterations"),
+                                  fp64_iterations=dc.get("iterations", 0) -
+                                  dc.get("fp32_iterations", 0),
+                                  corrections=dc.get("outer"), inner_tol=1e-5,
+                                  rel_err_vs_fp64=_rel(dc["u"], f64["u"]) if "u" in dc else None),
+        "ratio_defect_over_fp64": f64["ms"] / dc["ms"] if "ms" in dc else None,
         "spmv_fp64": {"ms": float(kms[0]), "gbs": spmv64 / kms[0] / 1e6,
                       "frac": spmv64 / kms[0] / 1e6 / peak},
         "spmv_fp32": {"ms": float(kms[3]), "gbs": spmv32 / kms[3] / 1e6,

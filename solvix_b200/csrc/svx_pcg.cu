@@ -318,7 +318,84 @@ spmv_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
     }
 }
 
-// r = f - K u (FP64, node blocks) and r.r, for the defect correction.
+// ------------------------------------------------------------ compensated residual
+// The true residual r = f - K u of a nearly converged solve is a difference
+// of two nearly equal sums: in plain FP64 its rounding error is ~1e-16 of
+// sum_j |K_ij u_j|, which on a stiff, high-contrast model is larger than
+// tol ||f|| itself (about 2e-10 ||f|| on the 480 x 48 x 48 heterogeneous
+// cantilever, so no iterate could ever pass a 1e-10 true-residual test).
+// Here every product and every addition keeps its exact rounding error:
+// the product's by a fused multiply-add (a x - fl(a x)), the sum's by
+// Knuth's TwoSum, the running sum carried as an unevaluated pair hi + lo.
+// The residual then comes out to ~1e-16 of its own size.  The explicit
+// round-to-nearest intrinsics keep the compiler from contracting the pairs'
+// arithmetic into fused operations.
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double b) {
+    const double s = __dadd_rn(hi, b);
+    const double bp = __dsub_rn(s, hi);
+    const double e = __dadd_rn(__dsub_rn(hi, __dsub_rn(s, bp)), __dsub_rn(b, bp));
+    hi = s;
+    lo = __dadd_rn(lo, e);
+}
+
+__device__ __forceinline__ void dd_mul_add(double& hi, double& lo, double a, double x) {
+    const double p = __dmul_rn(a, x);
+    dd_add(hi, lo, p);
+    lo = __dadd_rn(lo, __fma_rn(a, x, -p));
+}
+
+template <int G>
+__device__ __forceinline__ void group_sum_dd(double& hi, double& lo) {
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) {
+        const double oh = __shfl_xor_sync(0xffffffffu, hi, off);
+        const double ol = __shfl_xor_sync(0xffffffffu, lo, off);
+        dd_add(hi, lo, oh);
+        lo = __dadd_rn(lo, ol);
+    }
+}
+
+// f_i - (hi + lo): f_i and hi agree to a few bits near convergence, so the
+// first difference is exact
+__device__ __forceinline__ double dd_residual(double f, double hi, double lo) {
+    return __dsub_rn(__dsub_rn(f, hi), lo);
+}
+
+// One node's rows of K u as pairs (hi, lo), G lanes splitting its neighbour
+// blocks (the node-block layout, as node_rows); CG: u was written by other
+// CTAs of the launch and is read from L2.
+template <int ND, int G, bool CG>
+__device__ __forceinline__ void node_rows_dd(const int64_t* __restrict__ adj_ptr,
+                                             const int32_t* __restrict__ adj,
+                                             const int64_t* __restrict__ node_base,
+                                             const double* __restrict__ vals, const double* u,
+                                             int64_t i, int gl, double* hi, double* lo) {
+    const int64_t a0 = adj_ptr[i];
+    const int d = int(adj_ptr[i + 1] - a0);
+    const double* __restrict__ v = vals + node_base[i];
+    auto ld = [&](int64_t c) { return CG ? __ldcg(u + c) : u[c]; };
+    if (d == 0) {  // an unreferenced node: rows of length 1 (the diagonal)
+        if (gl == 0)
+#pragma unroll
+            for (int da = 0; da < ND; ++da) dd_mul_add(hi[da], lo[da], v[da], ld(i * ND + da));
+        return;
+    }
+    const int rowlen = ND * d;
+    for (int k = gl; k < d; k += G) {
+        const int64_t c = int64_t(__ldg(adj + a0 + k)) * ND;
+        double xv[ND];
+#pragma unroll
+        for (int db = 0; db < ND; ++db) xv[db] = ld(c + db);
+#pragma unroll
+        for (int da = 0; da < ND; ++da)
+#pragma unroll
+            for (int db = 0; db < ND; ++db)
+                dd_mul_add(hi[da], lo[da], __ldg(v + da * rowlen + k * ND + db), xv[db]);
+    }
+}
+
+// r = f - K u (FP64, node blocks, compensated sums) and r.r, for the
+// reliable updates of the mixed form and the defect correction.
 template <int ND, int G>
 __global__ void __launch_bounds__(BLOCK, NODE_BLOCKS_PER_SM)
 residual_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
@@ -334,17 +411,17 @@ residual_node_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
     for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
          nb += int64_t(gridDim.x) * nodes_per_block) {
         const int64_t i = nb + ((threadIdx.x & 31) / G);
-        double acc[ND];
+        double hi[ND], lo[ND];
 #pragma unroll
-        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+        for (int da = 0; da < ND; ++da) hi[da] = lo[da] = 0.0;
         if (i < n_nodes)
-            node_rows<ND, G, double, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
+            node_rows_dd<ND, G, false>(adj_ptr, adj, node_base, vals, u, i, gl, hi, lo);
 #pragma unroll
-        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+        for (int da = 0; da < ND; ++da) group_sum_dd<G>(hi[da], lo[da]);
         if (i < n_nodes && gl == 0)
 #pragma unroll
             for (int da = 0; da < ND; ++da) {
-                double ri = f[i * ND + da] - acc[da];
+                const double ri = dd_residual(f[i * ND + da], hi[da], lo[da]);
                 r[i * ND + da] = ri;
                 rr += ri * ri;
             }
@@ -2072,18 +2149,19 @@ batch_pcg_mixed_kernel(int count, const int32_t* __restrict__ order,
                 for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1;
                      nb += step) {
                     const int64_t i = nb + ((threadIdx.x & 31) / G);
-                    double acc[ND];
+                    double hi[ND], lo[ND];
 #pragma unroll
-                    for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                    for (int da = 0; da < ND; ++da) hi[da] = lo[da] = 0.0;
                     if (i < n1)
-                        node_rows_mv<ND, G, double>(adj_ptr, adj, node_base, vals, u, i, gl, acc);
+                        node_rows_dd<ND, G, false>(adj_ptr, adj, node_base, vals, u, i, gl, hi,
+                                                   lo);
 #pragma unroll
-                    for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                    for (int da = 0; da < ND; ++da) group_sum_dd<G>(hi[da], lo[da]);
                     if (i < n1 && gl == 0) {
 #pragma unroll
                         for (int da = 0; da < ND; ++da) {
                             const int64_t row = i * ND + da;
-                            const double ri = f[row] - acc[da];
+                            const double ri = dd_residual(f[row], hi[da], lo[da]);
                             r[row] = ri;
                             trr += ri * ri;
                             trz += ri * (ri * inv_diag[row]);
@@ -2327,19 +2405,19 @@ batch_pcg_cluster_kernel(int count, const int32_t* __restrict__ order,
                     for (int64_t nb = n0 + int64_t(threadIdx.x >> 5) * warp_nodes; nb < n1;
                          nb += step) {
                         const int64_t i = nb + ((threadIdx.x & 31) / G);
-                        double acc[ND];
+                        double hi[ND], lo[ND];
 #pragma unroll
-                        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
+                        for (int da = 0; da < ND; ++da) hi[da] = lo[da] = 0.0;
                         if (i < n1)
-                            node_rows_cg<ND, G, double, double>(adj_ptr, adj, node_base, vals, u,
-                                                                i, gl, acc);
+                            node_rows_dd<ND, G, true>(adj_ptr, adj, node_base, vals, u, i, gl,
+                                                      hi, lo);
 #pragma unroll
-                        for (int da = 0; da < ND; ++da) acc[da] = group_sum<G>(acc[da]);
+                        for (int da = 0; da < ND; ++da) group_sum_dd<G>(hi[da], lo[da]);
                         if (i < n1 && gl == 0) {
 #pragma unroll
                             for (int da = 0; da < ND; ++da) {
                                 const int64_t row = i * ND + da;
-                                const double ri = f[row] - acc[da];
+                                const double ri = dd_residual(f[row], hi[da], lo[da]);
                                 r[row] = ri;
                                 trr += ri * ri;
                                 trz += ri * (ri * inv_diag[row]);
@@ -3267,10 +3345,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
         res = hs.h->res;
     }
     // 2. FP32 operator on the same Krylov space to the tolerance, for at
-    // most as many iterations as the FP64 phase took; past that budget the
-    // FP64 operator continues on the same search directions (a solve whose
-    // hard part lies below tau gains nothing from FP32 and would carry the
-    // FP32 operator's error into its soft modes)
+    // most as many iterations as the FP64 phase took
     if (status == PCG_RELIABLE) {
         SVX_CUDA(cudaMemcpyAsync(r64.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         set_field(&PcgScalars::rr_stop, -1.0);
