@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 METRIC = "PCG DOF-iters/s & solves/s: mixed/batched vs FP64 at 1e-8 err; p50/p99 ms"
 UNIT = "DOF*iter/s"
 HBM_FALLBACK_GBS = 6650.0
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "pcg_persistent_fp64_c3d8_160x16x16.txt")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "pcg_smem_fp64_c3d8_160x16x16.txt")
 BATCH_TRAFFIC_FILE = os.path.join(ROOT, "profiles", "batch_pcg_fp64_plates4096_dram.txt")
 
 
@@ -130,7 +130,8 @@ def _profile_figure(path, key):
 
 
 def ncu_traffic():
-    """DRAM bytes per iteration of the persistent PCG kernel (ncu summary)."""
+    """DRAM bytes per iteration of the shared-memory persistent PCG kernel
+    (ncu summary)."""
     return _profile_figure(TRAFFIC_FILE, "dram_bytes_per_iteration")
 
 
@@ -402,7 +403,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                 "solves_per_s": world * e2e_steps / (float(e_ms.item()) / 1000.0)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "pcg_persistent_kernel<3,32,double> "
+        "roofline": {"bound": "hbm", "kernel": "pcg_smem_kernel<3,32,512,1,0,4> "
                                                  f"(FP64, {chunk} PCG iterations a launch)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,

@@ -410,7 +410,6 @@ void device_assemble(svx_ctx* ctx, svx_op* op) {
                                  cudaMemcpyDeviceToDevice, st));
     }
     op->vals32.reset();
-    op->vals32v.reset();
     op->vals32q.reset();
     op->valsT.reset();
     apply_dirichlet(ctx, op);
@@ -965,8 +964,7 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         if (const char* e = std::getenv("SVX_PCG_SMEM")) ctx->pcg_smem = (e[0] != '0');
         if (const char* e = std::getenv("SVX_PCG_ALG")) ctx->pcg_alg = (e[0] == '0') ? 0 : 1;
         if (const char* e = std::getenv("SVX_PCG_STAGE")) ctx->pcg_stage = (e[0] != '0');
-        if (const char* e = std::getenv("SVX_FP32_LAYOUT"))
-            ctx->fp32_layout = std::max(0, std::min(2, std::atoi(e)));
+        if (const char* e = std::getenv("SVX_FP32_QUADS")) ctx->fp32_quads = (e[0] != '0');
         if (const char* e = std::getenv("SVX_PCG_UNROLL")) {
             const long v = std::strtol(e, nullptr, 10);
             if (v == 1 || v == 2 || v == 4) ctx->pcg_unroll = int(v);

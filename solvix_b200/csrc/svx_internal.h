@@ -195,9 +195,9 @@ struct svx_ctx {
     // 1: the three-barrier form stages the gathered p window in shared
     // memory; SVX_PCG_STAGE=0 gathers from L2 (measurements)
     int pcg_stage = 1;
-    // the FP32 operator's vectorised copy: 2 quads, 1 float4-padded rows,
-    // 0 none (the node-block kernel); SVX_FP32_LAYOUT (measurements)
-    int fp32_layout = 2;
+    // 1: the graph form's FP32 SpMV runs on the quad copy of the operator,
+    // 0: on the node-block layout; SVX_FP32_QUADS (measurements)
+    int fp32_quads = 1;
 };
 
 namespace svx {
@@ -277,12 +277,6 @@ struct svx_op {
     // slot fastest: the shared-memory PCG kernel's operand (ndof >= 2)
     svx::DBuf<double> valsT;
     svx::DBuf<float> vals32;       // FP32 copy (mixed precision)
-    // the FP32 copy again with every node's rows 16-byte aligned and padded
-    // to whole float4s (3D operators, graph-form SpMV); base32v[i] is node
-    // i's first float, its rows are round_up(ndof * degree, 4) floats apart
-    svx::DBuf<float> vals32v;
-    svx::DBuf<int64_t> base32v;
-    int64_t n32v = 0;
     // the FP32 copy in quads (3D operators, graph-form SpMV): node i's 9
     // (da, db) rows over its neighbour slots, slot fastest, padded to a
     // multiple of 4 slots, from baseq[i]; adjq its neighbours padded with

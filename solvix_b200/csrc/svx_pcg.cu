@@ -49,12 +49,7 @@ constexpr int BLOCK = 256;
 // Resident blocks per SM the node-block SpMV kernels are compiled for; their
 // grids are exactly one wave of that many blocks per SM.
 constexpr int NODE_BLOCKS_PER_SM = 5;
-// The same for the vectorised FP32 SpMV, which holds two nodes' rows a lane.
-#ifndef SVX_SPMV32V_BPS
-#define SVX_SPMV32V_BPS 4
-#endif
-constexpr int SPMV32V_BLOCKS_PER_SM = SVX_SPMV32V_BPS;
-// ... and for the quad-layout FP32 SpMV (ND*ND float4 values a lane)
+// The same for the quad-layout FP32 SpMV (ND*ND float4 values a lane).
 #ifndef SVX_SPMV32Q_BPS
 #define SVX_SPMV32Q_BPS 3
 #endif
@@ -653,29 +648,6 @@ __global__ void compensated_fp32_kernel(int64_t n_nodes, const int64_t* __restri
 
 
 
-// ------------------------------------------------------------ padded FP32 operator
-// Rows of node i in the padded layout: round_up(ND d, 4) floats apart (4 for
-// a node no element uses, whose rows hold only their diagonal).
-__host__ __device__ inline int padded_row(int nd, int d) { return d == 0 ? 4 : (nd * d + 3) & ~3; }
-
-// vals32 (node-block layout) -> vals32v (padded): one thread per node row,
-// the padding zero-filled.
-template <int ND>
-__global__ void pad_fp32_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
-                                const int64_t* __restrict__ node_base,
-                                const int64_t* __restrict__ base32v,
-                                const float* __restrict__ vals32, float* __restrict__ out) {
-    const int64_t t = int64_t(blockIdx.x) * BLOCK + threadIdx.x;
-    const int64_t i = t / ND;
-    if (i >= n_nodes) return;
-    const int da = int(t % ND);
-    const int d = int(adj_ptr[i + 1] - adj_ptr[i]);
-    const int len = d == 0 ? 1 : ND * d, rs = padded_row(ND, d);
-    const float* src = vals32 + node_base[i] + int64_t(da) * len;
-    float* dst = out + base32v[i] + int64_t(da) * rs;
-    for (int c = 0; c < rs; ++c) dst[c] = c < len ? src[c] : 0.0f;
-}
-
 // vals (row da of node i, neighbour slot k, column db at node_base[i] +
 // da ND d + k ND + db) -> valsT, the same values of each node with the slot
 // fastest: (da ND + db) d + k.  One thread per (node, da, db); a node no
@@ -699,135 +671,6 @@ __global__ void transpose_blocks_kernel(int64_t n_nodes, const int64_t* __restri
     double* dst = out + base + int64_t(da * ND + db) * d;
     for (int k = 0; k < d; ++k) dst[k] = src[int64_t(k) * ND];
 }
-
-// q = K32 p for the difference-form FP32 operator in the padded layout and
-// the block partial of p.q (the last block forms pap and alpha, as
-// spmv_node_dot_kernel does).  One warp per node.  Lanes k < d stage the
-// node's neighbour differences p_j - p_i (p_i for its own block) in the
-// warp's shared buffer, in four planes by element index mod 4, so that the
-// lanes of one float4 word read consecutive doubles (no bank conflicts);
-// every lane then multiplies whole float4 words of the node's rows
-// (16-byte, coalesced) with the staged values in FP64.  The rows of the next
-// node are loaded before this node's are used, so one node's K stream is in
-// flight while the warp gathers and multiplies the other.  Needs at most 32
-// neighbour blocks a node.
-template <int ND>
-struct Rows32v {
-    static constexpr int PLANE = ((ND * 32 + 3) & ~3) >> 2;  // float4 words of a row, at most
-    static constexpr int PASSES = (ND * PLANE + 31) / 32;     // float4 words of a node per lane
-};
-
-template <int ND>
-__device__ __forceinline__ void load_rows32v(int64_t node, const int64_t* __restrict__ adj_ptr,
-                                             const int64_t* __restrict__ base32v,
-                                             const float* __restrict__ vals32v, int lane,
-                                             float4 (&out)[Rows32v<ND>::PASSES]) {
-    const int d = int(__ldg(adj_ptr + node + 1) - __ldg(adj_ptr + node));
-    const int words = ND * (padded_row(ND, d) >> 2);
-    const float4* v4 = reinterpret_cast<const float4*>(vals32v + __ldg(base32v + node));
-#pragma unroll
-    for (int ps = 0; ps < Rows32v<ND>::PASSES; ++ps) {
-        const int t = ps * 32 + lane;
-        out[ps] = t < words ? __ldg(v4 + t) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-}
-
-template <int ND, class V>
-__global__ void __launch_bounds__(BLOCK, SPMV32V_BLOCKS_PER_SM)
-spmv32v_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
-                        const int32_t* __restrict__ adj, const int64_t* __restrict__ base32v,
-                        const float* __restrict__ vals32v, const V* __restrict__ p,
-                        V* __restrict__ q, double* __restrict__ partials,
-                        PcgScalars* __restrict__ s) {
-    constexpr int PLANE = Rows32v<ND>::PLANE, PASSES = Rows32v<ND>::PASSES;
-    __shared__ double sh[32];
-    __shared__ double xw_all[BLOCK / 32][4][PLANE];
-    if (s->status != PCG_RUNNING) return;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double(*xw)[PLANE] = xw_all[w];
-    double dot = 0.0;
-    const int64_t warps = int64_t(gridDim.x) * (BLOCK / 32);
-    int64_t i = int64_t(blockIdx.x) * (BLOCK / 32) + w;
-    float4 kv[PASSES];
-    if (i < n_nodes) load_rows32v<ND>(i, adj_ptr, base32v, vals32v, lane, kv);
-    for (; i < n_nodes; i += warps) {
-        const int64_t a0 = adj_ptr[i];
-        const int d = int(adj_ptr[i + 1] - a0);
-        const int nq = padded_row(ND, d) >> 2;
-        if (d > 0) {
-            if (lane < d) {
-                const int32_t j = __ldg(adj + a0 + lane);
-#pragma unroll
-                for (int db = 0; db < ND; ++db) {
-                    const double xj = double(__ldg(p + int64_t(j) * ND + db));
-                    const int c = lane * ND + db;
-                    xw[c & 3][c >> 2] =
-                            (j != int32_t(i)) ? xj - double(__ldg(p + i * ND + db)) : xj;
-                }
-            }
-            const int len = ND * d;
-            if (lane < 4 * nq - len) {  // the padding of the last word multiplies zeros
-                const int c = len + lane;
-                xw[c & 3][c >> 2] = 0.0;
-            }
-        }
-        float4 kn[PASSES];
-        const int64_t nx = i + warps;
-        if (nx < n_nodes) load_rows32v<ND>(nx, adj_ptr, base32v, vals32v, lane, kn);
-        __syncwarp();
-        double acc[ND];
-#pragma unroll
-        for (int da = 0; da < ND; ++da) acc[da] = 0.0;
-        if (d == 0) {  // a node no element uses: word da holds row da's diagonal
-#pragma unroll
-            for (int da = 0; da < ND; ++da)
-                if (lane == da) acc[da] = double(kv[0].x) * double(__ldg(p + i * ND + da));
-        } else {
-#pragma unroll
-            for (int ps = 0; ps < PASSES; ++ps) {
-                const int t = ps * 32 + lane;
-                if (t < ND * nq) {
-                    const int row = t / nq, k = t - row * nq;
-                    double sum = double(kv[ps].x) * xw[0][k];
-                    sum += double(kv[ps].y) * xw[1][k];
-                    sum += double(kv[ps].z) * xw[2][k];
-                    sum += double(kv[ps].w) * xw[3][k];
-#pragma unroll
-                    for (int da = 0; da < ND; ++da)
-                        if (row == da) acc[da] += sum;
-                }
-            }
-        }
-#pragma unroll
-        for (int da = 0; da < ND; ++da) acc[da] = warp_sum(acc[da]);
-        if (lane == 0)
-#pragma unroll
-            for (int da = 0; da < ND; ++da) {
-                q[i * ND + da] = V(acc[da]);
-                dot += double(__ldg(p + i * ND + da)) * acc[da];
-            }
-        __syncwarp();  // the staged values are rewritten for the next node
-#pragma unroll
-        for (int ps = 0; ps < PASSES; ++ps) kv[ps] = kn[ps];
-    }
-    double bs = block_sum(dot, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = bs;
-    if (last_block(&s->count_a)) {
-        double pap = sum_partials(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            s->count_a = 0;
-            s->pap = pap;
-            if (pap <= 0.0 || isnan(pap)) {
-                s->status = PCG_BREAKDOWN;
-                s->it = s->it + 1;
-                s->res = sqrt(s->rr) / s->bnorm;
-            } else {
-                s->alpha = s->rz / pap;
-            }
-        }
-    }
-}
-
 
 // ------------------------------------------------------------ quad FP32 operator
 // vals32 (node-block layout) -> vals32q: node i's ND*ND (da, db) rows over
@@ -1545,7 +1388,10 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
 // into shared memory once an iteration (coalesced), instead of every node
 // gathering its neighbours' p from L2.  The window holds up to
 // STAGE_NODES_PER_NODE x nodes_cap nodes; a block whose window is wider
-// (an unstructured node order) gathers from L2 as before.
+// (an unstructured node order) gathers from L2 as before.  (On the
+// 160 x 16 x 16 C3D8 cantilever a block's window spans 5,800 nodes; staging
+// it whole in the shared memory left over, 139 KB, measured 26.5 against
+// 25.4 us an iteration gathering from L2.)
 constexpr int STAGE_NODES_PER_NODE = 4;
 
 __host__ __device__ inline size_t smem_adj_offset(int64_t nodes_cap, int nd) {
@@ -1555,12 +1401,10 @@ __host__ __device__ inline size_t smem_adj_offset(int64_t nodes_cap, int nd) {
 // Dynamic shared memory of pcg_smem_kernel for `nodes_cap` nodes of `nd`
 // dofs and at most max_deg neighbours: six vectors of nodes_cap * nd
 // doubles, the adjacency in load_shared_adj's layout (rounded up to 16
-// bytes), then for the three-barrier form the staging window.
-size_t smem_pcg_bytes(int64_t nodes_cap, int nd, int max_deg, int alg) {
+// bytes), then the staging window of stage_nodes nodes.
+size_t smem_pcg_bytes(int64_t nodes_cap, int nd, int max_deg, int64_t stage_nodes) {
     const size_t adj = (shared_adj_bytes(nodes_cap, max_deg) + 15) / 16 * 16;
-    const size_t stage =
-        alg == 0 ? size_t(STAGE_NODES_PER_NODE) * size_t(nodes_cap) * size_t(nd) * 8 : 0;
-    return smem_adj_offset(nodes_cap, nd) + adj + stage;
+    return smem_adj_offset(nodes_cap, nd) + adj + size_t(stage_nodes) * size_t(nd) * 8;
 }
 
 // One node's rows for the two-barrier form: x_j = z_j + beta * pprev_j.
@@ -1705,7 +1549,7 @@ pcg_smem_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
         __syncthreads();
         jlo = s_jlo;
         jhi = s_jhi;
-        staged = stage && nloc > 0 && (jhi - jlo + 1) <= STAGE_NODES_PER_NODE * nodes_cap;
+        staged = nloc > 0 && (jhi - jlo + 1) <= stage;
     }
     if (threadIdx.x == 0) {
         s_c[0] = vs->bnorm;
@@ -2612,7 +2456,7 @@ struct PcgRun {
 
     void enqueue_iteration(cudaStream_t st) {
         if constexpr (std::is_same<M, float>::value) {
-            if (vals == op->vals32.p && (op->vals32v.p || op->vals32q.p))
+            if (vals == op->vals32.p && op->vals32q.p)
                 launch_spmv_fp32(op, G, grid_r, st, p, q, partials, s);
             else
                 launch_spmv_node_dot<M, V>(op, G, grid_r, st, vals, p, q, partials, s);
@@ -2777,10 +2621,17 @@ struct PcgRun {
             int max_smem = 0;
             SVX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                                             ctx->device));
-            const size_t smem = smem_pcg_bytes(nodes_cap, ND, op->pat.max_deg, alg);
-            if (smem > size_t(max_smem)) return -1;
             void* fn = kernel_for();
             if (!fn) return -1;
+            cudaFuncAttributes fa{};
+            SVX_CUDA(cudaFuncGetAttributes(&fa, fn));
+            const size_t avail = size_t(max_smem) - std::min(size_t(max_smem), fa.sharedSizeBytes);
+            const size_t base = smem_pcg_bytes(nodes_cap, ND, op->pat.max_deg, 0);
+            if (base > avail) return -1;
+            // the three-barrier form's staging window
+            int stage = (alg == 0 && ctx->pcg_stage) ? STAGE_NODES_PER_NODE * nodes_cap : 0;
+            const size_t smem = smem_pcg_bytes(nodes_cap, ND, op->pat.max_deg, stage);
+            if (smem > avail) return -1;
             SVX_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(smem)));
             int bps = 0;
@@ -2803,7 +2654,6 @@ struct PcgRun {
             double* zp = z.p;
             int first = 1;
             int max_deg = std::max(op->pat.max_deg, 1);
-            int stage = ctx->pcg_stage;
             if (!p2) return -1;
             void* args[] = {&n_nodes, (void*)&a_ptr, (void*)&a_idx, (void*)&nbase,
                             (void*)&valsT, (void*)&inv_diag, (void*)&u, (void*)&r, (void*)&p,
@@ -2959,8 +2809,8 @@ void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
     SVX_LAUNCH_CHECK();
     // a vectorised copy for the graph form's FP32 SpMV (3D, <= 32 neighbour
     // blocks a node); its offsets depend only on the pattern
-    if (op->ndof != 3 || P.max_deg > 32 || op->n_nodes == 0 || ctx->fp32_layout == 0) return;
-    if (ctx->fp32_layout == 2) {
+    if (op->ndof != 3 || P.max_deg > 32 || op->n_nodes == 0 || !ctx->fp32_quads) return;
+    {
         if (!op->baseq.p) {
             std::vector<int64_t> ap(size_t(op->n_nodes) + 1), base(size_t(op->n_nodes) + 1);
             SVX_CUDA(cudaMemcpyAsync(ap.data(), P.adj_ptr.p, ap.size() * sizeof(int64_t),
@@ -2983,26 +2833,7 @@ void build_fp32_operator(svx_ctx* ctx, svx_op* op) {
             op->n_nodes, P.adj_ptr.p, P.adj.p, P.node_base.p, op->baseq.p, op->vals32.p,
             op->vals32q.p, op->adjq.p);
         SVX_LAUNCH_CHECK();
-        return;
     }
-    if (!op->base32v.p) {
-        std::vector<int64_t> ap(size_t(op->n_nodes) + 1), base(size_t(op->n_nodes) + 1);
-        SVX_CUDA(cudaMemcpyAsync(ap.data(), P.adj_ptr.p, ap.size() * sizeof(int64_t),
-                                 cudaMemcpyDeviceToHost, ctx->stream));
-        SVX_CUDA(cudaStreamSynchronize(ctx->stream));
-        base[0] = 0;
-        for (int64_t i = 0; i < op->n_nodes; ++i)
-            base[i + 1] = base[i] + 3 * int64_t(padded_row(3, int(ap[i + 1] - ap[i])));
-        op->base32v.alloc(ctx->pool, base.size());
-        SVX_CUDA(cudaMemcpyAsync(op->base32v.p, base.data(), base.size() * sizeof(int64_t),
-                                 cudaMemcpyHostToDevice, ctx->stream));
-        op->n32v = base.back();
-    }
-    op->vals32v.alloc(ctx->pool, size_t(op->n32v) + 4);
-    const int64_t rows = op->n_nodes * 3;
-    pad_fp32_kernel<3><<<unsigned((rows + BLOCK - 1) / BLOCK), BLOCK, 0, ctx->stream>>>(
-        op->n_nodes, P.adj_ptr.p, P.node_base.p, op->base32v.p, op->vals32.p, op->vals32v.p);
-    SVX_LAUNCH_CHECK();
 }
 
 // The graph form's FP32 SpMV: a vectorised kernel on its copy of the
@@ -3020,16 +2851,6 @@ void launch_spmv_fp32(const svx_op* op, int G, unsigned grid, cudaStream_t st, c
         spmv32q_node_dot_kernel<3, V><<<grid, BLOCK, 0, st>>>(op->n_nodes, P.adj_ptr.p,
                                                                op->baseq.p, op->adjq.p,
                                                                op->vals32q.p, p, q, partials, s);
-    } else if (op->vals32v.p) {
-        const Pattern& P = op->pat;
-        // one wave at this kernel's residency, never more blocks than the
-        // caller's partials hold
-        grid = unsigned(std::min<int64_t>(
-                {int64_t(grid), int64_t(op->ctx->sm_count) * SPMV32V_BLOCKS_PER_SM,
-                 (op->n_nodes + BLOCK / 32 - 1) / (BLOCK / 32)}));
-        spmv32v_node_dot_kernel<3, V><<<grid, BLOCK, 0, st>>>(op->n_nodes, P.adj_ptr.p,
-                                                               P.adj.p, op->base32v.p,
-                                                               op->vals32v.p, p, q, partials, s);
     } else {
         launch_spmv_node_dot<float, V>(op, G, grid, st, op->vals32.p, p, q, partials, s);
     }
