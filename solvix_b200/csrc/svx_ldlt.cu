@@ -9,13 +9,14 @@
 // one block column per step:
 //
 //   panel kernel   every block factors the diagonal tile (J, J) into L_JJ and
-//                  D_J (one warp, rows in registers, columns exchanged by
-//                  shuffles); block 0 stores them apart from the band (the
+//                  D_J (the whole block, in shared memory, one column per
+//                  step); block 0 stores them apart from the band (the
 //                  other blocks are still reading tile (J, J)); block g
 //                  solves the panel tile (J+1+g, J): W = A L_JJ^-T,
 //                  L = W D_J^-1;
-//   update kernel  one block per tile pair J < K <= I <= J + w:
-//                  A_IK -= W_IJ L_KJ^T (W keeps the product L D).
+//   update kernel  one 64-thread block per tile pair J < K <= I <= J + w:
+//                  A_IK -= W_IJ L_KJ^T (W keeps the product L D), a 4 x 4
+//                  register block per thread.
 //
 // Each step is two ordinary launches, so nothing on the device waits for
 // another block.  The pivot test is the reference's: D_i not finite or
@@ -36,6 +37,7 @@
 #include <cmath>
 
 #include "svx_internal.h"
+#include "svx_grid.h"
 
 namespace svx {
 
@@ -127,36 +129,31 @@ ldlt_panel_kernel(int64_t J, int64_t n, int w, int wj, double* __restrict__ band
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    if (warp == 0) {
-        // Right-looking LDL^T of the tile in registers: lane r holds row r.
-        // At column c every lane takes W[k][c] (k > c) from lane k by a
-        // shuffle before any lane replaces its own W[r][c] by L[r][c], so
-        // each entry gets A[r][k] - sum_c L[r][c] W[k][c] in column order.
-        const int r = lane;
-        double a[LT];
-#pragma unroll
-        for (int k = 0; k < LT; ++k) a[k] = s_l[r][k];
-#pragma unroll
-        for (int c = 0; c < LT; ++c) {
-            const double dc = __shfl_sync(0xffffffffu, a[c], c);
-            const int64_t eq = J * LT + c;
-            if (r == 0 && blockIdx.x == 0 && eq < n) {
-                const double lim = 1e-13 * fmax(row_max[eq], DBL_MIN);
-                if (!isfinite(dc) || dc <= lim)
-                    atomicMin(fail, (unsigned long long)(eq) << 1 | (dc < 0.0 ? 1ull : 0ull));
-            }
-            const double l = r > c ? a[c] / dc : 0.0;
-#pragma unroll
-            for (int k = c + 1; k < LT; ++k) {
-                const double wkc = __shfl_sync(0xffffffffu, a[c], k);
-                if (r >= k) a[k] -= l * wkc;
-            }
-            if (r > c) a[c] = l;
+    // Right-looking LDL^T of the tile in shared memory, the whole block at
+    // once: at column c every entry (r, k), c < k <= r, takes
+    // A[r][k] -= (W[r][c] / D_c) W[k][c] with W column c still unscaled,
+    // then column c becomes L = W / D_c; so each entry gets
+    // A[r][k] - sum_c L[r][c] W[k][c] in column order.
+    for (int c = 0; c < LT; ++c) {
+        const double dc = s_l[c][c];
+        const int64_t eq = J * LT + c;
+        if (threadIdx.x == 0 && blockIdx.x == 0 && eq < n) {
+            const double lim = 1e-13 * fmax(row_max[eq], DBL_MIN);
+            if (!isfinite(dc) || dc <= lim)
+                atomicMin(fail, (unsigned long long)(eq) << 1 | (dc < 0.0 ? 1ull : 0ull));
         }
-#pragma unroll
-        for (int k = 0; k < LT; ++k) s_l[r][k] = a[k];
+        {
+            // thread (r, g) takes row r, columns c + 1 + g, c + 9 + g, ... <= r
+            const int r = threadIdx.x >> 3, g = threadIdx.x & 7;
+            if (r > c) {
+                const double l = s_l[r][c] / dc;
+                for (int k = c + 1 + g; k <= r; k += 8) s_l[r][k] -= l * s_l[k][c];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x > c && threadIdx.x < LT) s_l[threadIdx.x][c] /= dc;
+        __syncthreads();
     }
-    __syncthreads();
     if (blockIdx.x == 0) {
         double* out = dfac + size_t(J) * LT2;
         for (int k = threadIdx.x; k < LT2; k += LBLOCK) out[k] = s_l[k / LT][k % LT];
@@ -196,11 +193,18 @@ ldlt_panel_kernel(int64_t J, int64_t n, int w, int wj, double* __restrict__ band
 // Step J, second half (grid: wj (wj + 1) / 2 blocks): block q takes the
 // pair (di, dk), 1 <= dk <= di <= wj, q = di (di - 1) / 2 + dk - 1, and
 // updates tile (J + di, di - dk) with W_(J+di) L_(J+dk)^T.
-__global__ void __launch_bounds__(LBLOCK)
+//
+// 64 threads a pair, each a 4 x 4 block of the tile in registers: both
+// operand tiles are staged in shared memory transposed (column c of W and
+// of L a row of 33 doubles), so at each c a thread reads 4 + 4 values for
+// 16 multiply-adds.  Every output is summed over c in column order, then
+// subtracted, as in a scalar loop.
+constexpr int UBLOCK = 64;
+__global__ void __launch_bounds__(UBLOCK)
 ldlt_update_kernel(int64_t J, int w, int wj, double* __restrict__ band,
                    const double* __restrict__ panel, const unsigned long long* fail) {
-    __shared__ double s_w[LT][LT + 1];
-    __shared__ double s_k[LT][LT + 1];
+    __shared__ double s_w[LT][LT + 1];  // s_w[c][r] = W[r][c]
+    __shared__ double s_k[LT][LT + 1];  // s_k[c][s] = L[s][c]
     __shared__ int s_flag;
     if (stopped(fail, &s_flag)) return;
     int q = int(blockIdx.x), di = 1;
@@ -210,25 +214,55 @@ ldlt_update_kernel(int64_t J, int w, int wj, double* __restrict__ band,
     }
     const int dk = q + 1;
     if (di > wj) return;
-    const double* wt = panel + size_t(di - 1) * LT2;
-    const double* lk = band + tile_off(J + dk, dk, w);
-    for (int k = threadIdx.x; k < LT2; k += LBLOCK) {
-        s_w[k / LT][k % LT] = wt[k];
-        s_k[k / LT][k % LT] = lk[k];
+    const double2* wt = reinterpret_cast<const double2*>(panel + size_t(di - 1) * LT2);
+    const double2* lk = reinterpret_cast<const double2*>(band + tile_off(J + dk, dk, w));
+    const int r0 = (threadIdx.x >> 3) * 4;
+    const int s0 = (threadIdx.x & 7) * 4;
+    double* t = band + tile_off(J + di, di - dk, w) + size_t(r0) * LT + s0;
+    // every load of the block in flight at once: both operand tiles as
+    // 16-byte words, and the thread's 4 x 4 outputs
+    constexpr int Q = LT2 / 2 / UBLOCK;
+    double2 wv[Q], lv[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        wv[q] = __ldg(wt + threadIdx.x + UBLOCK * q);
+        lv[q] = __ldg(lk + threadIdx.x + UBLOCK * q);
+    }
+    double tv[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tv[i][j] = t[size_t(i) * LT + j];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int e = 2 * (int(threadIdx.x) + UBLOCK * q), row = e / LT, col = e % LT;
+        s_w[col][row] = wv[q].x;
+        s_w[col + 1][row] = wv[q].y;
+        s_k[col][row] = lv[q].x;
+        s_k[col + 1][row] = lv[q].y;
     }
     __syncthreads();
-    const int r = threadIdx.x >> 3;
-    const int s0 = (threadIdx.x & 7) * 4;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 4
     for (int c = 0; c < LT; ++c) {
-        const double a = s_w[r][c];
+        double a[4], b[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[j] += a * s_k[s0 + j][c];
+        for (int i = 0; i < 4; ++i) a[i] = s_w[c][r0 + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = s_k[c][s0 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
     }
-    double* t = band + tile_off(J + di, di - dk, w) + size_t(r) * LT + s0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) t[j] -= acc[j];
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) t[size_t(i) * LT + j] = tv[i][j] - acc[i][j];
 }
 
 // L y = P f, y /= D, L^T x = y, u = P^T x in one block (y: nb * LT
@@ -301,6 +335,144 @@ ldlt_solve_kernel(int64_t n, int64_t nb, int w, const double* __restrict__ band,
         __syncthreads();
     }
     for (int64_t r = threadIdx.x; r < n; r += SBLOCK) u[r] = y[perm[r]];
+}
+
+// L y = P f, y /= D, L^T x = y, u = P^T x over the whole GPU (cooperative
+// launch, one block per SM, a bounded grid barrier per block row).  In the
+// forward sweep, iteration I: block 0 finishes y_I from the partial sums
+// the other blocks left for row I (tiles d >= 2, part[I & 1]) plus its own
+// T(I, 1) y_(I-1), then solves the diagonal tile; meanwhile block b >= 1
+// forms T(I+1, d) y_(I+1-d) for its tiles d = 1 + b, 1 + b + (B - 1), ...
+// (d >= 2: those y are final a barrier earlier) into part[(I+1) & 1].  The
+// backward sweep mirrors it with transposed tiles, z = y / D taken when a
+// block row is finished.  Every tile product has the same thread mapping
+// wherever it runs and block 0 adds the partial sums in d order, so the
+// result does not depend on the block count.
+constexpr int TBLOCK = 256;
+static_assert(TBLOCK == 8 * LT, "eight column (or row) groups of four per tile");
+
+// the 32 results of one tile product (forward: rows of T times x over its
+// columns; backward: columns of T times x over its rows), summed over the
+// eight groups in order; valid in threads 0..31 of the block.  x was
+// written by another block during the launch and is read from L2.
+template <bool TRANS>
+__device__ __forceinline__ double tile_product(const double* __restrict__ t,
+                                               const double* x, double (*s_red)[LT]) {
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = 4 * g + j;
+        const double xk = __ldcg(x + k);
+        s += TRANS ? t[size_t(k) * LT + lane] * xk : t[size_t(lane) * LT + k] * xk;
+    }
+    s_red[g][lane] = s;
+    __syncthreads();
+    double tot = 0.0;
+    if (threadIdx.x < LT)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) tot += s_red[q][threadIdx.x];
+    __syncthreads();
+    return tot;
+}
+
+__global__ void __launch_bounds__(TBLOCK)
+ldlt_solve_coop_kernel(int64_t n, int64_t nb, int w, const double* __restrict__ band,
+                       const double* __restrict__ dfac, const double* __restrict__ dvec,
+                       const int32_t* __restrict__ perm, const double* __restrict__ f,
+                       double* y, double* __restrict__ u, double* part, GridBarrier* gb,
+                       const unsigned long long* fail) {
+    __shared__ double s_red[8][LT];
+    __shared__ double s_acc[8][LT];
+    __shared__ int s_flag;
+    if (stopped(fail, &s_flag)) return;
+    const unsigned int B = gridDim.x;
+    unsigned int target = 0;
+    const int64_t rows = nb * LT;
+    const int64_t tid = int64_t(blockIdx.x) * TBLOCK + threadIdx.x, nthr = int64_t(B) * TBLOCK;
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const size_t pstride = size_t(w + 1) * LT;  // one buffer of part
+    for (int64_t i = tid; i < rows; i += nthr) y[i] = 0.0;
+    if (!grid_sync(gb, B, target)) return;
+    for (int64_t r = tid; r < n; r += nthr) y[perm[r]] = f[r];
+    if (!grid_sync(gb, B, target)) return;
+    // block 0's sum of the others' partials for block row R (d = 2..dmax):
+    // thread (lane, g) adds d = 2 + g, 10 + g, ... in order, then the groups
+    // are added in order
+    auto partial_sum = [&](int64_t R, int dmax) -> double {
+        const double* pb = part + size_t(R & 1) * pstride;
+        double s = 0.0;
+        for (int d = 2 + g; d <= dmax; d += 8) s += __ldcg(pb + size_t(d) * LT + lane);
+        s_acc[g][lane] = s;
+        __syncthreads();
+        double tot = 0.0;
+        if (threadIdx.x < LT)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) tot += s_acc[q][threadIdx.x];
+        __syncthreads();
+        return tot;
+    };
+    for (int64_t I = 0; I < nb; ++I) {
+        if (blockIdx.x == 0) {
+            const int dmax = int(I < w ? I : w);
+            double tot = partial_sum(I, dmax);
+            if (dmax >= 1) {
+                const double t1 = tile_product<false>(band + tile_off(I, 1, w),
+                                                       y + (I - 1) * LT, s_red);
+                tot = t1 + tot;
+            }
+            if (threadIdx.x < LT) {
+                double x = __ldcg(y + I * LT + lane) - tot;
+                const double* t = dfac + size_t(I) * LT2 + size_t(lane) * LT;
+                for (int c = 0; c < LT; ++c) {
+                    const double v = __shfl_sync(0xffffffffu, x, c);
+                    if (lane > c) x -= t[c] * v;
+                }
+                y[I * LT + lane] = x;
+            }
+        } else if (I + 1 < nb) {
+            const int64_t R = I + 1;
+            const int dmax = int(R < w ? R : w);
+            double* pb = part + size_t(R & 1) * pstride;
+            for (int d = 1 + int(blockIdx.x); d <= dmax; d += int(B) - 1) {
+                const double v = tile_product<false>(band + tile_off(R, d, w), y + (R - d) * LT,
+                                                      s_red);
+                if (threadIdx.x < LT) pb[size_t(d) * LT + lane] = v;
+            }
+        }
+        if (!grid_sync(gb, B, target)) return;
+    }
+    for (int64_t J = nb - 1; J >= 0; --J) {
+        if (blockIdx.x == 0) {
+            const int dmax = int(nb - 1 - J < w ? nb - 1 - J : w);
+            double tot = partial_sum(J, dmax);
+            if (dmax >= 1) {
+                const double t1 = tile_product<true>(band + tile_off(J + 1, 1, w),
+                                                      y + (J + 1) * LT, s_red);
+                tot = t1 + tot;
+            }
+            if (threadIdx.x < LT) {
+                double z = __ldcg(y + J * LT + lane) / dvec[J * LT + lane] - tot;
+                const double* t = dfac + size_t(J) * LT2 + lane;
+                for (int r = LT - 1; r >= 0; --r) {
+                    const double v = __shfl_sync(0xffffffffu, z, r);
+                    if (lane < r) z -= t[size_t(r) * LT] * v;
+                }
+                y[J * LT + lane] = z;
+            }
+        } else if (J >= 1) {
+            const int64_t R = J - 1;
+            const int dmax = int(nb - 1 - R < w ? nb - 1 - R : w);
+            double* pb = part + size_t(R & 1) * pstride;
+            for (int d = 1 + int(blockIdx.x); d <= dmax; d += int(B) - 1) {
+                const double v = tile_product<true>(band + tile_off(R + d, d, w),
+                                                     y + (R + d) * LT, s_red);
+                if (threadIdx.x < LT) pb[size_t(d) * LT + lane] = v;
+            }
+        }
+        if (!grid_sync(gb, B, target)) return;
+    }
+    for (int64_t r = tid; r < n; r += nthr) u[r] = __ldcg(y + perm[r]);
 }
 
 // ||f||^2, ||f - K u||^2, max |D_i| and min |D_i| (one block, fixed order).
@@ -420,14 +592,47 @@ LdltOutcome ldlt_direct(svx_ctx* ctx, svx_op* op, double* u) {
             J, n, w, wj, band.p, panel.p, dfac.p, dvec.p, row_max.p, fail.p);
         SVX_LAUNCH_CHECK();
         if (wj > 0) {
-            ldlt_update_kernel<<<unsigned(int64_t(wj) * (wj + 1) / 2), LBLOCK, 0, st>>>(
+            ldlt_update_kernel<<<unsigned(int64_t(wj) * (wj + 1) / 2), UBLOCK, 0, st>>>(
                 J, w, wj, band.p, panel.p, fail.p);
             SVX_LAUNCH_CHECK();
         }
     }
-    ldlt_solve_kernel<<<1, SBLOCK, 0, st>>>(n, nb, w, band.p, dfac.p, dvec.p, d_perm.p, op->f.p,
-                                            y.p, u, fail.p);
-    SVX_LAUNCH_CHECK();
+    // the substitutions over the whole GPU when a cooperative launch of one
+    // block per SM is possible, else in one block
+    int coop = 0, bps = 0;
+    SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+    SVX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, ldlt_solve_coop_kernel,
+                                                           TBLOCK, 0));
+    DBuf<double> part;
+    DBuf<GridBarrier> gb;
+    const bool coop_solve = coop && bps >= 1 && ctx->sm_count >= 2;
+    if (coop_solve) {
+        part.alloc(ctx->pool, 2 * (size_t(w) + 1) * LT);
+        gb.alloc(ctx->pool, 1);
+        SVX_CUDA(cudaMemsetAsync(gb.p, 0, sizeof(GridBarrier), st));
+        const double* band_p = band.p;
+        const double* dfac_p = dfac.p;
+        const double* dvec_p = dvec.p;
+        const int32_t* perm_p = d_perm.p;
+        const double* f_p = op->f.p;
+        double* y_p = y.p;
+        double* part_p = part.p;
+        GridBarrier* gb_p = gb.p;
+        const unsigned long long* fail_p = fail.p;
+        int64_t n_a = n, nb_a = nb;
+        int w_a = w;
+        void* args[] = {&n_a, &nb_a, &w_a, (void*)&band_p, (void*)&dfac_p, (void*)&dvec_p,
+                        (void*)&perm_p, (void*)&f_p, (void*)&y_p, (void*)&u, (void*)&part_p,
+                        (void*)&gb_p, (void*)&fail_p};
+        SVX_CUDA(cudaLaunchCooperativeKernel((void*)ldlt_solve_coop_kernel,
+                                             dim3(unsigned(ctx->sm_count)), dim3(TBLOCK), args,
+                                             0, st));
+        SVX_LAUNCH_CHECK();
+    } else {
+        ldlt_solve_kernel<<<1, SBLOCK, 0, st>>>(n, nb, w, band.p, dfac.p, dvec.p, d_perm.p,
+                                                op->f.p, y.p, u, fail.p);
+        SVX_LAUNCH_CHECK();
+    }
     spmv_fp64(ctx, op, op->vals.p, u, ku.p);
     ldlt_finish_kernel<<<1, SBLOCK, 0, st>>>(n, op->f.p, ku.p, dvec.p, out.p);
     SVX_LAUNCH_CHECK();
@@ -438,7 +643,13 @@ LdltOutcome ldlt_direct(svx_ctx* ctx, svx_op* op, double* u) {
     SVX_CUDA(cudaMemcpyAsync(&h_fail, fail.p, sizeof h_fail, cudaMemcpyDeviceToHost, st));
     SVX_CUDA(cudaMemcpyAsync(&h_bad, bad.p, sizeof h_bad, cudaMemcpyDeviceToHost, st));
     SVX_CUDA(cudaMemcpyAsync(h_out, out.p, sizeof h_out, cudaMemcpyDeviceToHost, st));
+    GridBarrier h_gb{};
+    if (coop_solve)
+        SVX_CUDA(cudaMemcpyAsync(&h_gb, gb.p, sizeof h_gb, cudaMemcpyDeviceToHost, st));
     SVX_CUDA(cudaStreamSynchronize(st));
+    if (h_gb.error)
+        throw ModelFail{SVX_CUDA_ERROR, 0, -1,
+                        "direct path: a grid barrier wait of the substitutions ran out"};
     float ms = 0.0f;
     SVX_CUDA(cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]));
     res.ms = ms;

@@ -32,6 +32,7 @@
 // serve the allocation-free entry point, which takes a caller's CSR.
 
 #include "svx_internal.h"
+#include "svx_grid.h"
 
 #include <cooperative_groups.h>
 
@@ -836,17 +837,12 @@ spmv32q_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
 #endif
 constexpr int PBLOCK = SVX_PBLOCK;
 constexpr int PBLOCKS_PER_SM = SVX_PBLOCKS_PER_SM;
-constexpr long long BARRIER_SPIN_LIMIT = 1LL << 25;
 // largest per-block shared adjacency copy of the persistent kernels (bytes;
 // 0 keeps the adjacency in global memory)
 #ifndef SVX_SHARED_ADJ_MAX
 #define SVX_SHARED_ADJ_MAX (96 * 1024)
 #endif
 constexpr long long SHARED_ADJ_MAX = SVX_SHARED_ADJ_MAX;
-// back-off between two polls of a grid barrier's arrival count
-#ifndef SVX_BARRIER_SLEEP_NS
-#define SVX_BARRIER_SLEEP_NS 32
-#endif
 
 // One node's rows given its d column node indices (cols: global memory,
 // read through the read-only path, or shared memory when SCOLS) and its
@@ -898,53 +894,6 @@ __device__ __forceinline__ void node_rows_cg(const int64_t* __restrict__ adj_ptr
     const int64_t a0 = adj_ptr[i];
     node_rows_cg_at<ND, G, M, V, false>(adj + a0, int(adj_ptr[i + 1] - a0), vals + node_base[i],
                                         x, i, gl, acc);
-}
-
-// Bounded grid-wide barrier (all blocks co-resident: cooperative launch).
-// gb->count only grows during a launch (the host zeroes it before each
-// launch); every block keeps its own running target, nblocks more per
-// barrier.  After bar.sync, thread 0 arrives with a gpu-scope release add
-// (cumulative over the block's writes ordered before it by the bar.sync)
-// and polls with acquire loads until the count reaches the target; the
-// closing bar.sync passes that on to the block.  A block that polls
-// spin_limit times raises gb->error and returns false, and so does a block
-// that finds the flag raised by another while it waits.
-__device__ __forceinline__ void barrier_arrive(unsigned int* p) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
-}
-__device__ __forceinline__ unsigned int barrier_count(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned int nblocks,
-                                          unsigned int& target,
-                                          long long spin_limit = BARRIER_SPIN_LIMIT) {
-    __shared__ int ok;
-    target += nblocks;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int good = 1;
-        barrier_arrive(&gb->count);
-        long long spins = 0;
-        while (barrier_count(&gb->count) < target) {
-            if (++spins > spin_limit) {
-                atomicExch(&gb->error, 1);
-                good = 0;
-                break;
-            }
-            if ((spins & 255) == 0 && *((volatile int*)&gb->error) != 0) {
-                good = 0;
-                break;
-            }
-#if SVX_BARRIER_SLEEP_NS > 0
-            __nanosleep(SVX_BARRIER_SLEEP_NS);
-#endif
-        }
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
 }
 
 // Fixed-order sum of n partials (stride `stride`, offset `off`) read from L2.
