@@ -1456,7 +1456,7 @@ def run_kernels(args, local_rank):
     * iteration: the FP64 node-block SpMV + p.Kp, the u/r update, the p
       update and the FP32 difference-form SpMV, each over --reps
       back-to-back launches (CUDA events);
-    * solve: one full FP64 solve (the persistent kernel below 50M nonzeros);
+    * solve: one full FP64 solve (the persistent kernel while K fits in L2);
     * batch / batch-3d: one batched solve of the first --batch-count plates
       of the 4,096-plate mix / C3D8 cantilevers of the served stream;
     * direct: the direct path twice, the second run's device time."""

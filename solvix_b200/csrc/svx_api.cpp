@@ -951,6 +951,7 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         std::unique_ptr<svx_ctx> ctx(new svx_ctx());
         ctx->device = device;
         ctx->sm_count = prop.multiProcessorCount;
+        ctx->l2_bytes = prop.l2CacheSize;
         if (const char* e = std::getenv("SVX_SHARED_ADJ_MAX")) {
             char* end = nullptr;
             const long long v = std::strtoll(e, &end, 10);

@@ -161,6 +161,7 @@ private:
 struct svx_ctx {
     int device = 0;
     int sm_count = 0;
+    int64_t l2_bytes = 0;  // the device's L2 cache size
     int batch_choice[4] = {-1, -1, -1, -1};  // autotuned batched-PCG shape: FP64 (2D, 3D),
                                              // mixed (2D, 3D)
     cudaStream_t stream = nullptr;

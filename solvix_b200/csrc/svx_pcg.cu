@@ -2692,18 +2692,22 @@ struct PinnedScalars {
 
 // Iterations per persistent launch: a few to tens of milliseconds of work,
 // so the host sees progress and a long solve is not one unbounded launch.
-// Systems above GRAPH_MIN_NNZ iterate with the three standalone kernels in a
-// CUDA graph instead of the persistent kernel: there an iteration streams
-// more than 400 MB, so launch gaps are noise, and the standalone node SpMV
-// (5 blocks of 256 threads per SM, more loads in flight) runs at ~80% of
-// the HBM copy peak where the persistent kernel's SpMV phase (2 blocks of
-// 512) reaches ~55%.  Below it, K stays in L2 and the persistent kernel's
-// absence of launch gaps wins.
+// Systems whose FP64 K does not fit in L2 (or above GRAPH_MIN_NNZ) iterate
+// with the three standalone kernels in a CUDA graph instead of the
+// persistent kernel: K streams from HBM every iteration, launch gaps are
+// noise, and the standalone node SpMV (5 blocks of 256 threads per SM,
+// more loads in flight) runs at ~80% of the HBM copy peak.  While K fits in
+// L2 the persistent kernel's absence of launch gaps and grid-wide state in
+// shared memory win (the 160 x 16 x 16 C3D8 cantilever, K 83 MB: 25.9
+// against 34.1 us an iteration); above it the graph form does (240 x 24 x 24,
+// K 277 MB: 79.0 against 82.4 us; the 480 x 48 x 48 conduction block, K
+// 250 MB: 11% more DOF-iterations per second over the whole solve).
 constexpr int64_t GRAPH_MIN_NNZ = 50000000;
 
 bool use_graph_form(const svx_ctx* ctx, const svx_op* op) {
-    const int64_t threshold = ctx->graph_min_nnz >= 0 ? ctx->graph_min_nnz : GRAPH_MIN_NNZ;
-    return op->pat.nnz > threshold;
+    if (ctx->graph_min_nnz >= 0) return op->pat.nnz > ctx->graph_min_nnz;
+    return op->pat.nnz > GRAPH_MIN_NNZ ||
+           (ctx->l2_bytes > 0 && op->pat.nnz * int64_t(sizeof(double)) > ctx->l2_bytes);
 }
 
 int persistent_chunk(int64_t nnz) {

@@ -313,9 +313,9 @@ def test_full_size_cantilever_c3d8_properties(ctx):
 
 
 def test_large_system_graph_path_fp64_and_mixed(ctx):
-    """Above 50M nonzeros the solve iterates the standalone kernels in a
-    CUDA graph (FP64) and the mixed form streams the difference-form FP32
-    operator there too.  Host-checked properties at 657k DOF: the true
+    """Above 50M nonzeros (and whenever K exceeds L2) the solve iterates
+    the standalone kernels in a CUDA graph (FP64) and the mixed form
+    streams the difference-form FP32 operator there too.  Host-checked properties at 657k DOF: the true
     residual of each solution through the CSR on the host, and mixed
     against FP64 within the mixed form's bar.  The stopping rule is the
     reference's, on the recursive residual (solver.rs:108-123); on this
