@@ -136,3 +136,24 @@ def test_flat_api_method_option(ctx):
     assert ref.solver_method == "ldlt"
     assert rel(sol.u, ref.u) <= 1e-8
     assert abs(sol.cond_estimate - ref.cond_estimate) <= 1e-6 * ref.cond_estimate
+
+
+def test_band_wider_than_the_grid(ctx):
+    """A band of more tiles than the substitution kernel has blocks (174
+    tiles against one block per SM, 148 on a B200): every block takes
+    several tiles of a block row.  The 24 x 36 x 36 hex cantilever (102,675
+    DOF, RCM half-bandwidth 5,549 rows) is too large for the oracle's serial
+    LDL^T, so the direct solution is checked against the device's FP64 PCG
+    and by its own residual."""
+    import torch
+
+    from solvix_b200 import workloads
+    flat = workloads.cantilever_c3d8(24, 36, 36)
+    sol = ctx.solve_flat(flat, method=abi.SVX_METHOD_LDLT)
+    assert sol.solver_method == "ldlt" and sol.iterations == 0
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert sol.factor_bandwidth == 5549 and (sol.factor_bandwidth + 31) // 32 > sms - 1
+    assert sol.final_residual <= 1e-8
+    pcg = ctx.solve_flat(flat)
+    assert rel(sol.u, pcg.u) <= 1e-8
+    assert np.max(np.abs(sol.von_mises - pcg.von_mises)) <= 1e-7 * np.max(np.abs(pcg.von_mises))
