@@ -2346,8 +2346,14 @@ unsigned grid_vec(const svx_ctx* ctx, int64_t n) {
 
 // Lanes per node for the node-block kernels: the smallest of 8 / 16 / 32
 // that covers the largest node degree (27 for interior C3D8 nodes).
-int pick_node_group(int max_deg) {
-    if (max_deg <= 8) return 8;
+// Lanes per node of the node-block kernels: enough to cover the neighbour
+// blocks once for 2D and 3D rows; one dof per node (conduction) gives a
+// lane a single value per neighbour, so 8 lanes take several neighbours
+// each and a warp 4 nodes (the 480 x 48 x 48 conduction block, 27
+// neighbours: 32 lanes per node left the SpMV latency bound at one node a
+// warp).
+int pick_node_group(int max_deg, int nd) {
+    if (nd == 1 || max_deg <= 8) return 8;
     if (max_deg <= 16) return 16;
     return 32;
 }
@@ -2825,7 +2831,7 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms4) {
     r.alloc(ctx->pool, n + 1);
     p.alloc(ctx->pool, n + 1);
     q.alloc(ctx->pool, n + 1);
-    const int G = pick_node_group(op->pat.max_deg);
+    const int G = pick_node_group(op->pat.max_deg, op->ndof);
     const unsigned grid_r = grid_nodes(ctx, op->n_nodes, G), grid_v = grid_vec(ctx, n);
     partials.alloc(ctx->pool, 2 * size_t(std::max(grid_r, grid_v)) + 2);
     s.alloc(ctx->pool, 1);
@@ -2869,7 +2875,7 @@ void time_iteration_kernels(svx_ctx* ctx, svx_op* op, int reps, double* ms4) {
 }
 
 void spmv_fp64(svx_ctx* ctx, const svx_op* op, const double* vals, const double* x, double* y) {
-    const int G = pick_node_group(op->pat.max_deg);
+    const int G = pick_node_group(op->pat.max_deg, op->ndof);
     const unsigned grid = grid_nodes(ctx, op->n_nodes, G);
     cudaStream_t st = ctx->stream;
     const Pattern& P = op->pat;
@@ -2900,7 +2906,7 @@ PcgResult pcg_fp64(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, int
         p2.alloc(ctx->pool, n + 1);
         SVX_CUDA(cudaMemsetAsync(p2.p, 0, (n + 1) * sizeof(double), st));
     }
-    const int G = pick_node_group(op->pat.max_deg);
+    const int G = pick_node_group(op->pat.max_deg, op->ndof);
     PcgRun<double, double, double> run;
     run.ctx = ctx;
     run.op = op;
@@ -3010,7 +3016,7 @@ PcgResult pcg_mixed(svx_ctx* ctx, svx_op* op, double tol, long long max_iter, do
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
     build_fp32_operator(ctx, op);
-    const int G = pick_node_group(op->pat.max_deg);
+    const int G = pick_node_group(op->pat.max_deg, op->ndof);
     DBuf<double> r, p, p2, q, r64, partials, rr_dev;
     DBuf<PcgScalars> s;
     DBuf<unsigned int> counter;
@@ -3219,7 +3225,7 @@ PcgResult pcg_defect_correction(svx_ctx* ctx, svx_op* op, double tol, long long 
     const int64_t n = op->n;
     cudaStream_t st = ctx->stream;
     build_fp32_operator(ctx, op);
-    const int G = pick_node_group(op->pat.max_deg);
+    const int G = pick_node_group(op->pat.max_deg, op->ndof);
     const unsigned grid_r = grid_nodes(ctx, op->n_nodes, G), grid_v = grid_vec(ctx, n);
     DBuf<float> r32, p32, q32, e32, d32;
     DBuf<double> r64, e64, r, p, q, partials, rr_dev;
