@@ -966,6 +966,7 @@ int svx_ctx_create(int device, svx_ctx_t** out) {
         if (const char* e = std::getenv("SVX_PCG_ALG")) ctx->pcg_alg = (e[0] == '0') ? 0 : 1;
         if (const char* e = std::getenv("SVX_PCG_STAGE")) ctx->pcg_stage = (e[0] != '0');
         if (const char* e = std::getenv("SVX_FP32_QUADS")) ctx->fp32_quads = (e[0] != '0');
+        if (const char* e = std::getenv("SVX_PCG_LANES")) ctx->pcg_lanes = std::atoi(e);
         if (const char* e = std::getenv("SVX_PCG_UNROLL")) {
             const long v = std::strtol(e, nullptr, 10);
             if (v == 1 || v == 2 || v == 4) ctx->pcg_unroll = int(v);

@@ -190,9 +190,12 @@ struct svx_ctx {
     // iteration, neighbours forming p from z and the previous p; 0 = three,
     // p stored); SVX_PCG_ALG in the environment at svx_ctx_create sets it
     int pcg_alg = -1;
-    // its nodes per warp step with all loads in flight (0: 4);
+    // its nodes per warp step with all loads in flight (0: 1);
     // SVX_PCG_UNROLL sets it
     int pcg_unroll = 0;
+    // lanes per node of the shared-memory kernel: 0 (or 8) eight, 32 (3D)
+    // or 16 (2D) the degree-covering groups; SVX_PCG_LANES (measurements)
+    int pcg_lanes = 0;
     // 1: the three-barrier form stages the gathered p window in shared
     // memory; SVX_PCG_STAGE=0 gathers from L2 (measurements)
     int pcg_stage = 1;

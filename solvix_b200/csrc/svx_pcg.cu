@@ -1400,12 +1400,11 @@ __device__ __forceinline__ double gathered(const double* x, const double* z, con
 // One node's rows, lane gl of its G-lane group taking neighbour blocks gl,
 // gl + G, ...  The values come from the transposed copy valsT (entry
 // (da, db) of neighbour slot k at (da ND + db) d + k from the node's base),
-// so the lanes' loads of one (da, db) are consecutive doubles: 7 sectors a
-// warp request for a C3D8 node against 21 in the row layout, whose lanes
-// stride ND doubles.  The first block is loaded under a predicate rather
-// than a branch, so that the U nodes of a warp step issue all their loads
-// before their first multiply-add; nodes with more than G neighbour blocks
-// (none in a C3D8 or CPS4 mesh at G = 32 / 16) loop over the rest.
+// so the loads of one (da, db) by the lanes of a group are consecutive
+// doubles, where in the row layout they stride ND doubles.  The first
+// block is loaded under a predicate rather than a branch, so that the U
+// nodes of a warp step issue its loads before their first multiply-add;
+// the blocks past the first G (a C3D8 node's 27 at G = 8) loop.
 template <int ND, int G, int ALG, bool XS>
 __device__ __forceinline__ void node_rows_pred(bool valid, const int32_t* cols, int d,
                                                const double* v, const double* x,
@@ -2534,8 +2533,19 @@ struct PcgRun {
         } else {
             cudaStream_t st = ctx->stream;
             const int ND = op->ndof;
+            // 8 lanes per node and one node a lane group per warp step (4
+            // nodes a warp), whatever the degree: each lane walks 3-4 of a
+            // C3D8 node's 27 neighbour blocks.  Measured against 32 lanes
+            // with 4 nodes a warp step (16 for 2D): the 160x16x16 C3D8
+            // cantilever 25.4 -> 19.5 us an iteration, its heterogeneous
+            // twin 25.4 -> 19.5, the 40x4x4 hex 7.54 -> 7.10, the 200x20
+            // CPS4 cantilever 7.26 -> 6.42 (2 and 4 nodes a lane group were
+            // slower with 8 lanes).  SVX_PCG_LANES (16 or 32) and
+            // SVX_PCG_UNROLL override it for measurements.
             const bool narrow = op->pat.max_deg <= 8;
-            const int G = ND == 3 ? (narrow ? 8 : 32) : (narrow ? 8 : 16);
+            const int G = ctx->pcg_lanes == 32 && ND == 3 && !narrow ? 32
+                          : ctx->pcg_lanes == 16 && ND != 3 && !narrow ? 16
+                                                                        : 8;
             int coop = 0;
             SVX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
             if (!coop) return -1;
@@ -2551,7 +2561,7 @@ struct PcgRun {
             const int nodes_cap = int((op->n_nodes + B - 1) / B);
             const int alg =
                 ctx->pcg_alg >= 0 ? ctx->pcg_alg : ((ND <= 2 || nodes_cap <= 64) ? 1 : 0);
-            const int unroll = ctx->pcg_unroll > 0 ? ctx->pcg_unroll : 4;
+            const int unroll = ctx->pcg_unroll > 0 ? ctx->pcg_unroll : 1;
             auto kernel_for = [&]() -> void* {
 #define SVX_SMEM_PICK(ND_, G_)                                                           \
     if (ND == ND_ && G == G_) {                                                          \
