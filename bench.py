@@ -403,7 +403,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                 "solves_per_s": world * e2e_steps / (float(e_ms.item()) / 1000.0)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "pcg_smem_kernel<3,32,512,1,0,4> "
+        "roofline": {"bound": "hbm", "kernel": "pcg_smem_kernel<3,8,512,1,0,1> "
                                                  f"(FP64, {chunk} PCG iterations a launch)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
