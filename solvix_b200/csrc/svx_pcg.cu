@@ -2352,6 +2352,13 @@ unsigned grid_vec(const svx_ctx* ctx, int64_t n) {
 // neighbours: 32 lanes per node left the SpMV latency bound at one node a
 // warp).
 int pick_node_group(int max_deg, int nd) {
+    // SVX_NODE_LANES (8, 16 or 32) forces the choice, for measurements
+    static const int forced = [] {
+        const char* e = std::getenv("SVX_NODE_LANES");
+        const int v = e ? std::atoi(e) : 0;
+        return (v == 8 || v == 16 || v == 32) ? v : 0;
+    }();
+    if (forced) return forced;
     if (nd == 1 || max_deg <= 8) return 8;
     if (max_deg <= 16) return 16;
     return 32;
