@@ -1340,7 +1340,7 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
 // (an unstructured node order) gathers from L2 as before.  (On the
 // 160 x 16 x 16 C3D8 cantilever a block's window spans 5,800 nodes; staging
 // it whole in the shared memory left over, 139 KB, measured 26.5 against
-// 25.4 us an iteration gathering from L2.)
+// 25.4 us an iteration gathering from L2, both with 32 lanes a node.)
 constexpr int STAGE_NODES_PER_NODE = 4;
 
 __host__ __device__ inline size_t smem_adj_offset(int64_t nodes_cap, int nd) {
@@ -2559,10 +2559,11 @@ struct PcgRun {
             // one block of 512 threads per SM: fewer arrivals per grid barrier
             // measured faster than 1,024-thread or two-block shapes.  The
             // two-barrier form (ALG 1) gathers two vectors per neighbour
-            // value: it wins for 2D and small 3D systems (the C1 cantilever
-            // 7.56 -> 6.24 us an iteration) and loses at the 160x16x16 C3D8
-            // size (25.7 -> 28.6 us); SVX_PCG_ALG and SVX_PCG_UNROLL
-            // override the choice for measurements.
+            // value: it wins for 2D and small 3D systems (with 8 lanes a
+            // node: the 200x20 CPS4 cantilever 7.81 -> 6.47 us an
+            // iteration, the 40x4x4 hex 8.37 -> 7.20) and loses at the
+            // 160x16x16 C3D8 size (19.6 -> 25.1 us); SVX_PCG_ALG and
+            // SVX_PCG_UNROLL override the choice for measurements.
             constexpr int PB = 512;
             const unsigned int B = unsigned(ctx->sm_count);
             const int nodes_cap = int((op->n_nodes + B - 1) / B);
@@ -2721,7 +2722,7 @@ struct PinnedScalars {
 // noise, and the standalone node SpMV (5 blocks of 256 threads per SM,
 // more loads in flight) runs at ~80% of the HBM copy peak.  While K fits in
 // L2 the persistent kernel's absence of launch gaps and grid-wide state in
-// shared memory win (the 160 x 16 x 16 C3D8 cantilever, K 83 MB: 25.9
+// shared memory win (the 160 x 16 x 16 C3D8 cantilever, K 83 MB: 19.5
 // against 34.1 us an iteration); above it the graph form does (240 x 24 x 24,
 // K 277 MB: 79.0 against 82.4 us; the 480 x 48 x 48 conduction block, K
 // 250 MB: 11% more DOF-iterations per second over the whole solve).
