@@ -477,10 +477,11 @@ typedef struct svx_batch_stats {
 } svx_batch_stats_t;
 
 /* Solves `count` independent models of equal ndof.  They are
- * assembled as one block-diagonal operator; one persistent launch then runs
- * every model's Jacobi-PCG with its own scalars, convergence test and
- * iteration budget (max(1000, 10 n_model) unless opts->max_iter > 0), one
- * CTA per model at a time, largest models first.  The CTA size and lanes
+ * assembled as one block-diagonal operator; one launch per size class then
+ * runs every model's Jacobi-PCG with its own scalars, convergence test and
+ * iteration budget (max(1000, 10 n_model) unless opts->max_iter > 0): one
+ * CTA per model for the small ones and one thread-block cluster per model
+ * for the large ones, largest models first.  The CTA size and lanes
  * per node are autotuned once per context and ndof, and kept.  Per model
  * outputs: u[k] (n_nodes*ndof) and von_mises[k] (n_elem), host arrays, any
  * may be NULL.  Each model is checked on its own: one that is rejected
