@@ -101,3 +101,16 @@ def test_mix_cpu_sample_is_bounded_and_labelled():
     assert cb["kind"] == "port" and cb["unit"] == bench.UNIT and cb["value"] > 0
     assert cb["extrapolated"] is True and cb["solves_per_s"] > 0
     assert "extrapolated" in cb["sample"]
+
+
+def test_algorithmic_bytes_of_the_160x16x16_cantilever():
+    """The roofline numerators: K values, one column index per 3 x 3 block,
+    adj_ptr and node_base, p gathered once, q written, p read for the dot;
+    then the two vector updates (11 doubles a row)."""
+    from solvix_b200.roofline import pcg_iteration_bytes, spmv_node_bytes
+    n, nnz, nodes = 139_587, 10_393_929, 46_529
+    spmv = spmv_node_bytes(n, nnz, 3, nodes)
+    assert spmv == 8 * nnz + 4 * nnz // 9 + 16 * (nodes + 1) + 24 * n
+    assert pcg_iteration_bytes(n, nnz, 3, nodes) == spmv + 88 * n == 104_149_180
+    # the FP32 operator streams 4-byte values and the same indices
+    assert spmv_node_bytes(n, nnz, 3, nodes, value_bytes=4) == spmv - 4 * nnz
