@@ -545,63 +545,6 @@ init_kernel(int64_t n, const B* __restrict__ b, double b_scale, U* __restrict__ 
     }
 }
 
-// Plain y = K x (FP64), one row per G lanes.
-template <int G>
-__global__ void __launch_bounds__(BLOCK)
-spmv_kernel(int64_t n, const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ col_idx,
-            const double* __restrict__ vals, const double* __restrict__ x,
-            double* __restrict__ y) {
-    const int gl = threadIdx.x & (G - 1);
-    const int64_t groups_per_block = BLOCK / G;
-    for (int64_t rb = warp_first_row<G>(groups_per_block); rb < n;
-         rb += int64_t(gridDim.x) * groups_per_block) {
-        const int64_t r = rb + ((threadIdx.x & 31) / G);
-        const bool valid = r < n;
-        double v =
-            valid ? row_dot<G, double>(col_idx, vals, x, row_ptr[r], row_ptr[r + 1], gl) : 0.0;
-#pragma unroll
-        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (valid && gl == 0) y[r] = v;
-    }
-}
-
-// Mixed precision outer step: r = f - K u (FP64), partial of r.r.
-template <int G>
-__global__ void __launch_bounds__(BLOCK)
-residual_kernel(int64_t n, const int32_t* __restrict__ row_ptr,
-                const int32_t* __restrict__ col_idx, const double* __restrict__ vals,
-                const double* __restrict__ u, const double* __restrict__ f,
-                double* __restrict__ r, double* __restrict__ partials,
-                unsigned int* counter, double* __restrict__ out_rr) {
-    __shared__ double sh[32];
-    const int gl = threadIdx.x & (G - 1);
-    const int64_t groups_per_block = BLOCK / G;
-    double rr = 0.0;
-    for (int64_t rb = warp_first_row<G>(groups_per_block); rb < n;
-         rb += int64_t(gridDim.x) * groups_per_block) {
-        const int64_t i = rb + ((threadIdx.x & 31) / G);
-        const bool valid = i < n;
-        double v =
-            valid ? row_dot<G, double>(col_idx, vals, u, row_ptr[i], row_ptr[i + 1], gl) : 0.0;
-#pragma unroll
-        for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (valid && gl == 0) {
-            double ri = f[i] - v;
-            r[i] = ri;
-            rr += ri * ri;
-        }
-    }
-    double b = block_sum(rr, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = b;
-    if (last_block(counter)) {
-        double t = sum_partials(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            *counter = 0;
-            *out_rr = t;
-        }
-    }
-}
-
 // The FP32 operator of the mixed form.  Rounding each entry of K to FP32
 // (relative error ~6e-8) breaks K's translation null space: for a smooth
 // field x the product K x is the small difference of large terms, and the
@@ -1354,34 +1297,6 @@ __host__ __device__ inline size_t smem_adj_offset(int64_t nodes_cap, int nd) {
 size_t smem_pcg_bytes(int64_t nodes_cap, int nd, int max_deg, int64_t stage_nodes) {
     const size_t adj = (shared_adj_bytes(nodes_cap, max_deg) + 15) / 16 * 16;
     return smem_adj_offset(nodes_cap, nd) + adj + size_t(stage_nodes) * size_t(nd) * 8;
-}
-
-// One node's rows for the two-barrier form: x_j = z_j + beta * pprev_j.
-template <int ND, int G>
-__device__ __forceinline__ void node_rows_zp(const int32_t* cols, int d, const double* v,
-                                             const double* z, const double* pprev, double beta,
-                                             int64_t i, int gl, double* acc) {
-    if (d == 0) {
-        if (gl == 0)
-#pragma unroll
-            for (int da = 0; da < ND; ++da)
-                acc[da] = v[da] * __fma_rn(beta, __ldcg(pprev + i * ND + da),
-                                           __ldcg(z + i * ND + da));
-        return;
-    }
-    const int rowlen = ND * d;
-    for (int k = gl; k < d; k += G) {
-        const int64_t c = int64_t(cols[k]) * ND;
-        double xv[ND];
-#pragma unroll
-        for (int db = 0; db < ND; ++db)
-            xv[db] = __fma_rn(beta, __ldcg(pprev + c + db), __ldcg(z + c + db));
-#pragma unroll
-        for (int da = 0; da < ND; ++da)
-#pragma unroll
-            for (int db = 0; db < ND; ++db)
-                acc[da] += __ldg(v + da * rowlen + k * ND + db) * xv[db];
-    }
 }
 
 // The gathered value of column c: p_c itself (ALG 0) or z_c + beta pprev_c
