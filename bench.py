@@ -86,11 +86,14 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(KERNEL_WORKLOADS), default="c3d8_160",
                     help="kernels form: the model")
     ap.add_argument("--kernel-mode", choices=["iteration", "solve", "batch", "batch-3d",
-                                              "direct"], default="iteration",
+                                              "direct", "defect"], default="iteration",
                     help="kernels form: the iteration kernels back to back (iteration), one "
                          "FP64 solve (solve), one batched solve of --batch-count plates or "
                          "C3D8 cantilevers of the served stream (batch, batch-3d), the direct "
-                         "path (direct)")
+                         "path (direct), an FP64 solve and one defect-correction solve per "
+                         "--inner-tols value (defect)")
+    ap.add_argument("--inner-tols", type=str, default="1e-1,1e-2,1e-3,1e-4,1e-5,1e-6",
+                    help="kernels form, defect mode: comma-separated inner tolerances")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--reps", type=int, default=20, help="kernels form: launches per kernel")
     ap.add_argument("--rates", type=str, default="",
@@ -1459,7 +1462,10 @@ def run_kernels(args, local_rank):
     * solve: one full FP64 solve (the persistent kernel while K fits in L2);
     * batch / batch-3d: one batched solve of the first --batch-count plates
       of the 4,096-plate mix / C3D8 cantilevers of the served stream;
-    * direct: the direct path twice, the second run's device time."""
+    * direct: the direct path twice, the second run's device time;
+    * defect: one FP64 solve, then one SVX_MIXED_DEFECT solve per inner
+      tolerance of --inner-tols, each with its iteration split, its device
+      PCG time against the FP64 one and its error against the FP64 u."""
     from solvix_b200 import Context, abi, workloads
     from solvix_b200.roofline import pcg_iteration_bytes, spmv_node_bytes
 
@@ -1497,7 +1503,35 @@ def run_kernels(args, local_rank):
         try:
             n, nnz = op.n, op.nnz
             out.update({"n": n, "nnz": nnz})
-            if args.kernel_mode == "solve":
+            if args.kernel_mode == "defect":
+                import numpy as np
+
+                from solvix_b200.model import NotConverged
+                u64, it64, _, _ = op.solve(max_iter=200000)
+                _, _, ms64, _, _ = op.solve_device(max_iter=200000, want_stress=False)
+                rows = []
+                for itol in (float(t) for t in args.inner_tols.split(",") if t):
+                    try:
+                        u, it, res, _ = op.solve(precision=abi.SVX_MIXED_DEFECT,
+                                                 inner_tol=itol, max_iter=200000)
+                    except NotConverged as e:
+                        rows.append({"inner_tol": itol, "error": f"NotConverged: {e}"})
+                        continue
+                    row = {"inner_tol": itol, "iterations": it,
+                           "fp32_iterations": op.last_fp32_iterations,
+                           "corrections": op.last_outer_iterations, "residual": res,
+                           "rel_err_vs_fp64": float(np.linalg.norm(u - u64) /
+                                                    np.linalg.norm(u64))}
+                    _, _, ms, _, _ = op.solve_device(precision=abi.SVX_MIXED_DEFECT,
+                                                     inner_tol=itol, max_iter=200000,
+                                                     want_stress=False)
+                    row.update({"pcg_ms": ms, "ms_per_iteration": ms / it,
+                                "vs_fp64": ms64 / ms})
+                    rows.append(row)
+                out.update({"fp64": {"iterations": it64, "pcg_ms": ms64,
+                                     "ms_per_iteration": ms64 / it64},
+                            "defect": rows})
+            elif args.kernel_mode == "solve":
                 runs = []
                 for _ in range(max(1, args.reps)):
                     runs.append(op.solve_device(precision=prec, want_stress=False,

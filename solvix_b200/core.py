@@ -258,6 +258,10 @@ class Operator:
         nnz = C.c_int64()
         self.lib.svx_op_dims(handle, C.byref(n), C.byref(nnz))
         self.n, self.nnz = int(n.value), int(nnz.value)
+        # iteration split of the last solve: FP32-operator iterations and
+        # outer steps (corrections or true-residual checks)
+        self.last_fp32_iterations = 0
+        self.last_outer_iterations = 0
 
     def free(self):
         if getattr(self, "handle", None):
@@ -351,6 +355,7 @@ class Operator:
         if st != abi.SVX_OK:
             _raise(st, err)
         self.last_fp32_iterations = int(sol.fp32_iterations)
+        self.last_outer_iterations = int(sol.outer_iterations)
         return u, int(sol.iterations), float(sol.final_residual), float(sol.cond_estimate)
 
     def stress(self):

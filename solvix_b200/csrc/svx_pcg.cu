@@ -661,30 +661,44 @@ __global__ void quad_fp32_kernel(int64_t n_nodes, const int64_t* __restrict__ ad
 // multiplies in FP64 with p_j - p_i (p_i for the node's own slot and the
 // padding, whose values are zero).  Per lane ND*ND 16-byte value loads are
 // in flight at once: four times the bytes of the node-block kernel's
-// scalar loads, which leave the FP32 operator latency-bound.
+// scalar loads, which leave the FP32 operator latency-bound.  A node's quad
+// count is (baseq[i+1] - baseq[i]) / (4*ND*ND), and both offsets are loaded
+// one node group ahead of their use, so each group's first dependent load
+// is its values, not its offsets.
 template <int ND, class V>
 __global__ void __launch_bounds__(BLOCK, SPMV32Q_BLOCKS_PER_SM)
-spmv32q_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ adj_ptr,
-                        const int64_t* __restrict__ baseq, const int32_t* __restrict__ adjq,
-                        const float* __restrict__ vals32q, const V* __restrict__ p,
-                        V* __restrict__ q, double* __restrict__ partials,
-                        PcgScalars* __restrict__ s) {
+spmv32q_node_dot_kernel(int64_t n_nodes, const int64_t* __restrict__ baseq,
+                        const int32_t* __restrict__ adjq, const float* __restrict__ vals32q,
+                        const V* __restrict__ p, V* __restrict__ q,
+                        double* __restrict__ partials, PcgScalars* __restrict__ s) {
     constexpr int G = 8;
     __shared__ double sh[32];
     if (s->status != PCG_RUNNING) return;
     const int gl = threadIdx.x & (G - 1);
     const int64_t nodes_per_block = BLOCK / G;
+    const int64_t stride = int64_t(gridDim.x) * nodes_per_block;
     double dot = 0.0;
-    for (int64_t nb = warp_first_row<G>(nodes_per_block); nb < n_nodes;
-         nb += int64_t(gridDim.x) * nodes_per_block) {
+    int64_t nb = warp_first_row<G>(nodes_per_block);
+    int64_t qa = 0, qb = 0;  // baseq[i], baseq[i + 1] of this lane's node
+    {
         const int64_t i = nb + ((threadIdx.x & 31) / G);
+        if (i < n_nodes) {
+            qa = __ldg(baseq + i);
+            qb = __ldg(baseq + i + 1);
+        }
+    }
+    for (; nb < n_nodes; nb += stride) {
+        const int64_t i = nb + ((threadIdx.x & 31) / G);
+        const int64_t q0 = qa;
+        const int dq4 = int(qb - qa) / (4 * ND * ND);
+        if (i + stride < n_nodes) {
+            qa = __ldg(baseq + i + stride);
+            qb = __ldg(baseq + i + stride + 1);
+        }
         double acc[ND];
 #pragma unroll
         for (int da = 0; da < ND; ++da) acc[da] = 0.0;
         if (i < n_nodes) {
-            const int d = int(__ldg(adj_ptr + i + 1) - __ldg(adj_ptr + i));
-            const int dq4 = d == 0 ? 1 : (d + 3) >> 2;
-            const int64_t q0 = __ldg(baseq + i);
             const float4* v4 = reinterpret_cast<const float4*>(vals32q + q0);
             const int4* a4 = reinterpret_cast<const int4*>(adjq + q0 / (ND * ND));
             double xi[ND];
@@ -2737,15 +2751,14 @@ template <class V>
 void launch_spmv_fp32(const svx_op* op, int G, unsigned grid, cudaStream_t st, const V* p, V* q,
                       double* partials, PcgScalars* s) {
     if (op->vals32q.p) {
-        const Pattern& P = op->pat;
         // one wave at this kernel's residency, never more blocks than the
         // caller's partials hold
         grid = unsigned(std::min<int64_t>(
                 {int64_t(grid), int64_t(op->ctx->sm_count) * SPMV32Q_BLOCKS_PER_SM,
                  (op->n_nodes + BLOCK / 8 - 1) / (BLOCK / 8)}));
-        spmv32q_node_dot_kernel<3, V><<<grid, BLOCK, 0, st>>>(op->n_nodes, P.adj_ptr.p,
-                                                               op->baseq.p, op->adjq.p,
-                                                               op->vals32q.p, p, q, partials, s);
+        spmv32q_node_dot_kernel<3, V><<<grid, BLOCK, 0, st>>>(op->n_nodes, op->baseq.p,
+                                                               op->adjq.p, op->vals32q.p, p, q,
+                                                               partials, s);
     } else {
         launch_spmv_node_dot<float, V>(op, G, grid, st, op->vals32.p, p, q, partials, s);
     }

@@ -312,12 +312,13 @@ def test_full_size_cantilever_c3d8_properties(ctx):
     assert abs(react[2::3].sum() - 5000.0) <= 1e-6 * 5000.0
 
 
-def test_large_system_graph_path_fp64_and_mixed(ctx):
+def test_large_system_graph_path_fp64_mixed_and_defect(ctx):
     """Above 50M nonzeros (and whenever K exceeds L2) the solve iterates
-    the standalone kernels in a CUDA graph (FP64) and the mixed form
-    streams the difference-form FP32 operator there too.  Host-checked properties at 657k DOF: the true
-    residual of each solution through the CSR on the host, and mixed
-    against FP64 within the mixed form's bar.  The stopping rule is the
+    the standalone kernels in a CUDA graph (FP64); the mixed form and the
+    defect correction's inner solves stream the difference-form FP32
+    operator there too.  Host-checked properties at 657k DOF: the true
+    residual of each solution through the CSR on the host, and both FP32
+    forms against FP64 within their bar.  The stopping rule is the
     reference's, on the recursive residual (solver.rs:108-123); on this
     100x-contrast model the FP64 recursion drifts from the true residual by
     a factor of about 30 over ~5,000 iterations, hence the 1e-8 bar on the
@@ -336,4 +337,12 @@ def test_large_system_graph_path_fp64_and_mixed(ctx):
     assert resm <= 1e-10
     assert np.linalg.norm(f_mod - a @ um) / np.linalg.norm(f_mod) <= 1e-8
     assert rel(um, u64) <= 1e-8
+    # the defect correction: FP32 inner solves (the quad-layout FP32 SpMV on
+    # FP32 vectors) inside FP64 corrections, with its iteration split
+    ud, itd, resd, _ = op.solve(precision=abi.SVX_MIXED_DEFECT)
+    assert resd <= 1e-10
+    assert np.linalg.norm(f_mod - a @ ud) / np.linalg.norm(f_mod) <= 1e-8
+    assert rel(ud, u64) <= 1e-8
+    assert op.last_outer_iterations >= 2
+    assert 0 < op.last_fp32_iterations <= itd
     op.free()
