@@ -634,10 +634,10 @@ int svx_diag_barrier_timeout(int device, long long spins, int* returned_ok, int*
  * array and it keeps the previous call's contents (each call clears what
  * must start at zero), so calls whose work overlaps on the GPU (other
  * threads, other streams) race; serialise them.  The first call on each
- * device looks up the array's device address and keeps it, so make that
- * first call before any stream capture; a cudaDeviceReset of that device
- * afterwards leaves the kept address stale, so do not call this entry point
- * on a device again after resetting it in the same process.
+ * device looks up the array's device address and keeps it.  A
+ * cudaDeviceReset of that device afterwards leaves the kept address stale,
+ * so do not call this entry point on a device again after resetting it in
+ * the same process.
  *
  * Returns SVX_OK; SVX_NOT_CONVERGED when max_iter is reached or the
  * recurrence breaks down (p.Kp <= 0 or NaN), with iterations / residual
