@@ -72,8 +72,8 @@ def parse_args():
                              "kernels"],
                     default="plain",
                     help="plain: the 160x16x16 C3D8 solve (default); batched: 4,096 uneven "
-                         "2D plates in one launch; precision: FP64 vs mixed on the "
-                         "480x48x48 heterogeneous C3D8 model; served: Poisson request "
+                         "2D plates in one launch; precision: FP64, relaxed mixed and defect "
+                         "correction on the 480x48x48 heterogeneous C3D8 model; served: Poisson request "
                          "stream through the continuous-batching server; thermal: steady "
                          "conduction in a 480x48x48 C3D8 block; direct: the band LDL^T "
                          "direct path; kernels: device times of single kernels on one "
@@ -596,67 +596,32 @@ PRECISION_NAME = ("C3D8 cantilever 480x48x48 over 2.0x0.2x0.2 m (1,154,881 nodes
 
 
 def run_precision(args, rank, world, local_rank):
-    """C3: plain FP64 and mixed solves of the heterogeneous model, from the
-    device-resident operator; error of mixed against FP64."""
-    import numpy as np
+    """--form precision: the default line's precision_c3 block (FP64,
+    relaxed mixed and defect-correction solves of the heterogeneous model,
+    device-timed) as a line of its own, its value the FP64 solve's
+    DOF-iterations per second."""
     import torch
 
-    from solvix_b200 import Context, abi, workloads
-
     torch.cuda.set_device(local_rank)
-    flat = workloads.heterogeneous_c3d8(480, 48, 48, seed=3)
-    n = flat.n_dof
-    ctx = Context(local_rank)
-    op = ctx.assemble(flat)
-    res = {}
-    for name, prec in (("fp64", abi.SVX_FP64), ("mixed", abi.SVX_MIXED)):
-        times, its = [], []
-        u = None
-        for _ in range(max(1, args.steps)):
-            t0 = time.perf_counter()
-            op.reassemble()
-            u, it, r, _c = op.solve(precision=prec, max_iter=200000)
-            times.append(time.perf_counter() - t0)
-            its.append(it)
-        res[name] = {"u": u, "iterations": its[-1], "s_per_solve": float(np.mean(times)),
-                     "residual": r, "fp32_iterations": op.last_fp32_iterations}
-    kms = op.time_kernels(reps=10)
-    err = float(np.linalg.norm(res["mixed"]["u"] - res["fp64"]["u"]) /
-                np.linalg.norm(res["fp64"]["u"]))
-    peak, peak_kind = measured_peaks()
-    nnz = op.nnz
-    from solvix_b200.roofline import spmv_node_bytes
-    spmv_bytes = spmv_node_bytes(n, nnz, flat.ndof, flat.n_nodes)
-    fp32_bytes = spmv_bytes - 4 * nnz
-    f64 = res["fp64"]
+    blk = precision_block(local_rank)
+    f64 = blk["fp64"]
+    peak, peak_kind = blk["peak_gbs"], blk["peak_source"]
     line = {
-        "metric": METRIC, "form": "precision", "value": n * f64["iterations"] / f64["s_per_solve"],
-        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": 0,
-        "ms_per_step": 1000 * f64["s_per_solve"], "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "form": "precision", "value": f64["dof_iter_per_s"],
+        "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": f64["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
-        "config": {"workload": PRECISION_NAME, "n_dof": n, "nnz": nnz},
-        "fp64": {"iterations": f64["iterations"], "s_per_solve": f64["s_per_solve"],
-                 "solves_per_s": 1 / f64["s_per_solve"], "residual": f64["residual"]},
-        "mixed": {"iterations": res["mixed"]["iterations"],
-                  "fp32_iterations": res["mixed"]["fp32_iterations"],
-                  "fp32_spmv_ms": float(kms[3]),
-                  "fp32_spmv_gbs": fp32_bytes / (kms[3] / 1000) / 1e9,
-                  "s_per_solve": res["mixed"]["s_per_solve"],
-                  "solves_per_s": 1 / res["mixed"]["s_per_solve"],
-                  "residual_fp64_true": res["mixed"]["residual"],
-                  "rel_err_vs_fp64": err,
-                  "speed_vs_fp64": f64["s_per_solve"] / res["mixed"]["s_per_solve"]},
+        "config": {"workload": PRECISION_NAME, "n_dof": blk["n_dof"], "nnz": blk["nnz"]},
+        "precision_c3": blk,
         "roofline": {"bound": "hbm", "kernel": "node-block FP64 SpMV (spmv_node_dot)",
-                     "achieved": spmv_bytes / (kms[0] / 1000) / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": spmv_bytes / (kms[0] / 1000) / 1e9 / peak,
-                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": int(spmv_bytes),
-                     "launch_ms": float(kms[0]), "traffic": None},
+                     "achieved": blk["spmv_fp64"]["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": blk["spmv_fp64"]["frac"], "peak_source": peak_kind,
+                     "launch_ms": blk["spmv_fp64"]["ms"], "traffic": None},
+        "clocks": blk["clocks"],
     }
-    op.free()
-    ctx.close()
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = precision_cpu_baseline(f64["iterations"], n)
+        line["cpu_baseline"] = precision_cpu_baseline(f64["iterations"], blk["n_dof"])
     return line
 
 
