@@ -114,3 +114,33 @@ def test_algorithmic_bytes_of_the_160x16x16_cantilever():
     assert pcg_iteration_bytes(n, nnz, 3, nodes) == spmv + 88 * n == 104_149_180
     # the FP32 operator streams 4-byte values and the same indices
     assert spmv_node_bytes(n, nnz, 3, nodes, value_bytes=4) == spmv - 4 * nnz
+
+
+def test_precision_form_line_carries_the_block(monkeypatch):
+    """--form precision wraps the default line's precision_c3 block in a
+    contract line of its own (the block itself is device-timed on a GPU)."""
+    import types
+
+    import torch
+    blk = {"workload": bench.PRECISION_NAME, "n_dof": 3464643, "nnz": 272673225,
+           "fp64": {"iterations": 7688, "ms_per_solve": 4400.0, "pcg_ms": 4300.0,
+                    "solves_per_s": 1000.0 / 4400.0,
+                    "dof_iter_per_s": 3464643 * 7688 / 4.4, "residual": 9.9e-11},
+           "mixed": {}, "defect_correction": {},
+           "ratio_mixed_over_fp64": 0.93, "ratio_defect_over_fp64": 0.46,
+           "spmv_fp64": {"ms": 0.451, "gbs": 5330.0, "frac": 0.815},
+           "spmv_fp32": {"ms": 0.271, "gbs": 4850.0, "frac": 0.74},
+           "peak_gbs": 6537.3, "peak_source": "measured", "timing": "t",
+           "clocks": {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 9}}
+    monkeypatch.setattr(bench, "precision_block", lambda rank: blk)
+    monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
+    args = types.SimpleNamespace(no_cpu_baseline=True)
+    line = bench.run_precision(args, 0, 1, 0)
+    assert line["form"] == "precision" and line["metric"] == bench.METRIC
+    assert line["unit"] == bench.UNIT and line["higher_is_better"] is True
+    assert line["value"] == blk["fp64"]["dof_iter_per_s"]
+    assert line["ms_per_step"] == blk["fp64"]["ms_per_solve"]
+    assert line["precision_c3"] is blk
+    assert line["roofline"]["frac"] == blk["spmv_fp64"]["frac"]
+    assert line["config"]["workload"] == bench.PRECISION_NAME
+    assert json.loads(json.dumps(line)) == line
